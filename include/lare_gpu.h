@@ -1,0 +1,197 @@
+/*
+ * lare_gpu.h - C ABI of the B200 (sm_100a) Lagrangian-remap timestep.
+ *
+ * The reference (Warwick-Plasma/Lare3d, Fortran 90) advances its state with
+ * argument-less module procedures that operate on the `shared_data` globals:
+ *
+ *   src/core/lare3d.f90:84   CALL lagrangian_step        (lagran.F90:50)
+ *   src/core/lare3d.f90:85   CALL eulerian_remap(step)   (remap.f90:33)
+ *   src/core/lare3d.f90:87   CALL eta_calc               (lagran.F90:1176)
+ *   src/core/lare3d.f90:88   CALL output_routines(step)  (diagnostics.F90:43,
+ *                            of which energy_account :517 is the hot part)
+ *
+ * This library owns a device-resident copy of that state and replaces those
+ * calls one for one.  Every array argument is a Fortran column-major array
+ * with exactly the ghost-inclusive bounds the reference allocates
+ * (mpi_routines.F90:295-327):
+ *
+ *   cell  rho, energy, eta         (-1:nx+2, -1:ny+2, -1:nz+2)
+ *   node  vx, vy, vz, visc3        (-2:nx+2, -2:ny+2, -2:nz+2)
+ *   face  bx                       (-2:nx+2, -1:ny+2, -1:nz+2)
+ *         by                       (-1:nx+2, -2:ny+2, -1:nz+2)
+ *         bz                       (-1:nx+2, -1:ny+2, -2:nz+2)
+ *   1-D   dxb (-1:nx+2), dxc (-1:nx+1), likewise y and z; grav (-1:nz+2)
+ *
+ * so that a Fortran driver passes its own arrays through iso_c_binding with
+ * no repacking.  All entry points return 0 on success and a negative
+ * LARE_E* code on failure; lare_gpu_last_error() gives the message.  A
+ * context is not thread-safe; it owns one CUDA stream.
+ */
+#ifndef LARE_GPU_H
+#define LARE_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Boundary codes, shared_data.F90:65-66. */
+#define LARE_BC_PERIODIC 1
+#define LARE_BC_USER 2
+#define LARE_BC_OPEN 3
+
+/* Status codes. */
+#define LARE_OK 0
+#define LARE_EINVAL (-1)     /* bad argument, size or unsupported option */
+#define LARE_ECUDA (-2)      /* CUDA runtime error */
+#define LARE_ENOMEM (-3)     /* device allocation failed */
+#define LARE_EDT (-4)        /* dt underflow / non-finite dt from set_dt */
+#define LARE_ESTAGES (-5)    /* RKL2 stage count not representable */
+#define LARE_ENOTFOUND (-6)  /* unknown field name */
+#define LARE_ENONFINITE (-7) /* non-finite value in uploaded state */
+
+/*
+ * Control scalars read by the hot path.  Field names follow
+ * src/control.f90 and src/core/shared_data.F90.
+ */
+typedef struct lare_params {
+  double gamma;            /* ratio of specific heats (setup.F90:46, control.f90:42) */
+  double visc1, visc2;     /* shock viscosity coefficients (control.f90:85-86) */
+  double eta_background;   /* background resistivity (control.f90:119) */
+  double eta0, j_max;      /* anomalous resistivity and current threshold (:121-126) */
+  double kappa_0;          /* normalised Spitzer conductivity (normalise.f90:54-55) */
+  double flux_limiter;     /* Larsen flux limiter (control.f90:134) */
+  double ionise_pot;       /* normalised ionisation potential, 0 unless EOS_ION (normalise.f90:48) */
+  double xi_n;             /* neutral fraction, a constant 0 or 1 under EOS_IDEAL (lare3d.f90:72) */
+  double va_max;           /* Boris Alfven speed limit (control.f90:184) */
+  double dt_multiplier;    /* CFL safety factor, 0.9 in the reference (shared_data.F90:60) */
+  double dt_from_restart;  /* dt used by the first set_dt after a restart (lagran.F90:1080-1086) */
+  double kappa_perp_ratio; /* extension: kappa_perp / kappa_par; 0 reproduces the reference */
+  int resistive_mhd;       /* control.f90:117 */
+  int conduction;          /* control.f90:130 */
+  int heat_flux_limiter;   /* control.f90:132 */
+  int use_viscous_damping; /* control.f90:89 */
+  int boris;               /* control.f90:183 */
+  int restart;             /* IC_RESTART (lare3d.f90:56-60) */
+  int xbc_min, xbc_max, ybc_min, ybc_max, zbc_min, zbc_max; /* control.f90:169-174 */
+} lare_params;
+
+/* Scalars of shared_data that the step updates. */
+typedef struct lare_scalars {
+  double time, dt, dtr;                /* shared_data.F90:126 */
+  double total_visc_heating;           /* shared_data.F90:133 */
+  double total_ohmic_heating;
+  int n_s_stages;                      /* last RKL2 stage count (conduct.f90:139) */
+  int peak_substeps;                   /* lagran.F90:141 */
+  int last_substeps;                   /* resistive sub-cycles of the last step */
+  int steps_taken;                     /* lagrangian steps since init */
+} lare_scalars;
+
+typedef struct lare_ctx lare_ctx;
+
+/*
+ * Create a context for an nx*ny*nz grid (each >= 4).  dxb/dxc etc. are the
+ * Fortran grid metrics written by setup.F90:grid (:92-247); cv is formed on
+ * the device as dxb*dyb*dzb exactly as setup.F90:239-245.  precision is 64
+ * (FP64 drop-in) or 32 (FP32 form: field arithmetic in FP32, dt reduction,
+ * budgets and RKL2 coefficients in FP64).  Replaces mpi_initialise's
+ * allocation (mpi_routines.F90:295-334) for the device copy.
+ */
+int lare_gpu_init(const lare_params* params, int nx, int ny, int nz,
+                  const double* dxb, const double* dxc,
+                  const double* dyb, const double* dyc,
+                  const double* dzb, const double* dzc,
+                  int precision, lare_ctx** out);
+
+/* Upload the state (host Fortran arrays, bounds as in the file header). */
+int lare_gpu_upload(lare_ctx* ctx, const double* rho, const double* energy,
+                    const double* vx, const double* vy, const double* vz,
+                    const double* bx, const double* by, const double* bz);
+
+/*
+ * Upload auxiliary arrays; any pointer may be NULL to keep the current
+ * contents.  eta: cell (as left by eta_calc, lare3d.f90:68); visc3: node;
+ * grav: 1-D (-1:nz+2); gamma_boris: cell (initialised to 1 by init).
+ */
+int lare_gpu_upload_aux(lare_ctx* ctx, const double* eta, const double* visc3,
+                        const double* grav, const double* gamma_boris);
+
+/* Set the simulation clock (time, dt) as held in shared_data. */
+int lare_gpu_set_time(lare_ctx* ctx, double time, double dt);
+
+/*
+ * lagran.F90:50 lagrangian_step, including the energy/density/velocity bcs.
+ * step is the driver's step counter (shared_data `step`), which the
+ * predictor's half-step remap passes to eulerian_remap (lagran.F90:1057).
+ */
+int lare_gpu_lagrangian_step(lare_ctx* ctx, int step);
+
+/* remap.f90:33 eulerian_remap(step): Strang-permuted x/y/z remap + bfield_bcs. */
+int lare_gpu_eulerian_remap(lare_ctx* ctx, int step);
+
+/* lagran.F90:1176 eta_calc. */
+int lare_gpu_eta_calc(lare_ctx* ctx);
+
+/* boundary.f90:48 boundary_conditions (b, energy, density, velocity). */
+int lare_gpu_boundary_conditions(lare_ctx* ctx);
+
+/*
+ * One timestep of the driver loop (lare3d.f90:83-87): lagrangian_step,
+ * eulerian_remap(step), eta_calc.  time/dt (may be NULL) receive the
+ * updated clock.
+ */
+int lare_gpu_step(lare_ctx* ctx, int step, double* time, double* dt);
+
+/*
+ * Run the driver loop from step first_step+1 until nsteps steps were taken
+ * or time >= t_end (lare3d.f90:80-89).  steps_done/time/dt may be NULL.
+ */
+int lare_gpu_run(lare_ctx* ctx, int first_step, int nsteps, double t_end,
+                 int* steps_done, double* time, double* dt);
+
+/*
+ * conduct.f90:39 conduct_heat on the current state with the given dt
+ * (RKL2 super-time-stepping, stages from calc_s_stages).  Used to time the
+ * conduction operator alone; n_stages (may be NULL) receives s.
+ */
+int lare_gpu_conduct_heat(lare_ctx* ctx, double dt, int* n_stages);
+
+/*
+ * diagnostics.F90:517 energy_account: out[0..4] = en_b, en_ke, en_int,
+ * total_visc_heating, total_ohmic_heating (the en.dat record, :79-83), FP64.
+ */
+int lare_gpu_energy(lare_ctx* ctx, double out[5]);
+
+/* Download the state into host Fortran arrays (any pointer may be NULL). */
+int lare_gpu_download(lare_ctx* ctx, double* rho, double* energy,
+                      double* vx, double* vy, double* vz,
+                      double* bx, double* by, double* bz);
+
+/*
+ * Copy any named device array (the reference's variable names: "rho",
+ * "vx1", "p_visc", "visc_heat", "alpha1", "cv1", "temperature", ...) to or
+ * from a host buffer laid out with that array's Fortran bounds.  Used for
+ * restart, SDF dumps and per-routine parity checks.
+ */
+int lare_gpu_get_field(lare_ctx* ctx, const char* name, double* host);
+int lare_gpu_set_field(lare_ctx* ctx, const char* name, const double* host);
+
+/* Bounds of a named array: lo[3], hi[3] (Fortran, inclusive). */
+int lare_gpu_field_bounds(lare_ctx* ctx, const char* name, int lo[3], int hi[3]);
+
+int lare_gpu_get_scalars(lare_ctx* ctx, lare_scalars* out);
+
+/* Number of kernel launches issued by this context since init. */
+long long lare_gpu_launch_count(lare_ctx* ctx);
+
+/* The CUDA stream (cudaStream_t) the context launches on. */
+void* lare_gpu_stream(lare_ctx* ctx);
+
+const char* lare_gpu_last_error(lare_ctx* ctx);
+
+void lare_gpu_destroy(lare_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LARE_GPU_H */

@@ -1,0 +1,263 @@
+// common.cuh - device layout, launch helpers and deterministic reductions.
+//
+// Layout: every 3-D array lives in one common padded box covering Fortran
+// indices -2..n+2 in each dimension (the union of the cell, node and face
+// bounds of mpi_routines.F90:295-327), x fastest, row pitch sx >= nx+5
+// rounded up to 4 elements.  One index formula then serves every
+// staggering, and element (i,j,k) of any array is  p0[i + sx*j + sxy*k]
+// with p0 pointing at Fortran (0,0,0).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <climits>
+#include <cstdint>
+
+namespace lare {
+
+template <class R>
+struct A3 {
+  R* p;  // element (0,0,0)
+  int sx, sxy;
+  __device__ __forceinline__ R& operator()(int i, int j, int k) const { return p[i + sx * j + sxy * k]; }
+};
+
+template <class R>
+struct A1 {
+  const R* p;  // element 0 (Fortran lower bound may be -1 or -2)
+  __device__ __forceinline__ R operator()(int i) const { return p[i]; }
+};
+
+template <class R>
+struct Num;
+template <>
+struct Num<double> {
+  static __host__ __device__ constexpr double tiny() { return DBL_MIN; }  // TINY(1.0_num)
+  static __host__ __device__ constexpr double huge() { return DBL_MAX; }  // HUGE(1.0_num)
+};
+template <>
+struct Num<float> {
+  static __host__ __device__ constexpr float tiny() { return FLT_MIN; }
+  static __host__ __device__ constexpr float huge() { return FLT_MAX; }
+};
+
+// Scalar slots kept in device memory so that a whole step can run (and be
+// captured in a CUDA graph) without the host knowing dt.
+enum Slot {
+  SC_DT = 0,       // dt (shared_data)
+  SC_DT2,          // dt2 = dt/2 (lagran.F90:132), also the predictor remap dt
+  SC_DTR,          // dtr
+  SC_TIME,         // time
+  SC_DTSUB,        // resistive sub-cycle dt (lagran.F90:143)
+  SC_DTCOND,       // dt used by an isolated conduct_heat call
+  SC_VISC2N,       // visc2_norm (lagran.F90:545)
+  SC_VISC_TOT,     // total_visc_heating
+  SC_OHM_TOT,      // total_ohmic_heating
+  SC_SUBSTEPS,     // resistive sub-cycles (integer value)
+  SC_STAGES,       // RKL2 stages (integer value)
+  SC_DTPARAB,      // explicit conduction limit
+  SC_EN_B, SC_EN_KE, SC_EN_INT,
+  SC_NSLOTS = 16
+};
+// Integer min-reduction targets (bit patterns of positive doubles order
+// like unsigned integers).
+enum USlot { U_DTMIN = 0, U_DTRMIN, U_DTPARAB, U_NSLOTS = 4 };
+
+struct Box {
+  int lo[3], hi[3];
+};
+
+template <class Fn>
+__global__ void __launch_bounds__(256) k_box(int i0, int j0, int k0, int ni, int nj, Fn fn) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= ni || j >= nj) return;
+  fn(i0 + i, j0 + j, k0 + (int)blockIdx.z);
+}
+
+template <class Fn>
+inline void launch_box(cudaStream_t s, long long& count, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn) {
+  int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+  if (ni <= 0 || nj <= 0 || nk <= 0) return;
+  dim3 blk(64, 4, 1);
+  dim3 grd((ni + 63) / 64, (nj + 3) / 4, nk);
+  k_box<<<grd, blk, 0, s>>>(i0, j0, k0, ni, nj, fn);
+  ++count;
+}
+
+// Single-thread kernel for scalar bookkeeping on the device.
+template <class Fn>
+__global__ void k_scalar(Fn fn) {
+  fn();
+}
+template <class Fn>
+inline void launch_scalar(cudaStream_t s, long long& count, Fn fn) {
+  k_scalar<<<1, 1, 0, s>>>(fn);
+  ++count;
+}
+
+// ---------------------------------------------------------------------
+// Deterministic sums: each block reduces NV values per thread in a fixed
+// tree and writes its partials; one block then adds the partials in a
+// fixed order.  Results are run-to-run reproducible (not equal to a
+// serial left-to-right sum, which no parallel order can reproduce).
+template <int NV>
+__device__ __forceinline__ void block_sum_write(double (&v)[NV], double* partial, int bid) {
+  __shared__ double sh[NV][8];
+  for (int q = 0; q < NV; ++q) {
+    double x = v[q];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    v[q] = x;
+  }
+  int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+  int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+  if (lane == 0)
+    for (int q = 0; q < NV; ++q) sh[q][warp] = v[q];
+  __syncthreads();
+  if (warp == 0) {
+    int nw = (blockDim.x * blockDim.y) >> 5;
+    for (int q = 0; q < NV; ++q) {
+      double x = lane < nw ? sh[q][lane] : 0.0;
+      for (int o = 4; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) partial[(size_t)bid * NV + q] = x;
+    }
+  }
+}
+
+template <int NV, class Fn>
+__global__ void __launch_bounds__(256) k_box_sum(int i0, int j0, int k0, int ni, int nj, Fn fn, double* partial) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  double v[NV];
+  for (int q = 0; q < NV; ++q) v[q] = 0.0;
+  if (i < ni && j < nj) fn(i0 + i, j0 + j, k0 + (int)blockIdx.z, v);
+  int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  block_sum_write<NV>(v, partial, bid);
+}
+
+template <int NV>
+__global__ void __launch_bounds__(1024) k_sum_partials(const double* partial, int nb, double* out, int accumulate) {
+  __shared__ double sh[NV][32];
+  int t = threadIdx.x;
+  for (int q = 0; q < NV; ++q) {
+    double x = 0.0;
+    for (int b = t; b < nb; b += blockDim.x) x += partial[(size_t)b * NV + q];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((t & 31) == 0) sh[q][t >> 5] = x;
+  }
+  __syncthreads();
+  if (t < 32) {
+    for (int q = 0; q < NV; ++q) {
+      double x = sh[q][t];
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (t == 0) out[q] = accumulate ? out[q] + x : x;
+    }
+  }
+}
+
+// Min of positive doubles through their bit patterns.
+__device__ __forceinline__ void atomic_min_pos(unsigned long long* u, double v) {
+  atomicMin(u, (unsigned long long)__double_as_longlong(v));
+}
+
+template <int NV, class Fn>
+__global__ void __launch_bounds__(256) k_box_min(int i0, int j0, int k0, int ni, int nj, Fn fn, unsigned long long* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  double v[NV];
+  for (int q = 0; q < NV; ++q) v[q] = DBL_MAX;
+  if (i < ni && j < nj) fn(i0 + i, j0 + j, k0 + (int)blockIdx.z, v);
+  __shared__ double sh[NV][8];
+  for (int q = 0; q < NV; ++q) {
+    double x = v[q];
+    for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_down_sync(0xffffffffu, x, o));
+    v[q] = x;
+  }
+  int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  int lane = tid & 31, warp = tid >> 5;
+  if (lane == 0)
+    for (int q = 0; q < NV; ++q) sh[q][warp] = v[q];
+  __syncthreads();
+  if (warp == 0) {
+    int nw = (blockDim.x * blockDim.y) >> 5;
+    for (int q = 0; q < NV; ++q) {
+      double x = lane < nw ? sh[q][lane] : DBL_MAX;
+      for (int o = 4; o > 0; o >>= 1) x = fmin(x, __shfl_down_sync(0xffffffffu, x, o));
+      if (lane == 0) atomic_min_pos(out + q, x);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// Ghost fills.  Every fill of boundary.f90 / mpiboundary.f90 on one rank is
+// a sequence of whole-plane copies (periodic self-exchange, BC_USER mirror)
+// or zeroings, applied dimension after dimension over the full extent of
+// the other dimensions.  Such a sequence equals the composite map
+//   out(i,j,k) = in(m_x(i), m_y(j), m_z(k))  (or 0 if any m_d says zero)
+// applied to every point that some step writes, where m_d maps a written
+// index to its source and leaves others alone.  All sources lie in the
+// never-written range, so one kernel can apply the map in place.
+struct GDim {
+  int lo, hi;      // array extent in this dimension
+  int a, b;        // contiguous never-written range
+  int nw;          // number of written indices
+  int widx[6];     // written indices
+  int wsrc[6];     // source index, or INT_MIN for "set to zero"
+};
+struct GSpec {
+  GDim d[3];
+  long long c0, c1, c2;  // points in the three disjoint regions
+};
+
+__device__ __forceinline__ int gmap(const GDim& g, int i, bool& zero) {
+  for (int q = 0; q < g.nw; ++q)
+    if (g.widx[q] == i) {
+      if (g.wsrc[q] == INT_MIN) { zero = true; return i; }
+      return g.wsrc[q];
+    }
+  return i;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_ghost(GSpec s, R* p0, R* p1, R* p2, int sx, int sxy) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const GDim &X = s.d[0], &Y = s.d[1], &Z = s.d[2];
+  int i, j, k;
+  if (t < s.c0) {
+    int iw = (int)(t % X.nw);
+    long long r = t / X.nw;
+    int ey = Y.hi - Y.lo + 1;
+    i = X.widx[iw];
+    j = Y.lo + (int)(r % ey);
+    k = Z.lo + (int)(r / ey);
+  } else if (t < s.c0 + s.c1) {
+    t -= s.c0;
+    int ex = X.b - X.a + 1;
+    i = X.a + (int)(t % ex);
+    long long r = t / ex;
+    j = Y.widx[(int)(r % Y.nw)];
+    k = Z.lo + (int)(r / Y.nw);
+  } else if (t < s.c0 + s.c1 + s.c2) {
+    t -= s.c0 + s.c1;
+    int ex = X.b - X.a + 1, ey = Y.b - Y.a + 1;
+    i = X.a + (int)(t % ex);
+    long long r = t / ex;
+    j = Y.a + (int)(r % ey);
+    k = Z.widx[(int)(r / ey)];
+  } else {
+    return;
+  }
+  bool zero = false;
+  int si = gmap(X, i, zero), sj = gmap(Y, j, zero), sk = gmap(Z, k, zero);
+  long long dst = i + (long long)sx * j + (long long)sxy * k;
+  long long src = si + (long long)sx * sj + (long long)sxy * sk;
+  R* ps[3] = {p0, p1, p2};
+  for (int q = 0; q < 3; ++q) {
+    R* p = ps[q];
+    if (!p) continue;
+    p[dst] = zero ? R(0) : p[src];
+  }
+}
+
+}  // namespace lare

@@ -1,0 +1,179 @@
+// lare_gpu.cu - the extern "C" boundary declared in include/lare_gpu.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+
+#include "../../include/lare_gpu.h"
+#include "engine_base.h"
+
+struct lare_ctx {
+  lare::EngineBase* e = nullptr;
+  int precision = 64;
+  std::string err;
+};
+
+namespace {
+bool bc_supported(int c) { return c == LARE_BC_PERIODIC || c == LARE_BC_USER; }
+
+int guard(lare_ctx* c) { return (c && c->e) ? LARE_OK : LARE_EINVAL; }
+}  // namespace
+
+extern "C" {
+
+int lare_gpu_init(const lare_params* p, int nx, int ny, int nz, const double* dxb, const double* dxc,
+                  const double* dyb, const double* dyc, const double* dzb, const double* dzc, int precision,
+                  lare_ctx** out) {
+  if (!out) return LARE_EINVAL;
+  *out = nullptr;
+  if (!p || !dxb || !dxc || !dyb || !dyc || !dzb || !dzc) return LARE_EINVAL;
+  if (nx < 4 || ny < 4 || nz < 4) return LARE_EINVAL;
+  if (precision != 64 && precision != 32) return LARE_EINVAL;
+  const int bcs[6] = {p->xbc_min, p->xbc_max, p->ybc_min, p->ybc_max, p->zbc_min, p->zbc_max};
+  for (int q = 0; q < 6; ++q)
+    if (!bc_supported(bcs[q])) return LARE_EINVAL;  // BC_OPEN (openboundary.f90) is not on this path
+  if (!(p->gamma > 1.0) || !(p->dt_multiplier > 0.0)) return LARE_EINVAL;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return LARE_ECUDA;
+  const double* m6[6] = {dxb, dxc, dyb, dyc, dzb, dzc};
+  std::string err;
+  lare::EngineBase* e = precision == 64 ? lare::make_engine_f64(p, nx, ny, nz, m6, err)
+                                        : lare::make_engine_f32(p, nx, ny, nz, m6, err);
+  if (!e) return err.find("cudaMalloc") != std::string::npos ? LARE_ENOMEM : LARE_ECUDA;
+  lare_ctx* c = new lare_ctx();
+  c->e = e;
+  c->precision = precision;
+  *out = c;
+  return LARE_OK;
+}
+
+int lare_gpu_upload(lare_ctx* c, const double* rho, const double* energy, const double* vx, const double* vy,
+                    const double* vz, const double* bx, const double* by, const double* bz) {
+  if (guard(c)) return LARE_EINVAL;
+  const double* s8[8] = {rho, energy, vx, vy, vz, bx, by, bz};
+  return c->e->upload(s8);
+}
+
+int lare_gpu_upload_aux(lare_ctx* c, const double* eta, const double* visc3, const double* grav,
+                        const double* gamma_boris) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->upload_aux(eta, visc3, grav, gamma_boris);
+}
+
+int lare_gpu_set_time(lare_ctx* c, double time, double dt) {
+  if (guard(c)) return LARE_EINVAL;
+  if (!std::isfinite(time) || !std::isfinite(dt) || dt < 0.0) return LARE_EINVAL;
+  return c->e->set_time(time, dt);
+}
+
+int lare_gpu_lagrangian_step(lare_ctx* c, int step) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->lagrangian_step(step);
+}
+
+int lare_gpu_eulerian_remap(lare_ctx* c, int step) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->eulerian_remap(step);
+}
+
+int lare_gpu_eta_calc(lare_ctx* c) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->eta_calc();
+}
+
+int lare_gpu_boundary_conditions(lare_ctx* c) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->boundary_conditions();
+}
+
+int lare_gpu_step(lare_ctx* c, int step, double* time, double* dt) {
+  if (guard(c)) return LARE_EINVAL;
+  int rc = c->e->lagrangian_step(step);
+  if (rc) return rc;
+  if ((rc = c->e->eulerian_remap(step))) return rc;
+  if ((rc = c->e->eta_calc())) return rc;
+  if (time || dt) {
+    lare_scalars s;
+    if ((rc = c->e->scalars(&s))) return rc;
+    if (time) *time = s.time;
+    if (dt) *dt = s.dt;
+  }
+  return LARE_OK;
+}
+
+int lare_gpu_run(lare_ctx* c, int first_step, int nsteps, double t_end, int* steps_done, double* time, double* dt) {
+  if (guard(c)) return LARE_EINVAL;
+  lare_scalars s;
+  int rc = c->e->scalars(&s);
+  if (rc) return rc;
+  int step = first_step, done = 0;
+  // lare3d.f90:80-89
+  while (!((done >= nsteps && nsteps >= 0) || s.time >= t_end)) {
+    ++step;
+    if ((rc = c->e->lagrangian_step(step))) return rc;
+    if ((rc = c->e->eulerian_remap(step))) return rc;
+    if ((rc = c->e->eta_calc())) return rc;
+    ++done;
+    if ((rc = c->e->scalars(&s))) return rc;
+  }
+  if (steps_done) *steps_done = done;
+  if (time) *time = s.time;
+  if (dt) *dt = s.dt;
+  return LARE_OK;
+}
+
+int lare_gpu_conduct_heat(lare_ctx* c, double dt, int* n_stages) {
+  if (guard(c)) return LARE_EINVAL;
+  if (!(dt > 0.0) || !std::isfinite(dt)) return LARE_EINVAL;
+  return c->e->conduct_heat(dt, n_stages);
+}
+
+int lare_gpu_energy(lare_ctx* c, double out[5]) {
+  if (guard(c) || !out) return LARE_EINVAL;
+  return c->e->energy(out);
+}
+
+int lare_gpu_download(lare_ctx* c, double* rho, double* energy, double* vx, double* vy, double* vz, double* bx,
+                      double* by, double* bz) {
+  if (guard(c)) return LARE_EINVAL;
+  double* s8[8] = {rho, energy, vx, vy, vz, bx, by, bz};
+  return c->e->download(s8);
+}
+
+int lare_gpu_get_field(lare_ctx* c, const char* name, double* host) {
+  if (guard(c) || !name || !host) return LARE_EINVAL;
+  return c->e->get_field(name, host);
+}
+
+int lare_gpu_set_field(lare_ctx* c, const char* name, const double* host) {
+  if (guard(c) || !name || !host) return LARE_EINVAL;
+  return c->e->set_field(name, host);
+}
+
+int lare_gpu_field_bounds(lare_ctx* c, const char* name, int lo[3], int hi[3]) {
+  if (guard(c) || !name || !lo || !hi) return LARE_EINVAL;
+  return c->e->field_bounds(name, lo, hi);
+}
+
+int lare_gpu_get_scalars(lare_ctx* c, lare_scalars* out) {
+  if (guard(c) || !out) return LARE_EINVAL;
+  return c->e->scalars(out);
+}
+
+long long lare_gpu_launch_count(lare_ctx* c) { return (c && c->e) ? c->e->launches() : -1; }
+
+void* lare_gpu_stream(lare_ctx* c) { return (c && c->e) ? c->e->stream() : nullptr; }
+
+const char* lare_gpu_last_error(lare_ctx* c) {
+  if (!c) return "null context";
+  if (!c->e) return c->err.c_str();
+  return c->e->error();
+}
+
+void lare_gpu_destroy(lare_ctx* c) {
+  if (!c) return;
+  delete c->e;
+  delete c;
+}
+
+}  // extern "C"

@@ -1,0 +1,242 @@
+"""Synthetic initial states (the user-deck layer, cf. src/initial_conditions.f90
+and src/control.f90) for the three plain-method workloads:
+
+* ``blast``          3-D MHD blast, 64^3 periodic unit cube, 100 steps at CFL 0.8
+* ``orszag_tang``    resistive 3-D Orszag-Tang-type vortex, 256^3 periodic
+                     [0, 2pi]^3, eta = 1e-3, 200 steps
+* ``conduction``     sheared arcade B = curl(A_y e_y), A_y = cos(kx) exp(-kz),
+                     isobaric Gaussian hot spots, kappa_par ~ T^{5/2}, RKL2
+
+Each returns a :class:`Deck` with control parameters, grid metrics and the
+Fortran-bounded state; ghost cells are filled by the caller's
+boundary_conditions (lare3d.f90:65).  Random perturbations come from the
+reference's KISS generator (random_generator.f90) seeded with
+random_init_local(seed).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from .abi import BC_PERIODIC, BC_USER, LareParams, State, default_params
+from .grid import grid
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_host_lib = None
+
+
+def host_lib():
+    global _host_lib
+    if _host_lib is None:
+        path = os.path.join(_HERE, "liblare_host.so")
+        if not os.path.exists(path):
+            raise RuntimeError("liblare_host.so is not built; run __graft_entry__.build()")
+        lib = C.CDLL(path)
+        lib.lare_kiss_fill.argtypes = [C.c_int, C.c_long, C.POINTER(C.c_double)]
+        lib.lare_kiss_fill.restype = None
+        _host_lib = lib
+    return _host_lib
+
+
+def kiss_uniform(seed: int, n: int) -> np.ndarray:
+    """n KISS draws in [0,1) after random_init_local(seed)."""
+    out = np.empty(n, dtype=np.float64)
+    host_lib().lare_kiss_fill(int(seed), int(n), out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+@dataclass
+class Deck:
+    name: str
+    params: LareParams
+    nx: int
+    ny: int
+    nz: int
+    metrics: dict
+    state: State
+    nsteps: int
+    grav: Optional[np.ndarray] = None
+    dt_fixed: Optional[float] = None   # conduction operator timing only
+    info: dict = field(default_factory=dict)
+
+
+def _coords(m, nx, ny, nz):
+    """Broadcastable coordinate arrays for cells (-1:n+2) and nodes (-2:n+2)."""
+    xc = m["xc"][:, None, None]
+    yc = m["yc"][None, :, None]
+    zc = m["zc"][None, None, :]
+    xb = m["xb"][:, None, None]
+    yb = m["yb"][None, :, None]
+    zb = m["zb"][None, None, :]
+    return xc, yc, zc, xb, yb, zb
+
+
+def blast(n: int = 64, **over) -> Deck:
+    g = 5.0 / 3.0
+    p = default_params(gamma=g, visc1=0.1, visc2=0.5, dt_multiplier=0.8)
+    for k, v in over.items():
+        setattr(p, k, v)
+    m = grid(n, n, n, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0))
+    st = State.zeros(n, n, n)
+    xc, yc, zc, *_ = _coords(m, n, n, n)
+    r = np.sqrt((xc - 0.5) ** 2 + (yc - 0.5) ** 2 + (zc - 0.5) ** 2)
+    pres = np.where(r < 0.1, 10.0, 0.1)
+    st["rho"][...] = 1.0
+    st["energy"][...] = np.asfortranarray(pres / ((g - 1.0) * 1.0))
+    b0 = 1.0 / math.sqrt(2.0)
+    st["bx"][...] = b0
+    st["by"][...] = b0
+    st["bz"][...] = 0.0
+    return Deck("blast", p, n, n, n, m, st, nsteps=100)
+
+
+def _curl_edges(Ax, Ay, Az, m, n):
+    """Discrete curl of periodic edge fields onto the face arrays.
+
+    Ax[i,j,k]: x-cell i, y-node j, z-node k; Ay: x-node, y-cell, z-node;
+    Az: x-node, y-node, z-cell.  A lattice index is the Fortran cell or node
+    index modulo n.  Each face takes the circulation of its four bounding
+    edges divided by its actual widths, over the face array's full Fortran
+    extent (ghosts are refreshed by bfield_bcs afterwards).
+    """
+    def w(lo, hi):
+        return np.arange(lo, hi + 1) % n
+
+    def width(arr, lo, hi):          # metric stored from Fortran index -1
+        return arr[np.arange(lo, hi + 1) + 1]
+
+    dxb, dyb, dzb = m["dxb"], m["dyb"], m["dzb"]
+    # bx(-2:n+2, -1:n+2, -1:n+2)
+    i, j, k = w(-2, n + 2), w(-1, n + 2), w(-1, n + 2)
+    jm, km = w(-2, n + 1), w(-2, n + 1)
+    bx = ((Az[np.ix_(i, j, k)] - Az[np.ix_(i, jm, k)]) / width(dyb, -1, n + 2)[None, :, None]
+          - (Ay[np.ix_(i, j, k)] - Ay[np.ix_(i, j, km)]) / width(dzb, -1, n + 2)[None, None, :])
+    # by(-1:n+2, -2:n+2, -1:n+2)
+    i, j, k = w(-1, n + 2), w(-2, n + 2), w(-1, n + 2)
+    im, km = w(-2, n + 1), w(-2, n + 1)
+    by = ((Ax[np.ix_(i, j, k)] - Ax[np.ix_(i, j, km)]) / width(dzb, -1, n + 2)[None, None, :]
+          - (Az[np.ix_(i, j, k)] - Az[np.ix_(im, j, k)]) / width(dxb, -1, n + 2)[:, None, None])
+    # bz(-1:n+2, -1:n+2, -2:n+2)
+    i, j, k = w(-1, n + 2), w(-1, n + 2), w(-2, n + 2)
+    im, jm = w(-2, n + 1), w(-2, n + 1)
+    bz = ((Ay[np.ix_(i, j, k)] - Ay[np.ix_(im, j, k)]) / width(dxb, -1, n + 2)[:, None, None]
+          - (Ax[np.ix_(i, j, k)] - Ax[np.ix_(i, jm, k)]) / width(dyb, -1, n + 2)[None, :, None])
+    return np.asfortranarray(bx), np.asfortranarray(by), np.asfortranarray(bz)
+
+
+def orszag_tang(n: int = 256, seed: int = 7, amp: float = 1.0e-3, **over) -> Deck:
+    g = 5.0 / 3.0
+    p = default_params(gamma=g, visc1=0.1, visc2=0.5, dt_multiplier=0.8,
+                       resistive_mhd=1, eta_background=1.0e-3, eta0=0.0, j_max=1.0e10)
+    for k, v in over.items():
+        setattr(p, k, v)
+    L = 2.0 * math.pi
+    m = grid(n, n, n, (0.0, L), (0.0, L), (0.0, L))
+    st = State.zeros(n, n, n)
+    xc, yc, zc, xb, yb, zb = _coords(m, n, n, n)
+    rho0 = 25.0 / (36.0 * math.pi)
+    p0 = 5.0 / (12.0 * math.pi)
+    st["rho"][...] = rho0
+    st["energy"][...] = p0 / ((g - 1.0) * rho0)
+    ones_n = np.ones((n + 5, n + 5, n + 5))
+    st["vx"][...] = np.asfortranarray(-np.sin(zb) * ones_n)
+    st["vy"][...] = np.asfortranarray(np.sin(xb) * ones_n)
+    st["vz"][...] = np.asfortranarray(np.sin(yb) * ones_n)
+    s4 = 1.0 / math.sqrt(4.0 * math.pi)
+    bx = st["bx"]
+    by = st["by"]
+    bz = st["bz"]
+    bx[...] = (-np.sin(m["zc"]) * s4)[None, None, :]
+    by[...] = (np.sin(2.0 * m["xc"]) * s4)[:, None, None]
+    bz[...] = (np.sin(m["yc"]) * s4)[None, :, None]
+    if amp != 0.0:
+        r = kiss_uniform(seed, 3 * n ** 3)
+        A = [(2.0 * r[q * n ** 3:(q + 1) * n ** 3] - 1.0).reshape((n, n, n), order="F") * amp for q in range(3)]
+        dbx, dby, dbz = _curl_edges(A[0], A[1], A[2], m, n)
+        bx += dbx
+        by += dby
+        bz += dbz
+    return Deck("orszag_tang", p, n, n, n, m, st, nsteps=200, info={"seed": seed, "amp": amp})
+
+
+def conduction(n: int = 256, seed: int = 11, nspots: int = 8, T0: float = 1.0,
+               kappa_0: float = 1.0e-3, dt_ratio: float = 50.0, **over) -> Deck:
+    """Sheared-arcade conduction workload: x, y periodic; z BC_USER."""
+    g = 5.0 / 3.0
+    p = default_params(gamma=g, conduction=1, heat_flux_limiter=1, flux_limiter=0.1,
+                       kappa_0=kappa_0, dt_multiplier=0.9,
+                       zbc_min=BC_USER, zbc_max=BC_USER)
+    for k, v in over.items():
+        setattr(p, k, v)
+    m = grid(n, n, n, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0), bcs=(BC_PERIODIC, BC_PERIODIC, BC_USER))
+    st = State.zeros(n, n, n)
+    xc, yc, zc, xb, yb, zb = _coords(m, n, n, n)
+    k = 2.0 * math.pi / 1.0
+    # A_y on y-edges (xb_i, yc_j, zb_k); B = curl(A_y e_y):
+    # bx = -dA_y/dz on x-faces, bz = dA_y/dx on z-faces (by = 0).
+    Ay = np.cos(k * m["xb"])[:, None] * np.exp(-k * m["zb"])[None, :]   # (x node -2:n+2, z node -2:n+2)
+    dzb = m["dzb"]
+    dxb = m["dxb"]
+    # bx(i, j, kc) for kc in -1:n+2 uses Ay(i, kc) - Ay(i, kc-1)
+    bxz = -(Ay[:, 1:] - Ay[:, :-1]) / dzb[None, :]            # (-2:n+2, -1:n+2)
+    st["bx"][...] = bxz[:, None, :]
+    bzx = (Ay[1:, :] - Ay[:-1, :]) / dxb[:, None]             # (-1:n+2, -2:n+2)
+    st["bz"][...] = bzx[:, None, :]
+    st["by"][...] = 0.0
+    # Temperature: T0 + sum of Gaussian hot spots (amplitude 10*T0, sigma = 8 cells)
+    sig = 8.0 / n
+    r = kiss_uniform(seed, 3 * nspots)
+    T = np.full((n + 4, n + 4, n + 4), T0)
+    for s in range(nspots):
+        cx, cy, cz = r[3 * s], r[3 * s + 1], 0.2 + 0.6 * r[3 * s + 2]
+        dx = np.abs(xc - cx)
+        dx = np.minimum(dx, 1.0 - dx)
+        dy = np.abs(yc - cy)
+        dy = np.minimum(dy, 1.0 - dy)
+        dz = zc - cz
+        T = T + 10.0 * T0 * np.exp(-(dx * dx + dy * dy + dz * dz) / (2.0 * sig * sig))
+    pres0 = 1.0
+    xi = p.xi_n
+    st["rho"][...] = np.asfortranarray(pres0 / T)
+    st["energy"][...] = np.asfortranarray(T * (2.0 - xi) / (g - 1.0))
+    # dt from the explicit limit of calc_s_stages (conduct.f90:80-129).
+    dtp = dt_parab_estimate(st, m, p, n)
+    d = Deck("conduction", p, n, n, n, m, st, nsteps=10, dt_fixed=dt_ratio * dtp,
+             info={"seed": seed, "nspots": nspots, "dt_parab": dtp, "dt_ratio": dt_ratio})
+    return d
+
+
+def dt_parab_estimate(st: State, m: dict, p: LareParams, n: int) -> float:
+    """numpy restatement of conduct.f90:64-129 (temperature, Larsen factor,
+    explicit conduction limit), used only to pick a workload dt."""
+    g = p.gamma
+    xi = p.xi_n
+    e = st["energy"]
+    T = (g - 1.0) / (2.0 - xi) * (e - (1.0 - xi) * p.ionise_pot)      # (-1:n+2)^3
+    Ti = T[1:n + 2, 1:n + 2, 1:n + 2]                                   # 0:n
+    dxb = m["dxb"][1:n + 2][:, None, None]
+    dyb = m["dyb"][1:n + 2][None, :, None]
+    dzb = m["dzb"][1:n + 2][None, None, :]
+    rho = st["rho"][1:n + 2, 1:n + 2, 1:n + 2]
+    temp = Ti ** 2.5
+    q_fs = p.flux_limiter * 42.85 * rho * Ti ** 1.5
+    qx = -p.kappa_0 * temp * (T[2:n + 3, 1:n + 2, 1:n + 2] - T[0:n + 1, 1:n + 2, 1:n + 2]) * 0.5 / dxb
+    qy = -p.kappa_0 * temp * (T[1:n + 2, 2:n + 3, 1:n + 2] - T[1:n + 2, 0:n + 1, 1:n + 2]) * 0.5 / dyb
+    qz = -p.kappa_0 * temp * (T[1:n + 2, 1:n + 2, 2:n + 3] - T[1:n + 2, 1:n + 2, 0:n + 1]) * 0.5 / dzb
+    lf = q_fs / np.sqrt(q_fs * q_fs + qx * qx + qy * qy + qz * qz)
+    if not p.heat_flux_limiter:
+        lf = np.ones_like(lf)
+    lf = lf[1:, 1:, 1:]
+    t = temp[1:, 1:, 1:]
+    r = rho[1:, 1:, 1:]
+    h2 = np.minimum(np.minimum(dxb[1:] ** 2, dyb[:, 1:] ** 2), dzb[:, :, 1:] ** 2)
+    dtp = np.min(r * h2 / (2.0 * p.kappa_0 * lf * t))
+    return float(p.dt_multiplier * dtp / math.sqrt(3.0))
+
+
+DECKS = {"blast": blast, "orszag_tang": orszag_tang, "conduction": conduction}
