@@ -1,0 +1,333 @@
+"""Throughput benchmark of the Lagrangian-remap timestep (one JSON line).
+
+Workload (N = 1): the resistive 3-D Orszag-Tang vortex on a 256^3 periodic
+[0, 2pi]^3 box, FP64 drop-in, one step = lagrangian_step + eulerian_remap +
+eta_calc (lare3d.f90:84-87).  Metric: cell-updates/s = nx*ny*nz*steps / time.
+Synthetic state generated on the host (no datasets exist for this code).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+* ``value``: device-resident throughput, CUDA events on the engine's stream
+  around K steps, max over ranks; 8 state arrays of 141 MB each exceed L2.
+* ``e2e``: the same metric through the C ABI with Fortran-layout host
+  buffers in pinned memory: every step uploads the state, steps, downloads.
+* ``roofline``: the dominant kernel of one profiled step; achieved =
+  algorithmic bytes / event-timed duration; peak = measured HBM copy rate.
+* ``cpu_baseline``: the oracle on the host cores, one step of the workload.
+* N > 1: independent replicas (the single-GPU path has no exchange step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def max_over_ranks(v, ws):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(deck, steps=1):
+    """The oracle on the host cores: one warm-up step and `steps` timed."""
+    from oracle import oracle
+    sim = oracle.simulation(deck)
+    sim.start(deck.state)
+    sim.step(1)
+    t = time.perf_counter()
+    for s in range(2, 2 + steps):
+        sim.step(s)
+    el = (time.perf_counter() - t) / steps
+    sim.close()
+    n3 = deck.nx * deck.ny * deck.nz
+    return {"value": n3 / el, "unit": "cell-updates/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{steps} step(s) of the {deck.nx}^3 workload after 1 warm-up step, {el:.2f} s/step"}
+
+
+def time_steps(sim, torch, stream, first, k):
+    """CUDA events around k device-resident steps on the engine's stream."""
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+    sim.run(first, k)
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1000.0
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    from lare3d_b200 import decks
+    deck = decks.orszag_tang(args.n)
+    from oracle import oracle
+    sim = oracle.simulation(deck)
+    sim.start(deck.state)
+    step = 0
+    for _ in range(args.warmup):
+        step += 1
+        sim.step(step)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        step += 1
+        sim.step(step)
+    el = time.perf_counter() - t
+    n3 = deck.nx * deck.ny * deck.nz
+    v = n3 * args.steps / el
+    out = {
+        "impl": "reference", "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded KISS perturbation of the Orszag-Tang state)",
+        "config": {"workload": f"resistive Orszag-Tang {args.n}^3 periodic, FP64, eta=1e-3, CFL 0.8",
+                   "grid": [args.n] * 3, "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": oracle.num_threads(), "kind": "port",
+                         "sample": f"{args.steps} steps after {args.warmup} warm-up steps (Fortran reference not buildable: no Fortran compiler)"},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    ws, rank, local = dist_setup(args)
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from lare3d_b200 import decks, gpu
+    from lare3d_b200.abi import State
+
+    n = args.n
+    deck = decks.orszag_tang(n)
+    sim = gpu.simulation(deck, precision=64)
+    sim.start(deck.state)
+    stream = torch.cuda.ExternalStream(gpu.stream_of(sim))
+    step = 0
+    sim.run(step, args.warmup)
+    step += args.warmup
+
+    # ---- device-resident timed region
+    clocks = Clocks(local)
+    barrier(ws)
+    clocks.start()
+    l0 = sim.launch_count()
+    el = time_steps(sim, torch, stream, step, args.steps)
+    launches = sim.launch_count() - l0
+    step += args.steps
+    ck = clocks.stop()
+    el_max = max_over_ranks(el, ws)
+    n3 = n ** 3
+    value = ws * n3 * args.steps / el_max
+
+    # ---- roofline of the dominant kernel (one profiled step)
+    sim.profile(True)
+    sim.run(step, 1)
+    step += 1
+    sim.profile(False)
+    prof = sim.profile_report()
+    total_ms = sum(p["ms"] for p in prof)
+    top = max((p for p in prof if p["words"] > 0), key=lambda p: p["ms"])
+    hbm, peak_kind = peaks()
+    per_launch_bytes = top["bytes"] / top["launches"]
+    per_launch_s = top["ms"] / top["launches"] / 1e3
+    achieved = per_launch_bytes / per_launch_s / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(top["site"])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": traffic, "kernel": top["site"], "share": top["ms"] / total_ms,
+                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": per_launch_bytes}
+
+    # ---- end to end through the C ABI with pinned host buffers
+    host = {}
+    for k, a in deck.state.arrays.items():
+        t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+        h = t.numpy().reshape(a.shape, order="F")
+        h[...] = a
+        host[k] = (t, h)
+    st = State(n, n, n, {k: v[1] for k, v in host.items()})
+    bi = sum(v[1].nbytes for v in host.values())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    sim.upload(st)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        step += 1
+        sim.upload(st)
+        sim.step(step)
+        sim.download(st)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_el = max_over_ranks(e0.elapsed_time(e1) / 1000.0, ws)
+    e2e = {"value": ws * n3 * args.e2e_steps / e2e_el, "unit": "cell-updates/s",
+           "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bi, "steps": args.e2e_steps}
+
+    # ---- the other forms (FP32, RKL2 conduction), rank 0 only
+    forms = {}
+    if rank == 0 and not args.no_forms:
+        s32 = gpu.simulation(deck, precision=32)
+        s32.start(deck.state)
+        s32.run(0, 2)
+        st32 = torch.cuda.ExternalStream(gpu.stream_of(s32))
+        el32 = time_steps(s32, torch, st32, 2, args.steps)
+        forms["fp32"] = {"value": n3 * args.steps / el32, "unit": "cell-updates/s",
+                         "ms_per_step": 1e3 * el32 / args.steps, "speedup_vs_fp64": (n3 * args.steps / el32) / value}
+        s32.close()
+        cdeck = decks.conduction(n)
+        for prec in (64, 32):
+            sc = gpu.simulation(cdeck, precision=prec)
+            sc.start(cdeck.state)
+            sc.conduct_heat(cdeck.dt_fixed)
+            stc = torch.cuda.ExternalStream(gpu.stream_of(sc))
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a0.record(stc)
+            reps = 3
+            for _ in range(reps):
+                ns = sc.conduct_heat(cdeck.dt_fixed)
+            a1.record(stc)
+            a1.synchronize()
+            elc = a0.elapsed_time(a1) / 1000.0 / reps
+            forms[f"conduction_rkl2_fp{prec}"] = {"value": n3 / elc, "unit": "cell-updates/s (one conduct_heat substep)",
+                                                  "ms_per_substep": 1e3 * elc, "stages": ns,
+                                                  "dt_over_dt_parab": cdeck.info["dt_ratio"]}
+            sc.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(deck, steps=1)
+
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded KISS perturbation of the Orszag-Tang state)",
+            "config": {"workload": f"resistive Orszag-Tang {n}^3 periodic, FP64 drop-in, eta=1e-3, CFL 0.8",
+                       "grid": [n, n, n], "l2": "inputs larger than L2 (8 state arrays x 141 MB)",
+                       "parallelism": f"replicas x{ws}"},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches,
+            "clocks": ck, "forms": forms,
+            "top_kernels": [{k: p[k] for k in ("site", "launches", "ms", "words")} for p in prof[:8]],
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

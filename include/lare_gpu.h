@@ -180,6 +180,17 @@ int lare_gpu_field_bounds(lare_ctx* ctx, const char* name, int lo[3], int hi[3])
 
 int lare_gpu_get_scalars(lare_ctx* ctx, lare_scalars* out);
 
+/*
+ * Instrumentation (not part of the reference interface).  profile(1)
+ * resets and starts per-launch-site timing with CUDA events on the
+ * context's stream; profile(0) stops it.  profile_report writes one line per
+ * launch site, "site<TAB>launches<TAB>total ms<TAB>algorithmic bytes<TAB>
+ * words per point", sorted by time, and returns the length it needs
+ * (including the terminating NUL).
+ */
+int lare_gpu_profile(lare_ctx* ctx, int enable);
+int lare_gpu_profile_report(lare_ctx* ctx, char* buf, int len);
+
 /* Number of kernel launches issued by this context since init. */
 long long lare_gpu_launch_count(lare_ctx* ctx);
 

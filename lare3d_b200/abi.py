@@ -220,6 +220,11 @@ class Binding:
             lc = getattr(lib, prefix + "launch_count")
             lc.argtypes = [C.c_void_p]
             lc.restype = C.c_longlong
+        if hasattr(lib, prefix + "profile"):
+            f("profile", [C.c_void_p, C.c_int])
+            pr = getattr(lib, prefix + "profile_report")
+            pr.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
+            pr.restype = C.c_int
 
     def _fn(self, name, argtypes, optional_precision=False):
         fn = getattr(self.lib, self.prefix + name)
@@ -269,8 +274,8 @@ class Simulation:
         g = None if grav is None else np.ascontiguousarray(grav, dtype=np.float64)
         self.b.call(self.ctx, "upload_aux", _ptr(eta), _ptr(visc3), None if g is None else g.ctypes.data_as(C.POINTER(C.c_double)), _ptr(gamma_boris))
 
-    def download(self) -> State:
-        st = State.zeros(self.nx, self.ny, self.nz)
+    def download(self, out: Optional[State] = None) -> State:
+        st = out if out is not None else State.zeros(self.nx, self.ny, self.nz)
         a = st.arrays
         self.b.call(self.ctx, "download", *[_ptr(a[k]) for k in ("rho", "energy", "vx", "vy", "vz", "bx", "by", "bz")])
         return st
@@ -333,6 +338,21 @@ class Simulation:
         s = LareScalars()
         self.b.call(self.ctx, "get_scalars", C.byref(s))
         return s
+
+    def profile(self, enable: bool):
+        self.b.call(self.ctx, "profile", 1 if enable else 0)
+
+    def profile_report(self):
+        """Per-launch-site timing: list of dicts sorted by total time."""
+        fn = getattr(self.b.lib, self.b.prefix + "profile_report")
+        need = fn(self.ctx, None, 0)
+        buf = C.create_string_buffer(max(need, 1))
+        fn(self.ctx, buf, len(buf))
+        out = []
+        for line in buf.value.decode().splitlines():
+            site, cnt, ms, by, words = line.split("\t")
+            out.append({"site": site, "launches": int(cnt), "ms": float(ms), "bytes": float(by), "words": int(words)})
+        return out
 
     def launch_count(self) -> int:
         return int(getattr(self.b.lib, self.b.prefix + "launch_count")(self.ctx))

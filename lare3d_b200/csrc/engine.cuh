@@ -17,7 +17,9 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/lare_gpu.h"
@@ -51,6 +53,26 @@ struct Arrays {
 
 enum Stag { ST_C = 0, ST_N = 1, ST_F = 2 };
 
+// Per-launch-site timing (instrumentation, off by default).  A site is a
+// launch statement (function, line); `words` is the number of distinct 3-D
+// arrays it reads plus writes, so bytes = words * points * sizeof(R).
+struct ProfSite {
+  const char* func;
+  int line;
+  int words;
+  long long count = 0;
+  double ms = 0.0, bytes = 0.0;
+};
+struct Prof {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;
+  size_t used = 0;
+  std::vector<int> ev_site;          // per event pair
+  std::vector<double> ev_bytes;
+  std::map<std::pair<const char*, int>, int> index;
+  std::vector<ProfSite> sites;
+};
+
 template <class R>
 struct Run {
   Par p;
@@ -72,20 +94,86 @@ struct Run {
   int cur_step = 0;
   int peak_substeps = 0, last_substeps = 0, steps_taken = 0, n_s_stages = 0;
   GSpec g_cell, g_node, g_bx, g_by, g_bz, g_cell_mpi, g_cell_user, g_dm[3];
+  Prof prof;
   std::string err;
+
+  // Bracket one launch with events when profiling.
+  int prof_begin(const char* func, int line, int words, double points) {
+    if (!prof.on) return -1;
+    auto key = std::make_pair(func, line);
+    auto it = prof.index.find(key);
+    int site;
+    if (it == prof.index.end()) {
+      site = (int)prof.sites.size();
+      prof.index[key] = site;
+      ProfSite ps;
+      ps.func = func;
+      ps.line = line;
+      ps.words = words;
+      prof.sites.push_back(ps);
+    } else {
+      site = it->second;
+    }
+    size_t k = prof.used;
+    while (prof.ev.size() < 2 * (k + 1)) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      prof.ev.push_back(e);
+    }
+    prof.ev_site.resize(k + 1);
+    prof.ev_bytes.resize(k + 1);
+    prof.ev_site[k] = site;
+    prof.ev_bytes[k] = (double)words * points * (double)sizeof(R);
+    cudaEventRecord(prof.ev[2 * k], s);
+    return (int)k;
+  }
+  void prof_end(int k) {
+    if (k < 0) return;
+    cudaEventRecord(prof.ev[2 * k + 1], s);
+    prof.used = k + 1;
+  }
+  // Fold recorded events into the per-site totals.
+  void prof_collect() {
+    cudaStreamSynchronize(s);
+    for (size_t k = 0; k < prof.used; ++k) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, prof.ev[2 * k], prof.ev[2 * k + 1]);
+      ProfSite& ps = prof.sites[prof.ev_site[k]];
+      ps.ms += ms;
+      ps.count += 1;
+      ps.bytes += prof.ev_bytes[k];
+    }
+    prof.used = 0;
+  }
 };
 
 // ---------------------------------------------------------------------
 // Launch shorthands
+template <class R, class Fn>
+inline void rbox(Run<R>& run, const char* func, int line, int words, int i0, int i1, int j0, int j1, int k0, int k1,
+                 Fn fn) {
+  double pts = (double)(i1 - i0 + 1) * (double)(j1 - j0 + 1) * (double)(k1 - k0 + 1);
+  int k = run.prof_begin(func, line, words, pts);
+  launch_box(run.s, run.launches, i0, i1, j0, j1, k0, k1, fn);
+  run.prof_end(k);
+}
+// LARE_BOX: one kernel over an inclusive Fortran index box.  LARE_BOXW also
+// states the kernel's algorithmic word count per point (arrays read +
+// written), used for the roofline of profiled launches.
 #define LARE_BOX(run, i0, i1, j0, j1, k0, k1, ...) \
-  launch_box((run).s, (run).launches, (i0), (i1), (j0), (j1), (k0), (k1), __VA_ARGS__)
+  rbox((run), __func__, __LINE__, 0, (i0), (i1), (j0), (j1), (k0), (k1), __VA_ARGS__)
+#define LARE_BOXW(run, words, i0, i1, j0, j1, k0, k1, ...) \
+  rbox((run), __func__, __LINE__, (words), (i0), (i1), (j0), (j1), (k0), (k1), __VA_ARGS__)
 
 template <class R>
 inline void ghost(Run<R>& run, const GSpec& g, A3<R> a, A3<R>* b = nullptr, A3<R>* c = nullptr) {
   long long tot = g.c0 + g.c1 + g.c2;
   if (tot <= 0) return;
   int blocks = (int)((tot + 255) / 256);
+  int narr = 1 + (b ? 1 : 0) + (c ? 1 : 0);
+  int k = run.prof_begin("ghost", 0, 2 * narr, (double)tot);
   k_ghost<R><<<blocks, 256, 0, run.s>>>(g, a.p, b ? b->p : nullptr, c ? c->p : nullptr, run.sx, run.sxy);
+  run.prof_end(k);
   ++run.launches;
 }
 
@@ -96,8 +184,10 @@ inline void box_sum(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1,
   dim3 blk(64, 4, 1);
   dim3 grd((ni + 63) / 64, (nj + 3) / 4, nk);
   int nb = grd.x * grd.y * grd.z;
+  int k = run.prof_begin("box_sum", 0, 0, (double)ni * nj * nk);
   k_box_sum<NV><<<grd, blk, 0, run.s>>>(i0, j0, k0, ni, nj, fn, run.partial);
   k_sum_partials<NV><<<1, 1024, 0, run.s>>>(run.partial, nb, run.sc + slot, acc ? 1 : 0);
+  run.prof_end(k);
   run.launches += 2;
 }
 
@@ -106,7 +196,9 @@ inline void box_min(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1,
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   dim3 blk(64, 4, 1);
   dim3 grd((ni + 63) / 64, (nj + 3) / 4, nk);
+  int k = run.prof_begin("box_min", 0, 0, (double)ni * nj * nk);
   k_box_min<NV><<<grd, blk, 0, run.s>>>(i0, j0, k0, ni, nj, fn, run.us + uslot);
+  run.prof_end(k);
   ++run.launches;
 }
 
@@ -152,7 +244,7 @@ void eta_calc(Run<R>& run) {
   auto bx = run.a.bx, by = run.a.by, bz = run.a.bz;
   auto dxc = run.a.dxc, dyc = run.a.dyc, dzc = run.a.dzc;
   const R jmax = (R)run.p.j_max, eb = (R)run.p.eta_background, e0 = (R)run.p.eta0;
-  LARE_BOX(run, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 4, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
     int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
     R jx = (bz(ix, iyp, iz) - bz(ix, iy, iz)) / dyc(iy) - (by(ix, iy, izp) - by(ix, iy, iz)) / dzc(iz);
     R jxp = (bz(ixp, iyp, iz) - bz(ixp, iy, iz)) / dyc(iy) - (by(ixp, iy, izp) - by(ixp, iy, iz)) / dzc(iz);
@@ -177,7 +269,7 @@ void viscous_damping(Run<R>& run) {
   auto qx = run.a.qx, qy = run.a.qy, qz = run.a.qz;
   auto dxb = run.a.dxb, dyb = run.a.dyb, dzb = run.a.dzb, dxc = run.a.dxc, dyc = run.a.dyc, dzc = run.a.dzc;
   const double* sc = run.sc;
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 7, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     int ixp = ix + 1, ixm = ix - 1, iyp = iy + 1, iym = iy - 1, izp = iz + 1, izm = iz - 1;
     A3<R> vv[3] = {vx, vy, vz};
     A3<R> qq[3] = {qx, qy, qz};
@@ -189,7 +281,7 @@ void viscous_damping(Run<R>& run) {
            ((v(ix, iy, izp) - v(ix, iy, iz)) / dzb(izp) - (v(ix, iy, iz) - v(ix, iy, izm)) / dzb(iz)) / dzc(iz));
     }
   });
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 9, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DT];
     vx(ix, iy, iz) = vx(ix, iy, iz) + dt * qx(ix, iy, iz);
     vy(ix, iy, iz) = vy(ix, iy, iz) + dt * qy(ix, iy, iz);
@@ -242,19 +334,19 @@ void shock_viscosity(Run<R>& run) {
   whole(run, [=] __device__(int i, int j, int k) {
     if (i < 0 || i > nx + 1 || j < 0 || j > ny + 1 || k < 0 || k > nz + 1) p_visc(i, j, k) = R(0);
   });
-  LARE_BOX(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 7, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     R rmin = fmax(rho(ix, iy, iz), Num<R>::tiny());
     R b2 = bx1(ix, iy, iz) * bx1(ix, iy, iz) + by1(ix, iy, iz) * by1(ix, iy, iz) + bz1(ix, iy, iz) * bz1(ix, iy, iz);
     cs(ix, iy, iz) = sqrt((g * pressure(ix, iy, iz) + gamma_boris(ix, iy, iz) * b2) / rmin);
   });
-  LARE_BOX(run, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 4, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
     int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
     R s = cs(ix, iy, iz) * cv(ix, iy, iz) + cs(ixp, iy, iz) * cv(ixp, iy, iz) + cs(ix, iyp, iz) * cv(ix, iyp, iz) +
           cs(ixp, iyp, iz) * cv(ixp, iyp, iz) + cs(ix, iy, izp) * cv(ix, iy, izp) + cs(ixp, iy, izp) * cv(ixp, iy, izp) +
           cs(ix, iyp, izp) * cv(ix, iyp, izp) + cs(ixp, iyp, izp) * cv(ixp, iyp, izp);
     cs_v(ix, iy, iz) = R(0.125) * s / cv_v(ix, iy, iz);
   });
-  LARE_BOX(run, 0, nx + 1, 0, ny + 2, 0, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 6, 0, nx + 1, 0, ny + 2, 0, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DT], v2n = (R)sc[SC_VISC2N];
     int i1 = ix - 1, j1 = iy - 1, k1 = iz - 1, i2 = ix, j2 = iy - 1, k2 = iz - 1;
     R dvdots = -(vx(i1, j1, k1) - vx(i2, j2, k2));
@@ -263,7 +355,7 @@ void shock_viscosity(Run<R>& run) {
                                            vy(i1, j1, k1) - vy(i2, j2, k2), vz(i1, j1, k1) - vz(i2, j2, k2),
                                            dxb(ix), dt, visc1, v2n);
   });
-  LARE_BOX(run, -1, nx + 1, 0, ny + 1, 0, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 6, -1, nx + 1, 0, ny + 1, 0, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DT], v2n = (R)sc[SC_VISC2N];
     int i1 = ix, j1 = iy - 1, k1 = iz - 1, i2 = ix, j2 = iy, k2 = iz - 1;
     R dvdots = -(vy(i1, j1, k1) - vy(i2, j2, k2));
@@ -272,7 +364,7 @@ void shock_viscosity(Run<R>& run) {
                                            vy(i1, j1, k1) - vy(i2, j2, k2), vz(i1, j1, k1) - vz(i2, j2, k2),
                                            dyb(iy), dt, visc1, v2n);
   });
-  LARE_BOX(run, -1, nx + 1, -1, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 6, -1, nx + 1, -1, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DT], v2n = (R)sc[SC_VISC2N];
     int i1 = ix, j1 = iy, k1 = iz - 1, i2 = ix, j2 = iy, k2 = iz;
     R dvdots = -(vz(i1, j1, k1) - vz(i2, j2, k2));
@@ -281,7 +373,7 @@ void shock_viscosity(Run<R>& run) {
                                            vy(i1, j1, k1) - vy(i2, j2, k2), vz(i1, j1, k1) - vz(i2, j2, k2),
                                            dzb(iz), dt, visc1, v2n);
   });
-  LARE_BOX(run, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 9, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
     int ixm = ix - 1, iym = iy - 1, izm = iz - 1, iyp = iy + 1, izp = iz + 1;
     auto d2 = [&](int a0, int b0, int c0, int a1, int b1, int c1) {
       R ux = vx(a0, b0, c0) - vx(a1, b1, c1);
@@ -315,7 +407,7 @@ void shock_viscosity(Run<R>& run) {
            R(0.25) * ddx * ddy * alpha3(ixm, iym, iz) * a11 - R(0.25) * ddx * ddy * alpha3(ix, iym, iz) * a12;
     visc_heat(ix, iy, iz) = vh / cv(ix, iy, iz);
   });
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 10, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     int ixm = ix - 1, ixp = ix + 1, iym = iy - 1, iyp = iy + 1, izm = iz - 1, izp = iz + 1;
     R a1 = alpha1(ix, iyp, izp) * dyc(iy) * dzc(iz);
     R a2 = alpha1(ixp, iyp, izp) * dyc(iy) * dzc(iz);
@@ -343,7 +435,7 @@ void shock_heating(Run<R>& run) {
   auto vx = run.a.vx, vy = run.a.vy, vz = run.a.vz, vx1 = run.a.vx1, vy1 = run.a.vy1, vz1 = run.a.vz1;
   auto alpha1 = run.a.alpha1, alpha2 = run.a.alpha2, alpha3 = run.a.alpha3, cv = run.a.cv, visc_heat = run.a.visc_heat;
   auto dxb = run.a.dxb, dyb = run.a.dyb, dzb = run.a.dzb;
-  LARE_BOX(run, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 11, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
     int ixm = ix - 1, iym = iy - 1, izm = iz - 1, iyp = iy + 1, izp = iz + 1;
     auto dd = [&](int a0, int b0, int c0, int a1, int b1, int c1) {
       return (vx(a0, b0, c0) - vx(a1, b1, c1)) * (vx1(a0, b0, c0) - vx1(a1, b1, c1)) +
@@ -385,10 +477,10 @@ void calc_s_stages(Run<R>& run, int dt_slot) {
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot, k0 = (R)run.p.kappa_0;
   const R fl = (R)run.p.flux_limiter;
   const bool limiter = run.p.heat_flux_limiter != 0;
-  LARE_BOX(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 2, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     temperature(ix, iy, iz) = (g - R(1)) / (R(2) - xi) * (energy(ix, iy, iz) - (R(1) - xi) * ip);
   });
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 3, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     if (!limiter) { larsen(ix, iy, iz) = R(1); return; }
     int ixm = ix - 1, ixp = ix + 1, iym = iy - 1, iyp = iy + 1, izm = iz - 1, izp = iz + 1;
     R T = temperature(ix, iy, iz);
@@ -519,7 +611,7 @@ void temperature_from(Run<R>& run, A3<R> e) {
   const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
   auto temperature = run.a.temperature;
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
-  LARE_BOX(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 2, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     temperature(ix, iy, iz) = (g - R(1)) / (R(2) - xi) * (e(ix, iy, iz) - (R(1) - xi) * ip);
   });
 }
@@ -527,8 +619,10 @@ void temperature_from(Run<R>& run, A3<R> e) {
 // Copy between whole arrays (Fortran whole-array assignment).
 template <class R>
 void copy_whole(Run<R>& run, A3<R> dst, A3<R> src) {
+  int k = run.prof_begin("copy_whole", 0, 2, (double)run.elems);
   cudaMemcpyAsync(dst.p - (2 + 2 * run.sx + 2 * run.sxy), src.p - (2 + 2 * run.sx + 2 * run.sxy),
                   run.elems * sizeof(R), cudaMemcpyDeviceToDevice, run.s);
+  run.prof_end(k);
 }
 
 // conduct.f90:299-416 heat_conduct_sts2, dt from sc[dt_slot]; the stage
@@ -565,7 +659,7 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
   copy_whole(run, Y3, energy);
   temperature_from(run, Y0);
   const R mt1 = (R)mu_tilde[1];
-  LARE_BOX(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 10, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[dt_slot];
     R f = heat_flux_gather<R>(h, ix, iy, iz);
     R lc = (R(1) / rho(ix, iy, iz)) * f;
@@ -582,7 +676,7 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
     const R gt = (R)gamma_tilde[j], mtj = (R)mu_tilde[j], mj = (R)mu[j], nj = (R)nu[j];
     const R omn = (R)(1.0 - mu[j] - nu[j]);
     const R omn_r = R(1) - mj - nj;
-    LARE_BOX(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
+    LARE_BOXW(run, 11, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
       const R dt = (R)sc[dt_slot];
       (void)omn;
       R f = heat_flux_gather<R>(h, ix, iy, iz);
@@ -602,7 +696,7 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
     }
   }
   if (s >= 2) {
-    LARE_BOX(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) { energy(ix, iy, iz) = Y3(ix, iy, iz); });
+    LARE_BOXW(run, 3, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) { energy(ix, iy, iz) = Y3(ix, iy, iz); });
   }
   energy_bcs(run);
 }
@@ -619,13 +713,13 @@ void resistive_effects(Run<R>& run) {
   auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb, dxc = A.dxc, dyc = A.dyc, dzc = A.dzc;
   const double* sc = run.sc;
   // bx1 = bx(-1:nx+2, ...) etc. (:1259-1261)
-  LARE_BOX(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 6, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     bx1(ix, iy, iz) = bx(ix, iy, iz);
     by1(ix, iy, iz) = by(ix, iy, iz);
     bz1(ix, iy, iz) = bz(ix, iy, iz);
   });
   // rkstep (:1470-1503)
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 8, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
     R jx1 = (bz(ix, iyp, iz) - bz(ix, iy, iz)) / dyc(iy) - (by(ix, iy, izp) - by(ix, iy, iz)) / dzc(iz);
     R jx2 = (bz(ixp, iyp, iz) - bz(ixp, iy, iz)) / dyc(iy) - (by(ixp, iy, izp) - by(ixp, iy, iz)) / dzc(iz);
@@ -642,7 +736,7 @@ void resistive_effects(Run<R>& run) {
   });
   // bstep (:1582-1635)
   auto kx = flux_x, ky = flux_y, kz = flux_z;
-  LARE_BOX(run, 0, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 4, 0, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DTSUB];
     int iym = iy - 1, izm = iz - 1;
     R area = dyb(iy) * dzb(iz);
@@ -650,7 +744,7 @@ void resistive_effects(Run<R>& run) {
                                         ky(ix, iy, iz) + ky(ix, iy, izm) - ky(ix, iym, iz) + ky(ix, iym, izm)) *
                                            dt / area;
   });
-  LARE_BOX(run, 1, nx, 0, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 4, 1, nx, 0, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DTSUB];
     int ixm = ix - 1, izm = iz - 1;
     R area = dxb(ix) * dzb(iz);
@@ -658,7 +752,7 @@ void resistive_effects(Run<R>& run) {
                                         kz(ix, iy, iz) + kz(ixm, iy, iz) - kz(ix, iy, izm) + kz(ixm, iy, izm)) *
                                            dt / area;
   });
-  LARE_BOX(run, 1, nx, 1, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 4, 1, nx, 1, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DTSUB];
     int ixm = ix - 1, iym = iy - 1;
     R area = dxb(ix) * dyb(iy);
@@ -755,7 +849,7 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
   const double* sc = run.sc;
 
   // cv1, cv2, dxb1 (xremap.f90:57-105)
-  LARE_BOX(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 7, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[dt_slot];
     int ixm = ix - 1, iym = iy - 1, izm = iz - 1;
     R vxb = (vx1(ix, iy, iz) + vx1(ix, iym, iz) + vx1(ix, iy, izm) + vx1(ix, iym, izm)) * R(0.25);
@@ -776,7 +870,7 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
     db1(ix, iy, iz) = dba(pp[a]) + dvv[a] * dt;
   });
   // dxc1 (xremap.f90:107-115)
-  LARE_BOX(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 2, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     int pp[3] = {ix, iy, iz}, q[3];
     shift(q, pp, a, 0);
     q[a] = min(pp[a] + 1, na + 2);
@@ -801,7 +895,7 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
     const int o = 3 - a - b;
     const A3<R> Bb = B[b], Ba = B[a];
     // v?_b?_flux (xremap.f90:340-470 and mirrors)
-    LARE_BOX(run, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
+    LARE_BOXW(run, 5, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
       const R dt = (R)sc[dt_slot];
       int pp[3] = {ix, iy, iz}, pm[3], pq[3], pp2[3], po[3];
       shift(pm, pp, a, 0); pm[a] = max(pp[a] - 1, -1);
@@ -826,12 +920,12 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
     });
     const Rg& ra = ps == 0 ? r1a : r2a;
     const Rg& rb = ps == 0 ? r1b : r2b;
-    LARE_BOX(run, ra.l[0], ra.h[0], ra.l[1], ra.h[1], ra.l[2], ra.h[2], [=] __device__(int ix, int iy, int iz) {
+    LARE_BOXW(run, 3, ra.l[0], ra.h[0], ra.l[1], ra.h[1], ra.l[2], ra.h[2], [=] __device__(int ix, int iy, int iz) {
       int pp[3] = {ix, iy, iz}, q[3];
       shift(q, pp, a, -1);
       Bb(ix, iy, iz) = Bb(ix, iy, iz) - flux(ix, iy, iz) + flux(q[0], q[1], q[2]);
     });
-    LARE_BOX(run, rb.l[0], rb.h[0], rb.l[1], rb.h[1], rb.l[2], rb.h[2], [=] __device__(int ix, int iy, int iz) {
+    LARE_BOXW(run, 3, rb.l[0], rb.h[0], rb.l[1], rb.h[1], rb.l[2], rb.h[2], [=] __device__(int ix, int iy, int iz) {
       int pp[3] = {ix, iy, iz}, q[3];
       shift(q, pp, b, -1);
       Ba(ix, iy, iz) = Ba(ix, iy, iz) + flux(ix, iy, iz) - flux(q[0], q[1], q[2]);
@@ -847,7 +941,7 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
   int lo[3], hi[3];
   for (int d = 0; d < 3; ++d) { lo[d] = 0; hi[d] = nn[d] + 1; }
   hi[a] = na;
-  LARE_BOX(run, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 5, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[dt_slot];
     int pp[3] = {ix, iy, iz}, pm[3], pq[3], pp2[3], q1[3], q2[3], q12[3];
     shift(pm, pp, a, -1); shift(pq, pp, a, 1); shift(pp2, pp, a, 2);
@@ -878,13 +972,13 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
       dm(q[0], q[1], q[2]) = dm(s[0], s[1], s[2]);
     });
   }
-  LARE_BOX(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 5, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
     int pp[3] = {ix, iy, iz}, q[3];
     shift(q, pp, a, -1);
     rho(ix, iy, iz) = (rho1(ix, iy, iz) * cv1(ix, iy, iz) + dm(q[0], q[1], q[2]) - dm(ix, iy, iz)) / cv2(ix, iy, iz);
   });
   // x_energy_flux (xremap.f90:539-601): all 0:n
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 7, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[dt_slot];
     int pp[3] = {ix, iy, iz}, pm[3], pq[3], pp2[3], q1[3], q2[3], q12[3];
     shift(pm, pp, a, -1); shift(pq, pp, a, 1); shift(pp2, pp, a, 2);
@@ -900,7 +994,7 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
     R dmu = fabs(dm(ix, iy, iz)) / area / L.dxbu / rhou;
     flux(ix, iy, iz) = (L.fu + L.Di * (R(1) - dmu)) * dm(ix, iy, iz);
   });
-  LARE_BOX(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 7, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
     int pp[3] = {ix, iy, iz}, q[3];
     shift(q, pp, a, -1);
     energy(ix, iy, iz) = (energy(ix, iy, iz) * cv1(ix, iy, iz) * rho1(ix, iy, iz) + flux(q[0], q[1], q[2]) -
@@ -910,7 +1004,7 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
   // Vertex quantities (xremap.f90:201-290)
   for (int d = 0; d < 3; ++d) { lo[d] = 0; hi[d] = nn[d]; }
   lo[a] = -1; hi[a] = na + 1;
-  LARE_BOX(run, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 3, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
     int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
     R s = rho1(ix, iy, iz) * cv1(ix, iy, iz) + rho1(ixp, iy, iz) * cv1(ixp, iy, iz) +
           rho1(ix, iyp, iz) * cv1(ix, iyp, iz) + rho1(ixp, iyp, iz) * cv1(ixp, iyp, iz) +
@@ -921,7 +1015,7 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
   });
   // cv1, cv2 vertex averages: both computed from the cell values before
   // either is overwritten (the reference's two loops read disjoint arrays).
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 4, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
     R s1 = cv1(ix, iy, iz) + cv1(ixp, iy, iz) + cv1(ix, iyp, iz) + cv1(ixp, iyp, iz) + cv1(ix, iy, izp) +
            cv1(ixp, iy, izp) + cv1(ix, iyp, izp) + cv1(ixp, iyp, izp);
@@ -930,30 +1024,30 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
     flux(ix, iy, iz) = s1;
     rv1(ix, iy, iz) = s2;  // rho_v1 used as a temporary here, as flux is in the reference
   });
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 4, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     cv1(ix, iy, iz) = flux(ix, iy, iz) * R(0.125);
     cv2(ix, iy, iz) = rv1(ix, iy, iz) * R(0.125);
   });
   // v1 along a averaged to the vertex-cell faces: a -2:n+1, transverse 0:n
   for (int d = 0; d < 3; ++d) { lo[d] = 0; hi[d] = nn[d]; }
   lo[a] = -2; hi[a] = na + 1;
-  LARE_BOX(run, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 2, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
     int pp[3] = {ix, iy, iz}, q[3];
     shift(q, pp, a, 1);
     flux(ix, iy, iz) = (va(ix, iy, iz) + va(q[0], q[1], q[2])) * R(0.5);
   });
-  LARE_BOX(run, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2],
+  LARE_BOXW(run, 2, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2],
            [=] __device__(int ix, int iy, int iz) { va(ix, iy, iz) = flux(ix, iy, iz); });
   // dm averaged to vertex-cell faces: a -1:n, transverse 0:n
   lo[a] = -1; hi[a] = na;
-  LARE_BOX(run, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 2, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
     int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
     flux(ix, iy, iz) = dm(ix, iy, iz) + dm(ixp, iy, iz) + dm(ix, iyp, iz) + dm(ixp, iyp, iz) + dm(ix, iy, izp) +
                        dm(ixp, iy, izp) + dm(ix, iyp, izp) + dm(ixp, iyp, izp);
   });
-  LARE_BOX(run, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2],
+  LARE_BOXW(run, 2, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2],
            [=] __device__(int ix, int iy, int iz) { dm(ix, iy, iz) = flux(ix, iy, iz) * R(0.125); });
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 5, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     int pp[3] = {ix, iy, iz}, q[3];
     shift(q, pp, a, -1);
     rv1(ix, iy, iz) = (rv(ix, iy, iz) * cv1(ix, iy, iz) + dm(q[0], q[1], q[2]) - dm(ix, iy, iz)) / cv2(ix, iy, iz);
@@ -964,7 +1058,7 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
     int l2[3], h2[3];
     for (int d = 0; d < 3; ++d) { l2[d] = 0; h2[d] = nn[d]; }
     l2[a] = -1; h2[a] = na;
-    LARE_BOX(run, l2[0], h2[0], l2[1], h2[1], l2[2], h2[2], [=] __device__(int ix, int iy, int iz) {
+    LARE_BOXW(run, 7, l2[0], h2[0], l2[1], h2[1], l2[2], h2[2], [=] __device__(int ix, int iy, int iz) {
       const R dt = (R)sc[dt_slot];
       int pp[3] = {ix, iy, iz}, pm[3], pq[3], pp2[3];
       shift(pm, pp, a, -1); shift(pq, pp, a, 1); shift(pp2, pp, a, 2);
@@ -979,7 +1073,7 @@ void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
       R f = L.fu + L.Di * (R(1) - dmu);
       flux(ix, iy, iz) = f * dm(ix, iy, iz);
     });
-    LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+    LARE_BOXW(run, 7, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
       int pp[3] = {ix, iy, iz}, q[3];
       shift(q, pp, a, -1);
       vc(ix, iy, iz) = (rv(ix, iy, iz) * vc(ix, iy, iz) * cv1(ix, iy, iz) + flux(q[0], q[1], q[2]) - flux(ix, iy, iz)) /
@@ -998,7 +1092,7 @@ void eulerian_remap(Run<R>& run, int step, bool predictor) {
   auto dxb = run.a.dxb, dyb = run.a.dyb, dzb = run.a.dzb;
   int pass[3] = {1, 1, 1};
   // B -> flux (remap.f90:43-69), including the -2 layers.
-  LARE_BOX(run, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     if (iy >= -1 && iz >= -1) bx(ix, iy, iz) = bx(ix, iy, iz) * dyb(iy) * dzb(iz);
     if (ix >= -1 && iz >= -1) by(ix, iy, iz) = by(ix, iy, iz) * dxb(ix) * dzb(iz);
     if (ix >= -1 && iy >= -1) bz(ix, iy, iz) = bz(ix, iy, iz) * dxb(ix) * dyb(iy);
@@ -1008,7 +1102,7 @@ void eulerian_remap(Run<R>& run, int step, bool predictor) {
   const int dt_slot = predictor ? SC_DT2 : SC_DT;
   for (int s = 0; s < 3; ++s) remap_axis(run, order[c][s], predictor, dt_slot, pass);
   // flux -> B (remap.f90:101-127)
-  LARE_BOX(run, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     if (iy >= -1 && iz >= -1) bx(ix, iy, iz) = bx(ix, iy, iz) / dyb(iy) / dzb(iz);
     if (ix >= -1 && iz >= -1) by(ix, iy, iz) = by(ix, iy, iz) / dxb(ix) / dzb(iz);
     if (ix >= -1 && iy >= -1) bz(ix, iy, iz) = bz(ix, iy, iz) / dxb(ix) / dyb(iy);
@@ -1131,7 +1225,7 @@ void predictor_corrector_step(Run<R>& run) {
   auto cv1 = A.cv1, cv = A.cv, energy = A.energy, pressure = A.pressure, rho = A.rho, visc_heat = A.visc_heat;
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
   const double* sc = run.sc;
-  LARE_BOX(run, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 7, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
     const R dt2 = (R)sc[SC_DT2];
     R dv = cv1(ix, iy, iz) / cv(ix, iy, iz) - R(1);
     R e1 = energy(ix, iy, iz) - pressure(ix, iy, iz) * dv / rho(ix, iy, iz);
@@ -1142,7 +1236,7 @@ void predictor_corrector_step(Run<R>& run) {
   auto vx = A.vx, vy = A.vy, vz = A.vz, vx1 = A.vx1, vy1 = A.vy1, vz1 = A.vz1;
   auto fx_visc = A.fx_visc, fy_visc = A.fy_visc, fz_visc = A.fz_visc;
   auto dxc = A.dxc, dyc = A.dyc, dzc = A.dzc, grav = A.grav;
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 16, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt2 = (R)sc[SC_DT2];
     int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
     R pp = pressure(ix, iy, iz), ppx = pressure(ixp, iy, iz), ppy = pressure(ix, iyp, iz);
@@ -1182,7 +1276,7 @@ void predictor_corrector_step(Run<R>& run) {
   copy_whole(run, A.bz, A.bz0);
   remap_v_bcs(run);
   shock_heating(run);
-  LARE_BOX(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 9, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     vx(ix, iy, iz) = R(2) * vx1(ix, iy, iz) - vx(ix, iy, iz);
     vy(ix, iy, iz) = R(2) * vy1(ix, iy, iz) - vy(ix, iy, iz);
     vz(ix, iy, iz) = R(2) * vz1(ix, iy, iz) - vz(ix, iy, iz);
@@ -1220,14 +1314,14 @@ int lagrangian_step(Run<R>& run, int step) {
   auto bx = A.bx, by = A.by, bz = A.bz, bx1 = A.bx1, by1 = A.by1, bz1 = A.bz1;
   auto rho = A.rho, energy = A.energy, pressure = A.pressure, cv = A.cv, rho_v = A.rho_v, cv_v = A.cv_v;
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
-  LARE_BOX(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 9, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     int ixm = ix - 1, iym = iy - 1, izm = iz - 1;
     bx1(ix, iy, iz) = (bx(ix, iy, iz) + bx(ixm, iy, iz)) * R(0.5);
     by1(ix, iy, iz) = (by(ix, iy, iz) + by(ix, iym, iz)) * R(0.5);
     bz1(ix, iy, iz) = (bz(ix, iy, iz) + bz(ix, iy, izm)) * R(0.5);
     pressure(ix, iy, iz) = (g - R(1)) * rho(ix, iy, iz) * (energy(ix, iy, iz) - (R(1) - xi) * ip);
   });
-  LARE_BOX(run, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXW(run, 4, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
     int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
     R rv = rho(ix, iy, iz) * cv(ix, iy, iz) + rho(ixp, iy, iz) * cv(ixp, iy, iz) + rho(ix, iyp, iz) * cv(ix, iyp, iz) +
            rho(ixp, iyp, iz) * cv(ixp, iyp, iz) + rho(ix, iy, izp) * cv(ix, iy, izp) +
@@ -1262,7 +1356,7 @@ int lagrangian_step(Run<R>& run, int step) {
       eta_calc(run);
       resistive_effects(run);
     }
-    LARE_BOX(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+    LARE_BOXW(run, 6, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
       int ixm = ix - 1, iym = iy - 1, izm = iz - 1;
       bx1(ix, iy, iz) = (bx(ix, iy, iz) + bx(ixm, iy, iz)) * R(0.5);
       by1(ix, iy, iz) = (by(ix, iy, iz) + by(ix, iym, iz)) * R(0.5);

@@ -24,6 +24,8 @@ class EngineBase {
   virtual int set_field(const char* name, const double* host) = 0;
   virtual int field_bounds(const char* name, int lo[3], int hi[3]) = 0;
   virtual int scalars(lare_scalars* out) = 0;
+  virtual int profile(int enable) = 0;
+  virtual int profile_report(char* buf, int len) = 0;
   virtual long long launches() const = 0;
   virtual void* stream() const = 0;
   virtual const char* error() const = 0;

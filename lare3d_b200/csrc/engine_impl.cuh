@@ -4,8 +4,10 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <string>
@@ -22,9 +24,11 @@ struct FieldDesc {
   int lo[3], hi[3];
 };
 
+// Scatter a Fortran-bounded array into the padded box, flagging any
+// non-finite input value in *bad.
 template <class R>
 __global__ void k_scatter(const double* __restrict__ src, R* __restrict__ dst0, int lo0, int lo1, int lo2, int e0,
-                          int e1, int e2, int sx, int sxy) {
+                          int e1, int e2, int sx, int sxy, int* bad) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long n = (long long)e0 * e1 * e2;
   if (t >= n) return;
@@ -32,7 +36,9 @@ __global__ void k_scatter(const double* __restrict__ src, R* __restrict__ dst0, 
   long long r = t / e0;
   int j = (int)(r % e1);
   int k = (int)(r / e1);
-  dst0[(lo0 + i) + (long long)sx * (lo1 + j) + (long long)sxy * (lo2 + k)] = (R)src[t];
+  double v = src[t];
+  if (!isfinite(v)) atomicOr(bad, 1);
+  dst0[(lo0 + i) + (long long)sx * (lo1 + j) + (long long)sxy * (lo2 + k)] = (R)v;
 }
 
 template <class R>
@@ -60,6 +66,7 @@ class EngineT : public EngineBase {
   Run<R> run;
   std::map<std::string, std::pair<A3<R>*, FieldDesc>> fields;
   double* staging = nullptr;   // device, one array of doubles
+  int* dflag = nullptr;        // device non-finite flag for uploads
   double* metric_stage = nullptr;
   R* metrics_dev = nullptr;
 
@@ -203,7 +210,8 @@ class EngineT : public EngineBase {
     run.partial_cap = nb * 4;
     run.partial = dalloc<double>(run.partial_cap, err);
     staging = dalloc<double>(run.elems, err);
-    if (!run.sc || !run.us || !run.partial || !staging) return LARE_ENOMEM;
+    dflag = dalloc<int>(1, err);
+    if (!run.sc || !run.us || !run.partial || !staging || !dflag) return LARE_ENOMEM;
     cudaMemsetAsync(run.sc, 0, SC_NSLOTS * sizeof(double), run.s);
     if (cudaMallocHost(&run.host_sc, SC_NSLOTS * sizeof(double)) != cudaSuccess) { err = "pinned"; return LARE_ENOMEM; }
 
@@ -314,7 +322,8 @@ class EngineT : public EngineBase {
     if (cudaMemcpyAsync(staging, host, n * sizeof(double), cudaMemcpyHostToDevice, run.s) != cudaSuccess)
       return fail(LARE_ECUDA, "host to device copy failed");
     int blocks = (int)((n + 255) / 256);
-    k_scatter<R><<<blocks, 256, 0, run.s>>>(staging, a.p, f.lo[0], f.lo[1], f.lo[2], e0, e1, e2, run.sx, run.sxy);
+    k_scatter<R><<<blocks, 256, 0, run.s>>>(staging, a.p, f.lo[0], f.lo[1], f.lo[2], e0, e1, e2, run.sx, run.sxy,
+                                            dflag);
     ++run.launches;
     return cuda_check("upload");
   }
@@ -331,25 +340,57 @@ class EngineT : public EngineBase {
     return LARE_OK;
   }
 
-  static bool all_finite(const double* h, size_t n) {
-    for (size_t i = 0; i < n; ++i)
-      if (!std::isfinite(h[i])) return false;
-    return true;
-  }
-
+  // Upload the state; the scatter kernels flag non-finite values on the
+  // device, so the host reads back one int after all copies.
   int upload(const double* const* s8) override {
     static const char* names[8] = {"rho", "energy", "vx", "vy", "vz", "bx", "by", "bz"};
+    cudaMemsetAsync(dflag, 0, sizeof(int), run.s);
     for (int q = 0; q < 8; ++q) {
       if (!s8[q]) continue;
       auto& f = fields[names[q]];
-      size_t n = (size_t)(f.second.hi[0] - f.second.lo[0] + 1) * (f.second.hi[1] - f.second.lo[1] + 1) *
-                 (f.second.hi[2] - f.second.lo[2] + 1);
-      if (!all_finite(s8[q], n)) return fail(LARE_ENONFINITE, std::string("non-finite value in ") + names[q]);
       int rc = put(*f.first, f.second, s8[q]);
       if (rc) return rc;
     }
+    int bad = 0;
+    cudaMemcpyAsync(&bad, dflag, sizeof(int), cudaMemcpyDeviceToHost, run.s);
     cudaError_t e = cudaStreamSynchronize(run.s);
-    return e == cudaSuccess ? LARE_OK : fail(LARE_ECUDA, cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(LARE_ECUDA, cudaGetErrorString(e));
+    if (bad) return fail(LARE_ENONFINITE, "non-finite value in the uploaded state");
+    return LARE_OK;
+  }
+
+  int profile(int enable) override {
+    if (enable) {
+      run.prof_collect();
+      run.prof.sites.clear();
+      run.prof.index.clear();
+      run.prof.used = 0;
+      run.prof.on = true;
+    } else {
+      run.prof_collect();
+      run.prof.on = false;
+    }
+    return LARE_OK;
+  }
+
+  // One line per launch site: "site<TAB>launches<TAB>ms<TAB>algorithmic bytes<TAB>words".
+  int profile_report(char* buf, int len) override {
+    run.prof_collect();
+    std::vector<ProfSite> v = run.prof.sites;
+    std::sort(v.begin(), v.end(), [](const ProfSite& a, const ProfSite& b) { return a.ms > b.ms; });
+    std::string out;
+    char line[256];
+    for (const ProfSite& ps : v) {
+      snprintf(line, sizeof(line), "%s:%d\t%lld\t%.6f\t%.0f\t%d\n", ps.func, ps.line, ps.count, ps.ms, ps.bytes,
+               ps.words);
+      out += line;
+    }
+    if (buf && len > 0) {
+      size_t n = out.size() < (size_t)(len - 1) ? out.size() : (size_t)(len - 1);
+      memcpy(buf, out.data(), n);
+      buf[n] = 0;
+    }
+    return (int)out.size() + 1;
   }
 
   int upload_aux(const double* eta, const double* visc3, const double* grav, const double* gamma_boris) override {

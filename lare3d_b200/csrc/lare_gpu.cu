@@ -160,6 +160,16 @@ int lare_gpu_get_scalars(lare_ctx* c, lare_scalars* out) {
   return c->e->scalars(out);
 }
 
+int lare_gpu_profile(lare_ctx* c, int enable) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->profile(enable);
+}
+
+int lare_gpu_profile_report(lare_ctx* c, char* buf, int len) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->profile_report(buf, len);
+}
+
 long long lare_gpu_launch_count(lare_ctx* c) { return (c && c->e) ? c->e->launches() : -1; }
 
 void* lare_gpu_stream(lare_ctx* c) { return (c && c->e) ? c->e->stream() : nullptr; }

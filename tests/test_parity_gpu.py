@@ -1,0 +1,218 @@
+"""GPU parity: the sm_100a engine against the oracle, through the C ABI.
+
+The FP64 engine is built without FMA contraction and keeps the reference's
+loop ranges and expression order, so every routine of the MHD step must
+agree with the oracle BIT FOR BIT (tolerance 0).  Conduction calls pow(),
+whose last bit may differ between CUDA and glibc; its tolerance is a
+relative L2 of 1e-12.  The FP32 form is compared with the FP64 oracle at the
+1e-5 relative-L2 bar.
+"""
+import numpy as np
+import pytest
+
+from conftest import STATE, rel_l2
+from lare3d_b200 import decks
+from lare3d_b200.abi import BC_USER, LareError
+
+pytestmark = pytest.mark.gpu
+
+INTERMEDIATE = ["p_visc", "visc_heat", "alpha1", "alpha2", "alpha3", "pressure", "vx1", "vy1", "vz1",
+                "visc_dep", "cv1", "rho_v", "cv_v", "fx_visc", "fy_visc", "fz_visc", "eta", "ohmic_dep"]
+
+
+def pair(deck, precision=64):
+    from lare3d_b200 import gpu
+    from oracle import oracle
+    r = oracle.simulation(deck)
+    g = gpu.simulation(deck, precision=precision)
+    r.start(deck.state)
+    g.start(deck.state)
+    return r, g
+
+
+def assert_bitwise(g, r, names, tag):
+    for f in names:
+        a, b = g.get_field(f), r.get_field(f)
+        nbad = int(np.count_nonzero(a != b))
+        assert nbad == 0, f"{tag}: {f} differs in {nbad} elements (max |d| {np.abs(a - b).max():.3e})"
+
+
+CASES = [
+    ("blast", dict(n=16)),
+    ("orszag_tang", dict(n=16)),
+    ("orszag_tang", dict(n=12, eta0=2.0e-3, j_max=0.5)),          # anomalous resistivity switch
+    ("blast", dict(n=12, xbc_min=BC_USER, xbc_max=BC_USER)),       # BC_USER mirrors in x
+    ("blast", dict(n=12, zbc_min=BC_USER, zbc_max=BC_USER, ybc_min=BC_USER, ybc_max=BC_USER)),
+    ("blast", dict(n=10, use_viscous_damping=1)),
+]
+
+
+@pytest.mark.parametrize("name,kw", CASES)
+def test_routines_bitwise(built, name, kw):
+    kw = dict(kw)
+    n = kw.pop("n")
+    d = getattr(decks, name)(n, **kw)
+    if kw.get("use_viscous_damping"):
+        from lare3d_b200.abi import alloc
+        v3 = alloc("node", n, n, n, 1e-3)
+        r, g = pair(d)
+        r.upload_aux(visc3=v3)
+        g.upload_aux(visc3=v3)
+    else:
+        r, g = pair(d)
+    assert_bitwise(g, r, STATE + ["eta"], "init")
+    for st in range(1, 7):
+        r.lagrangian_step(st)
+        g.lagrangian_step(st)
+        assert_bitwise(g, r, STATE + INTERMEDIATE, f"lagrangian_step {st}")
+        r.eulerian_remap(st)
+        g.eulerian_remap(st)
+        assert_bitwise(g, r, STATE + ["cv1"], f"eulerian_remap {st}")
+        r.eta_calc()
+        g.eta_calc()
+        assert_bitwise(g, r, ["eta"], f"eta_calc {st}")
+    sr, sg = r.scalars(), g.scalars()
+    assert sr.time == sg.time and sr.dt == sg.dt and sr.dtr == sg.dtr
+    assert sr.last_substeps == sg.last_substeps
+
+
+def test_ragged_grid_bitwise(built):
+    """Unequal nx, ny, nz exercise every axis-specific loop range."""
+    d = decks.blast(12)
+    from lare3d_b200.abi import State
+    from lare3d_b200.grid import grid
+    nx, ny, nz = 14, 10, 12
+    m = grid(nx, ny, nz, (0, 1.4), (0, 1.0), (0, 1.2))
+    st = State.zeros(nx, ny, nz)
+    rng = np.random.default_rng(3)
+    for k in STATE:
+        st[k][...] = rng.uniform(0.5, 1.5, st[k].shape) if k in ("rho", "energy") else rng.uniform(-0.3, 0.3, st[k].shape)
+    d2 = decks.Deck("ragged", d.params, nx, ny, nz, m, st, nsteps=6)
+    r, g = pair(d2)
+    for s in range(1, 7):
+        r.step(s)
+        g.step(s)
+        assert_bitwise(g, r, STATE, f"step {s}")
+
+
+@pytest.mark.slow
+def test_blast_64_100_steps(built):
+    """Blast at 64^3, 100 steps at CFL 0.8: relative L2 per field <= 1e-10
+    (observed: identical)."""
+    d = decks.blast(64)
+    r, g = pair(d)
+    for s in range(1, 101):
+        r.step(s)
+        g.step(s)
+    for f in STATE:
+        a, b = g.get_field(f), r.get_field(f)
+        assert rel_l2(a, b) <= 1e-10, f
+        assert np.array_equal(a, b), f
+    er, eg = r.energy(), g.energy()
+    for q in range(5):
+        assert abs(eg[q] - er[q]) <= 1e-12 * max(1.0, abs(er[q])), q
+
+
+def test_orszag_tang_32_50_steps(built):
+    d = decks.orszag_tang(32)
+    r, g = pair(d)
+    for s in range(1, 51):
+        r.step(s)
+        g.step(s)
+    for f in STATE:
+        assert np.array_equal(g.get_field(f), r.get_field(f)), f
+
+
+def test_conduction_parity(built):
+    d = decks.conduction(16)
+    r, g = pair(d)
+    for it in range(2):
+        assert r.conduct_heat(d.dt_fixed) == g.conduct_heat(d.dt_fixed)
+        for f in ("energy", "temperature", "larsen_factor"):
+            assert rel_l2(g.get_field(f), r.get_field(f)) <= 1e-12, f
+
+
+def test_conduction_in_step(built):
+    """Conduction inside lagrangian_step (lagran.F90:168-181, set_dt's
+    stage cap :1153-1162)."""
+    d = decks.conduction(12, kappa_0=1.0e-4)
+    r, g = pair(d)
+    for s in range(1, 4):
+        r.step(s)
+        g.step(s)
+        for f in STATE:
+            assert rel_l2(g.get_field(f), r.get_field(f)) <= 1e-12, (s, f)
+    assert r.scalars().n_s_stages == g.scalars().n_s_stages
+
+
+def test_fp32_form_error(built):
+    """FP32 form vs the FP64 oracle after 100 steps (bar: 1e-5 per field)."""
+    d = decks.blast(32)
+    r, g = pair(d, precision=32)
+    for s in range(1, 101):
+        r.step(s)
+        g.step(s)
+    errs = {f: rel_l2(g.get_field(f), r.get_field(f)) for f in STATE}
+    worst = max(errs.values())
+    assert worst <= 1e-5, errs
+
+
+def test_energy_budget_parity(built):
+    d = decks.orszag_tang(16)
+    r, g = pair(d)
+    for s in range(1, 6):
+        r.step(s)
+        g.step(s)
+    er, eg = r.energy(), g.energy()
+    for q in range(5):
+        assert abs(eg[q] - er[q]) <= 1e-12 * max(1e-30, abs(er[q])), (q, er[q], eg[q])
+
+
+def test_run_matches_steps(built):
+    d = decks.blast(12)
+    from lare3d_b200 import gpu
+    a = gpu.simulation(d)
+    b = gpu.simulation(d)
+    a.start(d.state)
+    b.start(d.state)
+    for s in range(1, 6):
+        a.step(s)
+    n, t, dt = b.run(0, 5)
+    assert n == 5
+    for f in STATE:
+        assert np.array_equal(a.get_field(f), b.get_field(f))
+    # t_end stops the loop (lare3d.f90:81)
+    c = gpu.simulation(d)
+    c.start(d.state)
+    n2, t2, _ = c.run(0, 1000, t_end=a.scalars().time * 0.5)
+    assert 0 < n2 < 5 and t2 >= a.scalars().time * 0.5
+
+
+def test_field_roundtrip_and_errors(built):
+    d = decks.blast(8)
+    from lare3d_b200 import gpu
+    g = gpu.simulation(d)
+    g.start(d.state)
+    x = np.asfortranarray(np.random.default_rng(0).standard_normal(g.get_field("energy").shape))
+    g.set_field("energy", x)
+    assert np.array_equal(g.get_field("energy"), x)
+    with pytest.raises(LareError):
+        g.get_field("nope")
+    bad = d.state.copy()
+    bad["rho"][3, 3, 3] = np.nan
+    with pytest.raises(LareError) as e:
+        g.upload(bad)
+    assert "LARE_ENONFINITE" in str(e.value)
+
+
+def test_div_b_gpu(built):
+    from test_oracle_cpu import div_b
+    n = 16
+    d = decks.orszag_tang(n)
+    from lare3d_b200 import gpu
+    g = gpu.simulation(d)
+    g.start(d.state)
+    for s in range(1, 11):
+        g.step(s)
+    st = g.download()
+    assert np.abs(div_b(st, d.metrics, n)).max() < 1e-12
