@@ -48,6 +48,7 @@ extern "C" {
 #define LARE_ESTAGES (-5)    /* RKL2 stage count not representable */
 #define LARE_ENOTFOUND (-6)  /* unknown field name */
 #define LARE_ENONFINITE (-7) /* non-finite value in uploaded state */
+#define LARE_ETOOLARGE (-8)  /* grid beyond a fixed-capacity entry point's limit */
 
 /*
  * Control scalars read by the hot path.  Field names follow
@@ -160,6 +161,38 @@ int lare_gpu_conduct_heat(lare_ctx* ctx, double dt, int* n_stages);
  * total_visc_heating, total_ohmic_heating (the en.dat record, :79-83), FP64.
  */
 int lare_gpu_energy(lare_ctx* ctx, double out[5]);
+
+/*
+ * Allocation-free energy budget.  This entry point has no counterpart in the
+ * reference; it computes what lare_gpu_energy returns in out[0..2] (en_b,
+ * en_ke, en_int, diagnostics.F90:517-609) from the CALLER's device arrays,
+ * without a context and without allocating any device memory.  It is meant
+ * for callers that hold the state in their own device memory and cannot let
+ * a library call cudaMalloc: a driver that owns a fixed device-memory pool,
+ * or one that must not add allocations (and the device synchronisation they
+ * imply) between its stream-ordered steps.
+ *
+ * All pointers are device pointers to the reference's Fortran-bounded
+ * arrays (cell rho/energy, node vx/vy/vz, face bx/by/bz, 1-D dxb(-1:nx+2),
+ * dyb, dzb); out3 is a device pointer receiving the three FP64 sums.  The
+ * work is enqueued on `stream` (a cudaStream_t, NULL = default stream) and
+ * the call returns without synchronising.
+ *
+ * Limit: (nx+1)*(ny+1)*(nz+1) <= LARE_NOALLOC_MAX_POINTS (grids up to
+ * 321^3); larger grids return LARE_ETOOLARGE before any work is enqueued.
+ * Its scratch is one fixed 96 KiB array in the library image that every GPU
+ * loading the library keeps until the process exits.  All calls share it:
+ * calls that overlap on the GPU (different streams without ordering) race
+ * and give wrong sums; calls on one stream are safe.  The first call on each
+ * device looks up the scratch address on that device (once); make that first
+ * call before any stream capture begins.
+ */
+#define LARE_NOALLOC_MAX_POINTS 33554432
+int lare_gpu_energy_noalloc(int nx, int ny, int nz, const double* rho, const double* energy,
+                            const double* vx, const double* vy, const double* vz,
+                            const double* bx, const double* by, const double* bz,
+                            const double* dxb, const double* dyb, const double* dzb,
+                            double* out3, void* stream);
 
 /* Download the state into host Fortran arrays (any pointer may be NULL). */
 int lare_gpu_download(lare_ctx* ctx, double* rho, double* energy,

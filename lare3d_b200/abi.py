@@ -26,6 +26,7 @@ ERRORS = {
     -5: "LARE_ESTAGES",
     -6: "LARE_ENOTFOUND",
     -7: "LARE_ENONFINITE",
+    -8: "LARE_ETOOLARGE",
 }
 
 

@@ -31,6 +31,7 @@ UNITS = [
     ("engine_f64.cu", ["--fmad=false"]),
     ("engine_f32.cu", ["--fmad=true"]),
     ("lare_gpu.cu", []),
+    ("lare_noalloc.cu", ["--fmad=false"]),
 ]
 
 
