@@ -140,6 +140,18 @@ def cpu_baseline(deck, steps=1):
             "sample": f"{steps} step(s) of the {deck.nx}^3 workload after 1 warm-up step, {el:.2f} s/step"}
 
 
+def dump_profile(prof, name):
+    """Write the per-launch-site table of one profiled step to gpurun_out/."""
+    path = os.path.join(ROOT, "gpurun_out", name)
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    total = sum(p["ms"] for p in prof) or 1.0
+    with open(path, "w") as f:
+        f.write("site\tlaunches\tms\tshare\tGB/s\twords\n")
+        for p in prof:
+            gbs = p["bytes"] / (p["ms"] * 1e-3) / 1e9 if p["ms"] > 0 else 0.0
+            f.write(f"{p['site']}\t{p['launches']}\t{p['ms']:.4f}\t{p['ms'] / total:.3f}\t{gbs:.0f}\t{p['words']}\n")
+
+
 def time_steps(sim, torch, stream, first, k):
     """CUDA events around k device-resident steps on the engine's stream."""
     e0 = torch.cuda.Event(enable_timing=True)
@@ -232,6 +244,7 @@ def main():
     step += 1
     sim.profile(False)
     prof = sim.profile_report()
+    dump_profile(prof, f"profile_fp64_rank{rank}.tsv")
     total_ms = sum(p["ms"] for p in prof)
     top = max((p for p in prof if p["words"] > 0), key=lambda p: p["ms"])
     hbm, peak_kind = peaks()
@@ -280,6 +293,10 @@ def main():
         s32.run(0, 2)
         st32 = torch.cuda.ExternalStream(gpu.stream_of(s32))
         el32 = time_steps(s32, torch, st32, 2, args.steps)
+        s32.profile(True)
+        s32.run(2 + args.steps, 1)
+        s32.profile(False)
+        dump_profile(s32.profile_report(), "profile_fp32_rank0.tsv")
         forms["fp32"] = {"value": n3 * args.steps / el32, "unit": "cell-updates/s",
                          "ms_per_step": 1e3 * el32 / args.steps, "speedup_vs_fp64": (n3 * args.steps / el32) / value}
         s32.close()

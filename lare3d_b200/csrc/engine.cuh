@@ -43,8 +43,10 @@ struct Arrays {
   // lagran.F90 temporaries
   A3<R> bx0, by0, bz0, bx1, by1, bz1, alpha1, alpha2, alpha3, visc_heat, pressure, rho_v, cv_v;
   A3<R> flux_x, flux_y, flux_z, curlb, fx_visc, fy_visc, fz_visc, qx, qy, qz, energy0, cs, cs_v;
-  // [xyz]remap.f90 temporaries
+  // [xyz]remap.f90 temporaries (f1, f2: the two B fluxes; rho_alt: second
+  // density buffer; cv1v, cv2v, dmv: vertex averages; mf?: momentum fluxes)
   A3<R> db1, dc1, r_rho_v, r_rho_v1, rho1, dm, cv2, flux;
+  A3<R> f1, f2, rho_alt, cv1v, cv2v, dmv, mfx, mfy, mfz;
   // conduct.f90 temporaries
   A3<R> larsen, c_flux, Y0, Y1, Y2, Y3, Lc_Y0;
   // 1-D metrics (pointers at Fortran index 0)
@@ -819,270 +821,11 @@ __device__ __forceinline__ LimOut<R> limiter(R v_advect, R fm, R fi, R fp, R fp2
   return L;
 }
 
-struct Ax3 {
-  int a, t1, t2;
-};
-__device__ __forceinline__ void shift(int (&q)[3], const int (&p)[3], int d, int s) {
-  q[0] = p[0]; q[1] = p[1]; q[2] = p[2]; q[d] += s;
-}
+}  // namespace lare
 
-// xremap.f90:37-336 remap_x and its mirrors yremap.f90:37-337,
-// zremap.f90:37-336 (the files differ by the axis permutation and, for the
-// constrained-transport updates, by loop ranges tabulated below).
-// dt_slot selects dt (corrector) or dt/2 (predictor half-step).
-template <class R>
-void remap_axis(Run<R>& run, int a, bool predictor, int dt_slot, int pass[3]) {
-  const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
-  const int nn[3] = {nx, ny, nz};
-  const int na = nn[a];
-  const int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
-  Arrays<R>& A = run.a;
-  auto vx1 = A.vx1, vy1 = A.vy1, vz1 = A.vz1, cv = A.cv, cv1 = A.cv1, cv2 = A.cv2, db1 = A.db1, dc1 = A.dc1;
-  A1<R> dbm[3] = {A.dxb, A.dyb, A.dzb};
-  A1<R> dcm[3] = {A.dxc, A.dyc, A.dzc};
-  A3<R> V1[3] = {A.vx1, A.vy1, A.vz1};
-  A3<R> V[3] = {A.vx, A.vy, A.vz};
-  A3<R> B[3] = {A.bx, A.by, A.bz};
-  const A1<R> dba = dbm[a], dbt1 = dbm[t1], dbt2 = dbm[t2], dct1 = dcm[t1], dct2 = dcm[t2];
-  const A3<R> va = V1[a];
-  const R pass_t1 = (R)pass[t1], pass_t2 = (R)pass[t2];
-  const double* sc = run.sc;
+#include "remap.cuh"
 
-  // cv1, cv2, dxb1 (xremap.f90:57-105)
-  LARE_BOXW(run, 7, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
-    const R dt = (R)sc[dt_slot];
-    int ixm = ix - 1, iym = iy - 1, izm = iz - 1;
-    R vxb = (vx1(ix, iy, iz) + vx1(ix, iym, iz) + vx1(ix, iy, izm) + vx1(ix, iym, izm)) * R(0.25);
-    R vxbm = (vx1(ixm, iy, iz) + vx1(ixm, iym, iz) + vx1(ixm, iy, izm) + vx1(ixm, iym, izm)) * R(0.25);
-    R vyb = (vy1(ix, iy, iz) + vy1(ixm, iy, iz) + vy1(ix, iy, izm) + vy1(ixm, iy, izm)) * R(0.25);
-    R vybm = (vy1(ix, iym, iz) + vy1(ixm, iym, iz) + vy1(ix, iym, izm) + vy1(ixm, iym, izm)) * R(0.25);
-    R vzb = (vz1(ix, iy, iz) + vz1(ixm, iy, iz) + vz1(ix, iym, iz) + vz1(ixm, iym, iz)) * R(0.25);
-    R vzbm = (vz1(ix, iy, izm) + vz1(ixm, iy, izm) + vz1(ix, iym, izm) + vz1(ixm, iym, izm)) * R(0.25);
-    R dvv[3] = {vxb - vxbm, vyb - vybm, vzb - vzbm};
-    int pp[3] = {ix, iy, iz};
-    R term_t1 = pass_t1 * dvv[t1] / dbt1(pp[t1]);
-    R term_t2 = pass_t2 * dvv[t2] / dbt2(pp[t2]);
-    R term_a = dvv[a] / dba(pp[a]);
-    R dv = (term_t1 + term_t2 + term_a) * dt;
-    cv1(ix, iy, iz) = cv(ix, iy, iz) * (R(1) + dv);
-    dv = (term_t1 + term_t2) * dt;
-    cv2(ix, iy, iz) = cv(ix, iy, iz) * (R(1) + dv);
-    db1(ix, iy, iz) = dba(pp[a]) + dvv[a] * dt;
-  });
-  // dxc1 (xremap.f90:107-115)
-  LARE_BOXW(run, 2, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
-    int pp[3] = {ix, iy, iz}, q[3];
-    shift(q, pp, a, 0);
-    q[a] = min(pp[a] + 1, na + 2);
-    dc1(ix, iy, iz) = R(0.5) * (db1(ix, iy, iz) + db1(q[0], q[1], q[2]));
-  });
-
-  // Constrained-transport updates; ranges as written in each file
-  // (xremap.f90:121-157, yremap.f90:122-158, zremap.f90:121-157).
-  struct Rg { int l[3], h[3]; };
-  auto full = [&]() { Rg r; for (int d = 0; d < 3; ++d) { r.l[d] = 0; r.h[d] = nn[d] + 1; } return r; };
-  Rg r1a = full(), r1b = full(), r2a = full(), r2b = full();
-  if (a == 0) {
-    r2a.l[0] = 1; r2a.h[0] = nx; r2a.l[1] = 1; r2a.h[1] = ny; r2a.l[2] = 0; r2a.h[2] = nz;
-    r2b.l[0] = 0; r2b.h[0] = nx;
-  } else if (a == 1) {
-    r2b.l[0] = 1; r2b.h[0] = nx; r2b.l[1] = 0; r2b.h[1] = ny; r2b.l[2] = 1; r2b.h[2] = nz;
-  }
-  const int bfirst = a == 0 ? 1 : 0, bsecond = a == 2 ? 1 : 2;
-  auto flux = A.flux;
-  for (int ps = 0; ps < 2; ++ps) {
-    const int b = ps == 0 ? bfirst : bsecond;
-    const int o = 3 - a - b;
-    const A3<R> Bb = B[b], Ba = B[a];
-    // v?_b?_flux (xremap.f90:340-470 and mirrors)
-    LARE_BOXW(run, 5, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
-      const R dt = (R)sc[dt_slot];
-      int pp[3] = {ix, iy, iz}, pm[3], pq[3], pp2[3], po[3];
-      shift(pm, pp, a, 0); pm[a] = max(pp[a] - 1, -1);
-      shift(pq, pp, a, 1);
-      shift(pp2, pp, a, 0); pp2[a] = min(pp[a] + 2, na + 2);
-      shift(po, pp, o, -1);
-      R v_advect = (va(pp[0], pp[1], pp[2]) + va(po[0], po[1], po[2])) * R(0.5);
-      auto dbv = [&](const int (&q)[3]) {
-        int t[3];
-        shift(t, q, b, 1);
-        return (db1(q[0], q[1], q[2]) + db1(t[0], t[1], t[2])) * R(0.5);
-      };
-      R dbx = dbv(pp), dbxp = dbv(pq), dbxp2 = dbv(pp2), dbxm = dbv(pm);
-      R fm = Bb(pm[0], pm[1], pm[2]) / dbxm;
-      R fi = Bb(pp[0], pp[1], pp[2]) / dbx;
-      R fp = Bb(pq[0], pq[1], pq[2]) / dbxp;
-      R fp2 = Bb(pp2[0], pp2[1], pp2[2]) / dbxp2;
-      LimOut<R> L = limiter<R>(v_advect, fm, fi, fp, fp2, dc1(pp[0], pp[1], pp[2]), dc1(pm[0], pm[1], pm[2]),
-                               dc1(pq[0], pq[1], pq[2]), db1(pp[0], pp[1], pp[2]), db1(pq[0], pq[1], pq[2]), dbx,
-                               dbxp, dt, true);
-      flux(ix, iy, iz) = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
-    });
-    const Rg& ra = ps == 0 ? r1a : r2a;
-    const Rg& rb = ps == 0 ? r1b : r2b;
-    LARE_BOXW(run, 3, ra.l[0], ra.h[0], ra.l[1], ra.h[1], ra.l[2], ra.h[2], [=] __device__(int ix, int iy, int iz) {
-      int pp[3] = {ix, iy, iz}, q[3];
-      shift(q, pp, a, -1);
-      Bb(ix, iy, iz) = Bb(ix, iy, iz) - flux(ix, iy, iz) + flux(q[0], q[1], q[2]);
-    });
-    LARE_BOXW(run, 3, rb.l[0], rb.h[0], rb.l[1], rb.h[1], rb.l[2], rb.h[2], [=] __device__(int ix, int iy, int iz) {
-      int pp[3] = {ix, iy, iz}, q[3];
-      shift(q, pp, b, -1);
-      Ba(ix, iy, iz) = Ba(ix, iy, iz) + flux(ix, iy, iz) - flux(q[0], q[1], q[2]);
-    });
-  }
-  if (predictor) return;  // xremap.f90:159-162 (pass flag not reset)
-
-  auto dm = A.dm, rho1 = A.rho1, rho = A.rho, energy = A.energy, rv = A.r_rho_v, rv1 = A.r_rho_v1;
-  // dm = 0; rho1 = rho (xremap.f90:164-166)
-  whole(run, [=] __device__(int i, int j, int k) { dm(i, j, k) = R(0); });
-  copy_whole(run, rho1, rho);
-  // x_mass_flux (xremap.f90:474-533): a 0:n, transverse 0:n+1
-  int lo[3], hi[3];
-  for (int d = 0; d < 3; ++d) { lo[d] = 0; hi[d] = nn[d] + 1; }
-  hi[a] = na;
-  LARE_BOXW(run, 5, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
-    const R dt = (R)sc[dt_slot];
-    int pp[3] = {ix, iy, iz}, pm[3], pq[3], pp2[3], q1[3], q2[3], q12[3];
-    shift(pm, pp, a, -1); shift(pq, pp, a, 1); shift(pp2, pp, a, 2);
-    shift(q1, pp, t1, -1); shift(q2, pp, t2, -1); shift(q12, q1, t2, -1);
-    R area = dbt1(pp[t1]) * dbt2(pp[t2]);
-    R v_advect = (va(pp[0], pp[1], pp[2]) + va(q1[0], q1[1], q1[2]) + va(q2[0], q2[1], q2[2]) +
-                  va(q12[0], q12[1], q12[2])) * R(0.25);
-    LimOut<R> L = limiter<R>(v_advect, rho(pm[0], pm[1], pm[2]), rho(ix, iy, iz), rho(pq[0], pq[1], pq[2]),
-                             rho(pp2[0], pp2[1], pp2[2]), dc1(ix, iy, iz), dc1(pm[0], pm[1], pm[2]),
-                             dc1(pq[0], pq[1], pq[2]), db1(ix, iy, iz), db1(pq[0], pq[1], pq[2]), R(0), R(0), dt,
-                             false);
-    dm(ix, iy, iz) = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt * area;
-  });
-  // dm_[xyz]_bcs
-  if (run.p.per[a]) {
-    ghost(run, run.g_dm[a], dm);
-  } else {
-    int tl[3], th[3];
-    for (int d = 0; d < 3; ++d) { tl[d] = 0; th[d] = nn[d] + 1; }
-    tl[a] = 0; th[a] = 0;
-    LARE_BOX(run, tl[0], th[0], tl[1], th[1], tl[2], th[2], [=] __device__(int ix, int iy, int iz) {
-      int pp[3] = {ix, iy, iz}, s[3], q[3];
-      shift(s, pp, a, 0); s[a] = na;
-      shift(q, pp, a, 0); q[a] = na + 1;
-      dm(q[0], q[1], q[2]) = dm(s[0], s[1], s[2]);
-      shift(s, pp, a, 0); s[a] = 0;
-      shift(q, pp, a, 0); q[a] = -1;
-      dm(q[0], q[1], q[2]) = dm(s[0], s[1], s[2]);
-    });
-  }
-  LARE_BOXW(run, 5, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
-    int pp[3] = {ix, iy, iz}, q[3];
-    shift(q, pp, a, -1);
-    rho(ix, iy, iz) = (rho1(ix, iy, iz) * cv1(ix, iy, iz) + dm(q[0], q[1], q[2]) - dm(ix, iy, iz)) / cv2(ix, iy, iz);
-  });
-  // x_energy_flux (xremap.f90:539-601): all 0:n
-  LARE_BOXW(run, 7, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
-    const R dt = (R)sc[dt_slot];
-    int pp[3] = {ix, iy, iz}, pm[3], pq[3], pp2[3], q1[3], q2[3], q12[3];
-    shift(pm, pp, a, -1); shift(pq, pp, a, 1); shift(pp2, pp, a, 2);
-    shift(q1, pp, t1, -1); shift(q2, pp, t2, -1); shift(q12, q1, t2, -1);
-    R area = dbt1(pp[t1]) * dbt2(pp[t2]);
-    R v_advect = (va(pp[0], pp[1], pp[2]) + va(q1[0], q1[1], q1[2]) + va(q2[0], q2[1], q2[2]) +
-                  va(q12[0], q12[1], q12[2])) * R(0.25);
-    LimOut<R> L = limiter<R>(v_advect, energy(pm[0], pm[1], pm[2]), energy(ix, iy, iz),
-                             energy(pq[0], pq[1], pq[2]), energy(pp2[0], pp2[1], pp2[2]), dc1(ix, iy, iz),
-                             dc1(pm[0], pm[1], pm[2]), dc1(pq[0], pq[1], pq[2]), db1(ix, iy, iz),
-                             db1(pq[0], pq[1], pq[2]), R(0), R(0), dt, false);
-    R rhou = rho1(ix, iy, iz) * L.vad_p + rho1(pq[0], pq[1], pq[2]) * L.vad_m;
-    R dmu = fabs(dm(ix, iy, iz)) / area / L.dxbu / rhou;
-    flux(ix, iy, iz) = (L.fu + L.Di * (R(1) - dmu)) * dm(ix, iy, iz);
-  });
-  LARE_BOXW(run, 7, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
-    int pp[3] = {ix, iy, iz}, q[3];
-    shift(q, pp, a, -1);
-    energy(ix, iy, iz) = (energy(ix, iy, iz) * cv1(ix, iy, iz) * rho1(ix, iy, iz) + flux(q[0], q[1], q[2]) -
-                          flux(ix, iy, iz)) /
-                         (cv2(ix, iy, iz) * rho(ix, iy, iz));
-  });
-  // Vertex quantities (xremap.f90:201-290)
-  for (int d = 0; d < 3; ++d) { lo[d] = 0; hi[d] = nn[d]; }
-  lo[a] = -1; hi[a] = na + 1;
-  LARE_BOXW(run, 3, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
-    int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
-    R s = rho1(ix, iy, iz) * cv1(ix, iy, iz) + rho1(ixp, iy, iz) * cv1(ixp, iy, iz) +
-          rho1(ix, iyp, iz) * cv1(ix, iyp, iz) + rho1(ixp, iyp, iz) * cv1(ixp, iyp, iz) +
-          rho1(ix, iy, izp) * cv1(ix, iy, izp) + rho1(ixp, iy, izp) * cv1(ixp, iy, izp) +
-          rho1(ix, iyp, izp) * cv1(ix, iyp, izp) + rho1(ixp, iyp, izp) * cv1(ixp, iyp, izp);
-    rv(ix, iy, iz) = s / (cv1(ix, iy, iz) + cv1(ixp, iy, iz) + cv1(ix, iyp, iz) + cv1(ixp, iyp, iz) +
-                          cv1(ix, iy, izp) + cv1(ixp, iy, izp) + cv1(ix, iyp, izp) + cv1(ixp, iyp, izp));
-  });
-  // cv1, cv2 vertex averages: both computed from the cell values before
-  // either is overwritten (the reference's two loops read disjoint arrays).
-  LARE_BOXW(run, 4, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
-    int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
-    R s1 = cv1(ix, iy, iz) + cv1(ixp, iy, iz) + cv1(ix, iyp, iz) + cv1(ixp, iyp, iz) + cv1(ix, iy, izp) +
-           cv1(ixp, iy, izp) + cv1(ix, iyp, izp) + cv1(ixp, iyp, izp);
-    R s2 = cv2(ix, iy, iz) + cv2(ixp, iy, iz) + cv2(ix, iyp, iz) + cv2(ixp, iyp, iz) + cv2(ix, iy, izp) +
-           cv2(ixp, iy, izp) + cv2(ix, iyp, izp) + cv2(ixp, iyp, izp);
-    flux(ix, iy, iz) = s1;
-    rv1(ix, iy, iz) = s2;  // rho_v1 used as a temporary here, as flux is in the reference
-  });
-  LARE_BOXW(run, 4, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
-    cv1(ix, iy, iz) = flux(ix, iy, iz) * R(0.125);
-    cv2(ix, iy, iz) = rv1(ix, iy, iz) * R(0.125);
-  });
-  // v1 along a averaged to the vertex-cell faces: a -2:n+1, transverse 0:n
-  for (int d = 0; d < 3; ++d) { lo[d] = 0; hi[d] = nn[d]; }
-  lo[a] = -2; hi[a] = na + 1;
-  LARE_BOXW(run, 2, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
-    int pp[3] = {ix, iy, iz}, q[3];
-    shift(q, pp, a, 1);
-    flux(ix, iy, iz) = (va(ix, iy, iz) + va(q[0], q[1], q[2])) * R(0.5);
-  });
-  LARE_BOXW(run, 2, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2],
-           [=] __device__(int ix, int iy, int iz) { va(ix, iy, iz) = flux(ix, iy, iz); });
-  // dm averaged to vertex-cell faces: a -1:n, transverse 0:n
-  lo[a] = -1; hi[a] = na;
-  LARE_BOXW(run, 2, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
-    int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
-    flux(ix, iy, iz) = dm(ix, iy, iz) + dm(ixp, iy, iz) + dm(ix, iyp, iz) + dm(ixp, iyp, iz) + dm(ix, iy, izp) +
-                       dm(ixp, iy, izp) + dm(ix, iyp, izp) + dm(ixp, iyp, izp);
-  });
-  LARE_BOXW(run, 2, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2],
-           [=] __device__(int ix, int iy, int iz) { dm(ix, iy, iz) = flux(ix, iy, iz) * R(0.125); });
-  LARE_BOXW(run, 5, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
-    int pp[3] = {ix, iy, iz}, q[3];
-    shift(q, pp, a, -1);
-    rv1(ix, iy, iz) = (rv(ix, iy, iz) * cv1(ix, iy, iz) + dm(q[0], q[1], q[2]) - dm(ix, iy, iz)) / cv2(ix, iy, iz);
-  });
-  // x_mom{x,y,z}_flux (xremap.f90:605-895) and the v updates (:292-329)
-  for (int comp = 0; comp < 3; ++comp) {
-    const A3<R> vc = V[comp];
-    int l2[3], h2[3];
-    for (int d = 0; d < 3; ++d) { l2[d] = 0; h2[d] = nn[d]; }
-    l2[a] = -1; h2[a] = na;
-    LARE_BOXW(run, 7, l2[0], h2[0], l2[1], h2[1], l2[2], h2[2], [=] __device__(int ix, int iy, int iz) {
-      const R dt = (R)sc[dt_slot];
-      int pp[3] = {ix, iy, iz}, pm[3], pq[3], pp2[3];
-      shift(pm, pp, a, -1); shift(pq, pp, a, 1); shift(pp2, pp, a, 2);
-      R area = dct1(pp[t1]) * dct2(pp[t2]);
-      R v_advect = va(ix, iy, iz);
-      LimOut<R> L = limiter<R>(v_advect, vc(pm[0], pm[1], pm[2]), vc(ix, iy, iz), vc(pq[0], pq[1], pq[2]),
-                               vc(pp2[0], pp2[1], pp2[2]), db1(pq[0], pq[1], pq[2]), db1(ix, iy, iz),
-                               db1(pp2[0], pp2[1], pp2[2]), dc1(ix, iy, iz), dc1(pq[0], pq[1], pq[2]), R(0), R(0), dt,
-                               false);
-      R rhou = rv(ix, iy, iz) * L.vad_p + rv(pq[0], pq[1], pq[2]) * L.vad_m;
-      R dmu = fabs(dm(ix, iy, iz)) / area / L.dxbu / rhou;
-      R f = L.fu + L.Di * (R(1) - dmu);
-      flux(ix, iy, iz) = f * dm(ix, iy, iz);
-    });
-    LARE_BOXW(run, 7, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
-      int pp[3] = {ix, iy, iz}, q[3];
-      shift(q, pp, a, -1);
-      vc(ix, iy, iz) = (rv(ix, iy, iz) * vc(ix, iy, iz) * cv1(ix, iy, iz) + flux(q[0], q[1], q[2]) - flux(ix, iy, iz)) /
-                       (cv2(ix, iy, iz) * rv1(ix, iy, iz));
-    });
-  }
-  boundary_conditions(run);
-  pass[a] = 0;
-}
+namespace lare {
 
 // remap.f90:33-131 eulerian_remap
 template <class R>
@@ -1100,7 +843,13 @@ void eulerian_remap(Run<R>& run, int step, bool predictor) {
   static const int order[6][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}, {0, 2, 1}, {2, 1, 0}, {1, 0, 2}};
   int c = ((step % 6) + 6) % 6;
   const int dt_slot = predictor ? SC_DT2 : SC_DT;
-  for (int s = 0; s < 3; ++s) remap_axis(run, order[c][s], predictor, dt_slot, pass);
+  for (int s = 0; s < 3; ++s) {
+    switch (order[c][s]) {
+      case 0: remap_sweep<0>(run, predictor, dt_slot, pass); break;
+      case 1: remap_sweep<1>(run, predictor, dt_slot, pass); break;
+      default: remap_sweep<2>(run, predictor, dt_slot, pass); break;
+    }
+  }
   // flux -> B (remap.f90:101-127)
   LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     if (iy >= -1 && iz >= -1) bx(ix, iy, iz) = bx(ix, iy, iz) / dyb(iy) / dzb(iz);

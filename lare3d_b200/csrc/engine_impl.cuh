@@ -188,7 +188,8 @@ class EngineT : public EngineBase {
         &run.a.visc_heat, &run.a.pressure, &run.a.rho_v, &run.a.cv_v, &run.a.flux_x, &run.a.flux_y,
         &run.a.flux_z, &run.a.curlb, &run.a.fx_visc, &run.a.fy_visc, &run.a.fz_visc, &run.a.qx, &run.a.qy,
         &run.a.qz, &run.a.energy0, &run.a.cs, &run.a.cs_v, &run.a.db1, &run.a.dc1, &run.a.r_rho_v,
-        &run.a.r_rho_v1, &run.a.rho1, &run.a.dm, &run.a.cv2, &run.a.flux};
+        &run.a.r_rho_v1, &run.a.rho1, &run.a.dm, &run.a.cv2, &run.a.flux, &run.a.f1, &run.a.f2,
+        &run.a.rho_alt, &run.a.cv1v, &run.a.cv2v, &run.a.dmv, &run.a.mfx, &run.a.mfy, &run.a.mfz};
     if (p.conduction) {
       for (A3<R>* x : {&run.a.larsen, &run.a.c_flux, &run.a.Y0, &run.a.Y1, &run.a.Y2, &run.a.Y3, &run.a.Lc_Y0})
         all.push_back(x);

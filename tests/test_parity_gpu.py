@@ -67,7 +67,8 @@ def test_routines_bitwise(built, name, kw):
         assert_bitwise(g, r, STATE + INTERMEDIATE, f"lagrangian_step {st}")
         r.eulerian_remap(st)
         g.eulerian_remap(st)
-        assert_bitwise(g, r, STATE + ["cv1"], f"eulerian_remap {st}")
+        # cv1 after the remap is scratch (vertex averages in the reference)
+        assert_bitwise(g, r, STATE, f"eulerian_remap {st}")
         r.eta_calc()
         g.eta_calc()
         assert_bitwise(g, r, ["eta"], f"eta_calc {st}")
