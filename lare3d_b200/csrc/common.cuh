@@ -219,9 +219,34 @@ __device__ __forceinline__ int gmap(const GDim& g, int i, bool& zero) {
   return i;
 }
 
+// Up to kMaxGhostJobs fills in one launch: blockIdx.y selects the job; a job
+// applies one GSpec to up to three arrays.
+constexpr int kMaxGhostJobs = 6;
+template <class R>
+struct GJobs {
+  GSpec s[kMaxGhostJobs];
+  R* p[kMaxGhostJobs][3];
+  int n;
+};
+
+template <class R>
+__device__ __forceinline__ void ghost_point(const GSpec& s, R* p0, R* p1, R* p2, int sx, int sxy, long long t);
+
+template <class R>
+__global__ void __launch_bounds__(256) k_ghost_multi(GJobs<R> J, int sx, int sxy) {
+  const int j = blockIdx.y;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  ghost_point<R>(J.s[j], J.p[j][0], J.p[j][1], J.p[j][2], sx, sxy, t);
+}
+
 template <class R>
 __global__ void __launch_bounds__(256) k_ghost(GSpec s, R* p0, R* p1, R* p2, int sx, int sxy) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  ghost_point<R>(s, p0, p1, p2, sx, sxy, t);
+}
+
+template <class R>
+__device__ __forceinline__ void ghost_point(const GSpec& s, R* p0, R* p1, R* p2, int sx, int sxy, long long t) {
   const GDim &X = s.d[0], &Y = s.d[1], &Z = s.d[2];
   int i, j, k;
   if (t < s.c0) {

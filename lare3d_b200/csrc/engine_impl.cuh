@@ -425,7 +425,7 @@ class EngineT : public EngineBase {
     return cuda_check("lagrangian_step");
   }
   int eulerian_remap(int step) override {
-    lare::eulerian_remap(run, step, false);
+    lare::eulerian_remap(run, step);
     return cuda_check("eulerian_remap");
   }
   int eta_calc() override {

@@ -1,0 +1,676 @@
+// lagran.cuh - lagrangian_step (lagran.F90:50-200) with its callees, fused.
+//
+// Kernels (each element computed by the reference's own expression over
+// the reference's own inputs, so results are bit-identical; only where
+// intermediates live changes):
+//   LP1 prologue   face->cell B, pressure, sound speed cs, vertex rho_v and
+//                  cv_v (:83-125, shock_viscosity :551-559); the cell B
+//                  averages stay in registers
+//   LP2 cs_v       (:561-581)
+//   LP3 alphas     the three edge-viscosity loops (:583-678)
+//   LP4 p_visc, visc_heat and the viscous forces (:680-789)
+//   RS1 eta_calc + rkstep: one current evaluation serves both (:1182-1225,
+//                  :1470-1503, identical expressions)
+//   RS2 bstep      the three face updates (:1582-1631) into a second B
+//                  buffer; bfield_bcs then writes every element outside
+//                  the update ranges, so the buffers swap instead of the
+//                  bx1 = bx copy (:1259-1261)
+//   RS3 ohmic heating, energy = MAX(energy, 0) and total_ohmic_heating
+//   PR  the predictor's half-dt B remap on a converted copy of B, so the
+//                  saved bx0 and the restore (:223-225, :389-393) become a
+//                  pointer swap, and v is read in place of the vx1 = vx copy
+//   PC1 energy = MAX(energy0 + delta, 0) (:180-181) and the predictor
+//                  pressure (:234-249)
+//   PC2 vertex forces and the half-step velocity (:251-387)
+//   PC3 shock_heating (:861-937) and v = 2 v1 - v (:399-407) into a second
+//                  v buffer
+//   PC4 final cv1, energy, rho and total_visc_heating (:415-462)
+// The repeated velocity_bcs at the end of lagrangian_step (:198) follows an
+// identical one with no velocity change in between, so it is skipped.
+#pragma once
+
+#include <utility>
+
+namespace lare {
+
+// Vertex current of eta_calc (lagran.F90:1190-1216), rkstep (:1479-1494)
+// and the predictor force (:358-373): the three places use the same
+// expressions, evaluated here once.
+template <class R>
+__device__ __forceinline__ void vertex_current(const R* bx, const R* by, const R* bz, int c, int sx, int sxy,
+                                               R dxc, R dyc, R dzc, R& jx, R& jy, R& jz) {
+  R jx1 = (bz[c + sx] - bz[c]) / dyc - (by[c + sxy] - by[c]) / dzc;
+  R jx2 = (bz[c + 1 + sx] - bz[c + 1]) / dyc - (by[c + 1 + sxy] - by[c + 1]) / dzc;
+  R jy1 = (bx[c + sxy] - bx[c]) / dzc - (bz[c + 1] - bz[c]) / dxc;
+  R jy2 = (bx[c + sx + sxy] - bx[c + sx]) / dzc - (bz[c + 1 + sx] - bz[c + sx]) / dxc;
+  R jz1 = (by[c + 1] - by[c]) / dxc - (bx[c + sx] - bx[c]) / dyc;
+  R jz2 = (by[c + 1 + sxy] - by[c + sxy]) / dxc - (bx[c + sx + sxy] - bx[c + sxy]) / dyc;
+  jx = (jx1 + jx2) * R(0.5);
+  jy = (jy1 + jy2) * R(0.5);
+  jz = (jz1 + jz2) * R(0.5);
+}
+
+// ---------------------------------------------------------------------
+// eta_calc (lagran.F90:1176-1230), optionally fused with rkstep (:1470-1503)
+// whose fluxes need eta at the same vertex.
+template <class R>
+void eta_and_rkstep(Run<R>& run, bool with_rkstep) {
+  const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
+  const int sx = run.sx, sxy = run.sxy;
+  R* const eta = run.a.eta.p;
+  if (!run.p.resistive_mhd) {
+    whole(run, [=] __device__(int i, int j, int k) { eta[i + sx * j + sxy * k] = R(0); });
+    return;
+  }
+  const R* bx = run.a.bx.p;
+  const R* by = run.a.by.p;
+  const R* bz = run.a.bz.p;
+  R* const fxp = run.a.flux_x.p;
+  R* const fyp = run.a.flux_y.p;
+  R* const fzp = run.a.flux_z.p;
+  R* const curlb = run.a.curlb.p;
+  auto dxc = run.a.dxc, dyc = run.a.dyc, dzc = run.a.dzc;
+  const R jmax = (R)run.p.j_max, eb = (R)run.p.eta_background, e0 = (R)run.p.eta0;
+  LARE_BOXW(run, with_rkstep ? 8 : 4, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
+    const int c = ix + sx * iy + sxy * iz;
+    R jx, jy, jz;
+    vertex_current<R>(bx, by, bz, c, sx, sxy, dxc(ix), dyc(iy), dzc(iz), jx, jy, jz);
+    R j2 = jx * jx + jy * jy + jz * jz;
+    R e = sqrt(j2) > jmax ? eb + e0 : eb;
+    eta[c] = e;
+    if (with_rkstep && ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz) {
+      fxp[c] = -jx * e * dxc(ix) * R(0.5);
+      fyp[c] = -jy * e * dyc(iy) * R(0.5);
+      fzp[c] = -jz * e * dzc(iz) * R(0.5);
+      curlb[c] = e * j2;
+    }
+  });
+}
+
+template <class R>
+void eta_calc(Run<R>& run) {
+  eta_and_rkstep(run, false);
+}
+
+// ---------------------------------------------------------------------
+// lagran.F90:1239-1452 resistive_effects (first order, no cooling term),
+// after eta_and_rkstep.
+template <class R>
+void resistive_update(Run<R>& run) {
+  const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
+  const int sx = run.sx, sxy = run.sxy;
+  Arrays<R>& A = run.a;
+  const R* bxo = A.bx.p;
+  const R* byo = A.by.p;
+  const R* bzo = A.bz.p;
+  R* const bxn = A.bx1.p;
+  R* const byn = A.by1.p;
+  R* const bzn = A.bz1.p;
+  const R* kx = A.flux_x.p;
+  const R* ky = A.flux_y.p;
+  const R* kz = A.flux_z.p;
+  auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb, dxc = A.dxc, dyc = A.dyc, dzc = A.dzc;
+  const double* sc = run.sc;
+  // RS2: bstep (:1588-1631) into the second buffers
+  LARE_BOXW(run, 9, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+    const R dt = (R)sc[SC_DTSUB];
+    const int c = ix + sx * iy + sxy * iz;
+    if (iy >= 1 && iz >= 1) {
+      R area = dyb(iy) * dzb(iz);
+      bxn[c] = bxo[c] + (kz[c] - kz[c - sx] + kz[c - sxy] - kz[c - sx - sxy] - ky[c] + ky[c - sxy] - ky[c - sx] +
+                         ky[c - sx - sxy]) * dt / area;
+    }
+    if (ix >= 1 && iz >= 1) {
+      R area = dxb(ix) * dzb(iz);
+      byn[c] = byo[c] + (kx[c] - kx[c - sxy] + kx[c - 1] - kx[c - 1 - sxy] - kz[c] + kz[c - 1] - kz[c - sxy] +
+                         kz[c - 1 - sxy]) * dt / area;
+    }
+    if (ix >= 1 && iy >= 1) {
+      R area = dxb(ix) * dyb(iy);
+      bzn[c] = bzo[c] + (ky[c] - ky[c - 1] + ky[c - sx] - ky[c - 1 - sx] - kx[c] + kx[c - sx] - kx[c - 1] +
+                         kx[c - 1 - sx]) * dt / area;
+    }
+  });
+  std::swap(A.bx.p, A.bx1.p);
+  std::swap(A.by.p, A.by1.p);
+  std::swap(A.bz.p, A.bz1.p);
+  bfield_bcs(run);
+  // RS3: ohmic heating (1:n), MAX(energy, 0) (-1:n+2) and the
+  // total_ohmic_heating sum over vertices 0:n (:1270-1328)
+  R* const energy = A.energy.p;
+  R* const ohmic = A.ohmic_dep.p;
+  const R* curlb = A.curlb.p;
+  const R* rho = A.rho.p;
+  box_sum<1>(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz, double* v) {
+    const R dt = (R)sc[SC_DTSUB];
+    const int c = ix + sx * iy + sxy * iz;
+    R e = energy[c];
+    if (ix >= 1 && ix <= nx && iy >= 1 && iy <= ny && iz >= 1 && iz <= nz) {
+      R lh = +(curlb[c] + curlb[c - 1] + curlb[c - sx] + curlb[c - 1 - sx] + curlb[c - sxy] + curlb[c - 1 - sxy] +
+               curlb[c - sx - sxy] + curlb[c - 1 - sx - sxy]) * dt / (R(8) * rho[c]);
+      ohmic[c] = ohmic[c] + lh;
+      e = e + lh;
+    }
+    energy[c] = e > R(0) ? e : R(0);
+    if (ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz) {
+      R w1 = dt * dxc(ix) * dyc(iy) * dzc(iz) * curlb[c];
+      if (ix == 0 || ix == nx) w1 = w1 * R(0.5);
+      if (iy == 0 || iy == ny) w1 = w1 * R(0.5);
+      if (iz == 0 || iz == nz) w1 = w1 * R(0.5);
+      v[0] = (double)w1;
+    }
+  }, SC_OHM_TOT, true);
+  energy_bcs(run);
+}
+
+// ---------------------------------------------------------------------
+// LP1-LP4: prologue and shock_viscosity (lagran.F90:83-125, 532-857)
+template <class R>
+void prologue_and_shock_viscosity(Run<R>& run) {
+  const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
+  const int sx = run.sx, sxy = run.sxy;
+  Arrays<R>& A = run.a;
+  if (!run.visc2_norm_set) {
+    run.visc2_norm_set = true;
+    double v2n = 0.25 * (run.p.gamma + 1.0) * run.p.visc2;
+    if (sizeof(R) == 4) v2n = (double)(R(0.25) * (R(run.p.gamma) + R(1)) * R(run.p.visc2));
+    cudaMemcpyAsync(run.sc + SC_VISC2N, &v2n, sizeof(double), cudaMemcpyHostToDevice, run.s);
+    cudaStreamSynchronize(run.s);
+  }
+  const R* bx = A.bx.p;
+  const R* by = A.by.p;
+  const R* bz = A.bz.p;
+  const R* rho = A.rho.p;
+  const R* energy = A.energy.p;
+  const R* cv = A.cv.p;
+  const R* gamma_boris = A.gamma_boris.p;
+  R* const pressure = A.pressure.p;
+  R* const cs = A.cs.p;
+  R* const rho_v = A.rho_v.p;
+  R* const cv_v = A.cv_v.p;
+  R* const p_visc = A.p_visc.p;
+  const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
+  // LP1
+  LARE_BOXW(run, 11, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+    const int c = ix + sx * iy + sxy * iz;
+    R bx1 = (bx[c] + bx[c - 1]) * R(0.5);
+    R by1 = (by[c] + by[c - sx]) * R(0.5);
+    R bz1 = (bz[c] + bz[c - sxy]) * R(0.5);
+    R r = rho[c];
+    R pr = (g - R(1)) * r * (energy[c] - (R(1) - xi) * ip);
+    pressure[c] = pr;
+    R rmin = fmax(r, Num<R>::tiny());
+    R b2 = bx1 * bx1 + by1 * by1 + bz1 * bz1;
+    cs[c] = sqrt((g * pr + gamma_boris[c] * b2) / rmin);
+    if (ix == -1 || ix == nx + 2 || iy == -1 || iy == ny + 2 || iz == -1 || iz == nz + 2)
+      p_visc[c] = R(0);  // p_visc = 0 (:548) outside the 0:n+1 MAX loop
+    if (ix <= nx + 1 && iy <= ny + 1 && iz <= nz + 1) {
+      // the eight cells around vertex c, in the reference's order
+      const int o1 = 1, o2 = sx, o3 = 1 + sx, o4 = sxy, o5 = 1 + sxy, o6 = sx + sxy, o7 = 1 + sx + sxy;
+      R rv = rho[c] * cv[c] + rho[c + o1] * cv[c + o1] + rho[c + o2] * cv[c + o2] + rho[c + o3] * cv[c + o3] +
+             rho[c + o4] * cv[c + o4] + rho[c + o5] * cv[c + o5] + rho[c + o6] * cv[c + o6] +
+             rho[c + o7] * cv[c + o7];
+      R cvv = cv[c] + cv[c + o1] + cv[c + o2] + cv[c + o3] + cv[c + o4] + cv[c + o5] + cv[c + o6] + cv[c + o7];
+      rho_v[c] = rv / cvv;
+      cv_v[c] = R(0.125) * cvv;
+    }
+  });
+  if (run.p.use_viscous_damping) viscous_damping(run);
+  // LP2: cs_v (:561-581)
+  R* const cs_v = A.cs_v.p;
+  LARE_BOXW(run, 4, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
+    const int c = ix + sx * iy + sxy * iz;
+    const int o1 = 1, o2 = sx, o3 = 1 + sx, o4 = sxy, o5 = 1 + sxy, o6 = sx + sxy, o7 = 1 + sx + sxy;
+    R s = cs[c] * cv[c] + cs[c + o1] * cv[c + o1] + cs[c + o2] * cv[c + o2] + cs[c + o3] * cv[c + o3] +
+          cs[c + o4] * cv[c + o4] + cs[c + o5] * cv[c + o5] + cs[c + o6] * cv[c + o6] + cs[c + o7] * cv[c + o7];
+    cs_v[c] = R(0.125) * s / cv_v[c];
+  });
+  // LP3: alpha1 (0:n+1, 0:n+2, 0:n+2), alpha2 (-1:n+1, 0:n+1, 0:n+2),
+  // alpha3 (-1:n+1, -1:n+1, 0:n+1)
+  const R* vx = A.vx.p;
+  const R* vy = A.vy.p;
+  const R* vz = A.vz.p;
+  R* const alpha1 = A.alpha1.p;
+  R* const alpha2 = A.alpha2.p;
+  R* const alpha3 = A.alpha3.p;
+  auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb, dxc = A.dxc, dyc = A.dyc, dzc = A.dzc;
+  const R visc1 = (R)run.p.visc1;
+  const double* sc = run.sc;
+  LARE_BOXW(run, 8, -1, nx + 1, -1, ny + 2, 0, nz + 2, [=] __device__(int ix, int iy, int iz) {
+    const R dt = (R)sc[SC_DT], v2n = (R)sc[SC_VISC2N];
+    const int c = ix + sx * iy + sxy * iz;
+    auto edge = [&](const R* vcomp, int i1, int i2, R dx) {
+      R dvdots = -(vcomp[i1] - vcomp[i2]);
+      return edge_viscosity<R>(dvdots, rho_v[i1], rho_v[i2], cs_v[i1], cs_v[i2], vx[i1] - vx[i2], vy[i1] - vy[i2],
+                               vz[i1] - vz[i2], dx, dt, visc1, v2n);
+    };
+    if (ix >= 0 && iy >= 0) alpha1[c] = edge(vx, c - 1 - sx - sxy, c - sx - sxy, dxb(ix));
+    if (iy >= 0 && iy <= ny + 1) alpha2[c] = edge(vy, c - sx - sxy, c - sxy, dyb(iy));
+    if (iy <= ny + 1 && iz <= nz + 1) alpha3[c] = edge(vz, c - sxy, c, dzb(iz));
+  });
+  // LP4: p_visc and visc_heat (0:n+1), viscous forces (0:n)
+  R* const visc_heat = A.visc_heat.p;
+  R* const fxv = A.fx_visc.p;
+  R* const fyv = A.fy_visc.p;
+  R* const fzv = A.fz_visc.p;
+  LARE_BOXW(run, 13, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
+    const int c = ix + sx * iy + sxy * iz;
+    auto d2 = [&](int p0, int p1) {
+      R ux = vx[p0] - vx[p1];
+      R uy = vy[p0] - vy[p1];
+      R uz = vz[p0] - vz[p1];
+      return ux * ux + uy * uy + uz * uz;
+    };
+    const int X = 1, Y = sx, Z = sxy;
+    R a1 = d2(c - X - Y - Z, c - Y - Z);
+    R a2 = d2(c - Y - Z, c - Z);
+    R a3 = d2(c - Z, c - X - Z);
+    R a4 = d2(c - X - Z, c - X - Y - Z);
+    R a5 = d2(c - X - Y, c - Y);
+    R a6 = d2(c - Y, c);
+    R a7 = d2(c, c - X);
+    R a8 = d2(c - X, c - X - Y);
+    R a9 = d2(c - Z, c);
+    R a10 = d2(c - X - Z, c - X);
+    R a11 = d2(c - X - Y - Z, c - X - Y);
+    R a12 = d2(c - Y - Z, c - Y);
+    R pv = R(0);
+    pv = fmax(pv, -alpha1[c] * sqrt(a1));
+    pv = fmax(pv, -alpha2[c] * sqrt(a2));
+    pv = fmax(pv, -alpha3[c] * sqrt(a9));
+    p_visc[c] = pv;
+    R ddx = dxb(ix), ddy = dyb(iy), ddz = dzb(iz);
+    R vh = -R(0.25) * ddy * ddz * alpha1[c] * a1 - R(0.25) * ddx * ddz * alpha2[c] * a2 -
+           R(0.25) * ddy * ddz * alpha1[c + Y] * a3 - R(0.25) * ddx * ddz * alpha2[c - X] * a4 -
+           R(0.25) * ddy * ddz * alpha1[c + Z] * a5 - R(0.25) * ddx * ddz * alpha2[c + Z] * a6 -
+           R(0.25) * ddy * ddz * alpha1[c + Y + Z] * a7 - R(0.25) * ddx * ddz * alpha2[c - X + Z] * a8 -
+           R(0.25) * ddx * ddy * alpha3[c] * a9 - R(0.25) * ddx * ddy * alpha3[c - X] * a10 -
+           R(0.25) * ddx * ddy * alpha3[c - X - Y] * a11 - R(0.25) * ddx * ddy * alpha3[c - Y] * a12;
+    visc_heat[c] = vh / cv[c];
+    if (ix <= nx && iy <= ny && iz <= nz) {
+      R b1 = alpha1[c + Y + Z] * dyc(iy) * dzc(iz);
+      R b2 = alpha1[c + X + Y + Z] * dyc(iy) * dzc(iz);
+      R b3 = alpha2[c + Z] * dxc(ix) * dzc(iz);
+      R b4 = alpha2[c + Y + Z] * dxc(ix) * dzc(iz);
+      R b5 = alpha3[c] * dxc(ix) * dyc(iy);
+      R b6 = alpha3[c + Z] * dxc(ix) * dyc(iy);
+      R cvv = cv_v[c];
+      auto f = [&](const R* v) {
+        R v0 = v[c];
+        return (b1 * (v0 - v[c - X]) + b2 * (v0 - v[c + X]) + b3 * (v0 - v[c - Y]) + b4 * (v0 - v[c + Y]) +
+                b5 * (v0 - v[c - Z]) + b6 * (v0 - v[c + Z])) / cvv;
+      };
+      fxv[c] = f(vx);
+      fyv[c] = f(vy);
+      fzv[c] = f(vz);
+    }
+  });
+}
+
+// ---------------------------------------------------------------------
+// lagran.F90:1070-1166 set_dt, on the device.
+template <class R>
+void set_dt(Run<R>& run) {
+  const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
+  const int sx = run.sx, sxy = run.sxy;
+  double* sc = run.sc;
+  unsigned long long* us = run.us;
+  if (run.set_dt_first) {
+    run.set_dt_first = false;
+    if (run.p.restart) {
+      const double d = run.p.dt_from_restart;
+      launch_scalar(run.s, run.launches, [=] __device__() {
+        sc[SC_DT] = d;
+        sc[SC_DT2] = 0.5 * d;
+      });
+      return;
+    }
+  }
+  Arrays<R>& A = run.a;
+  const R* bx = A.bx.p;
+  const R* by = A.by.p;
+  const R* bz = A.bz.p;
+  const R* rho = A.rho.p;
+  const R* pressure = A.pressure.p;
+  const R* p_visc = A.p_visc.p;
+  const R* vx = A.vx.p;
+  const R* vy = A.vy.p;
+  const R* vz = A.vz.p;
+  const R* eta = A.eta.p;
+  R* const gamma_boris = A.gamma_boris.p;
+  auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb;
+  const bool boris = run.p.boris != 0, resistive = run.p.resistive_mhd != 0;
+  const R g = (R)run.p.gamma;
+  const R va_max2 = (R)run.p.va_max * (R)run.p.va_max;
+  if (!run.gamma_boris_one || boris) {
+    whole(run, [=] __device__(int i, int j, int k) {
+      if (i >= -1 && j >= -1 && k >= -1) gamma_boris[i + sx * j + sxy * k] = R(1);
+    });
+    run.gamma_boris_one = !boris;
+  }
+  launch_scalar(run.s, run.launches, [=] __device__() {
+    us[U_DTMIN] = (unsigned long long)__double_as_longlong(DBL_MAX);
+    us[U_DTRMIN] = (unsigned long long)__double_as_longlong(DBL_MAX);
+  });
+  box_min<2>(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz, double* v) {
+    const int c = ix + sx * iy + sxy * iz;
+    R w1 = bx[c] * bx[c] + by[c] * by[c] + bz[c] * bz[c];
+    R rho0 = fmax(rho[c], Num<R>::tiny());
+    R w2 = w1 / rho0;
+    R gb = gamma_boris[c];
+    if (boris && (w2 >= va_max2)) {
+      gb = R(1) / (R(1) + w2 / va_max2);
+      gamma_boris[c] = gb;
+    }
+    R cs2 = (g * pressure[c] + gb * w1) / rho0;
+    R c_visc2 = p_visc[c] / rho0;
+    R length = fmin(fmin(dxb(ix), dyb(iy)), dzb(iz));
+    R dt1 = length / (sqrt(c_visc2) + sqrt(cs2 + c_visc2));
+    R dt_local = fmin(Num<R>::huge(), dt1);
+    R dt2 = fmin(fmin(dxb(ix) / fmax(fabs(vx[c]), Num<R>::tiny()), dyb(iy) / fmax(fabs(vy[c]), Num<R>::tiny())),
+                 dzb(iz) / fmax(fabs(vz[c]), Num<R>::tiny()));
+    dt_local = fmin(dt_local, dt2);
+    R dt3 = Num<R>::huge();
+    if (resistive) {
+      R dxlocal = R(1) / (R(1) / (dxb(ix) * dxb(ix)) + R(1) / (dyb(iy) * dyb(iy)) + R(1) / (dzb(iz) * dzb(iz)));
+      dt3 = R(0.2) * dxlocal / fmax(eta[c], Num<R>::tiny());
+    }
+    v[0] = (double)dt_local;
+    v[1] = (double)dt3;
+  }, U_DTMIN);
+  const double mult = run.p.dt_multiplier;
+  const bool f32 = sizeof(R) == 4;
+  launch_scalar(run.s, run.launches, [=] __device__() {
+    double dtm = __longlong_as_double((long long)us[U_DTMIN]);
+    double dtrm = __longlong_as_double((long long)us[U_DTRMIN]);
+    if (f32) {
+      dtm = fmin(dtm, (double)FLT_MAX);
+      dtrm = fmin(dtrm, (double)FLT_MAX);
+    }
+    sc[SC_DT] = mult * dtm;
+    sc[SC_DTR] = mult * dtrm;
+  });
+  if (run.p.conduction) {
+    calc_s_stages(run, SC_DT);
+    launch_scalar(run.s, run.launches, [=] __device__() {
+      const double ss_limit = 60;
+      int ns = (int)sc[SC_STAGES];
+      if (ns >= ss_limit) {
+        double f1 = 2.0 * ss_limit * ss_limit - 9.0;
+        double f2 = (double)(2 * ns * ns - 9);
+        sc[SC_DT] = sc[SC_DT] * f1 / f2;
+        sc[SC_DTR] = sc[SC_DTR] * f1 / f2;
+      }
+    });
+  }
+  launch_scalar(run.s, run.launches, [=] __device__() {
+    sc[SC_TIME] = sc[SC_TIME] + sc[SC_DT];
+    sc[SC_DT2] = 0.5 * sc[SC_DT];
+  });
+}
+
+// ---------------------------------------------------------------------
+// The predictor's B-only remap (b_field_and_cv1_update, lagran.F90:1050-
+// 1060): B * area is written to the bx0 buffers, which then serve as B for
+// the three half-dt sweeps, the back-conversion and bfield_bcs.  On return
+// run.a.bx holds the predicted B and run.a.bx0 the untouched B of the step.
+template <class R>
+void predictor_remap(Run<R>& run, int step) {
+  const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
+  const int sx = run.sx, sxy = run.sxy;
+  Arrays<R>& A = run.a;
+  const R* bx = A.bx.p;
+  const R* by = A.by.p;
+  const R* bz = A.bz.p;
+  R* const px = A.bx0.p;
+  R* const py = A.by0.p;
+  R* const pz = A.bz0.p;
+  auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb;
+  LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
+    const int c = ix + sx * iy + sxy * iz;
+    if (iy >= -1 && iz >= -1) px[c] = bx[c] * dyb(iy) * dzb(iz);
+    if (ix >= -1 && iz >= -1) py[c] = by[c] * dxb(ix) * dzb(iz);
+    if (ix >= -1 && iy >= -1) pz[c] = bz[c] * dxb(ix) * dyb(iy);
+  });
+  std::swap(A.bx.p, A.bx0.p);
+  std::swap(A.by.p, A.by0.p);
+  std::swap(A.bz.p, A.bz0.p);
+  // vx1 = vx (lagran.F90:1051-1053): the sweeps read v itself
+  R* const keep[3] = {A.vx1.p, A.vy1.p, A.vz1.p};
+  A.vx1.p = A.vx.p;
+  A.vy1.p = A.vy.p;
+  A.vz1.p = A.vz.p;
+  static const int order[6][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}, {0, 2, 1}, {2, 1, 0}, {1, 0, 2}};
+  int cse = ((step % 6) + 6) % 6;
+  int pass[3] = {1, 1, 1};
+  for (int s = 0; s < 3; ++s) {
+    switch (order[cse][s]) {
+      case 0: remap_sweep<0>(run, true, SC_DT2, pass); break;
+      case 1: remap_sweep<1>(run, true, SC_DT2, pass); break;
+      default: remap_sweep<2>(run, true, SC_DT2, pass); break;
+    }
+  }
+  A.vx1.p = keep[0];
+  A.vy1.p = keep[1];
+  A.vz1.p = keep[2];
+  R* const qx = A.bx.p;
+  R* const qy = A.by.p;
+  R* const qz = A.bz.p;
+  LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
+    const int c = ix + sx * iy + sxy * iz;
+    if (iy >= -1 && iz >= -1) qx[c] = qx[c] / dyb(iy) / dzb(iz);
+    if (ix >= -1 && iz >= -1) qy[c] = qy[c] / dxb(ix) / dzb(iz);
+    if (ix >= -1 && iy >= -1) qz[c] = qz[c] / dxb(ix) / dyb(iy);
+  });
+  bfield_bcs(run);
+}
+
+// ---------------------------------------------------------------------
+// lagran.F90:208-478 predictor_corrector_step (non-CAUCHY, no cooling),
+// including the energy0 + delta_energy / MAX(energy, 0) of :180-181.
+template <class R>
+void predictor_corrector_step(Run<R>& run) {
+  const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
+  const int sx = run.sx, sxy = run.sxy;
+  Arrays<R>& A = run.a;
+  predictor_remap(run, run.cur_step);
+  // PC1 (-1:n+2): energy = MAX(energy0 + delta, 0); predictor pressure (0:n+1)
+  R* const energy = A.energy.p;
+  const R* energy0 = A.energy0.p;
+  R* const pressure = A.pressure.p;
+  const R* cv1 = A.cv1.p;
+  const R* cv = A.cv.p;
+  const R* rho = A.rho.p;
+  const R* visc_heat = A.visc_heat.p;
+  const bool cond = run.p.conduction != 0;
+  const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
+  const double* sc = run.sc;
+  LARE_BOXW(run, 8, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+    const int c = ix + sx * iy + sxy * iz;
+    R e;
+    if (cond) {
+      R e0 = energy0[c];
+      R d = energy[c] - e0;
+      e = e0 + d;
+    } else {
+      e = energy[c] + R(0);
+    }
+    e = e > R(0) ? e : R(0);
+    energy[c] = e;
+    if (ix >= 0 && ix <= nx + 1 && iy >= 0 && iy <= ny + 1 && iz >= 0 && iz <= nz + 1) {
+      const R dt2 = (R)sc[SC_DT2];
+      R dv = cv1[c] / cv[c] - R(1);
+      R e1 = e - pressure[c] * dv / rho[c];
+      e1 = e1 + visc_heat[c] * dt2 / rho[c];
+      pressure[c] = (e1 - (R(1) - xi) * ip) * (g - R(1)) * rho[c] * cv[c] / cv1[c];
+    }
+  });
+  // PC2 (0:n): vertex forces with the predicted B; half-step velocity
+  const R* bx = A.bx.p;  // predicted B
+  const R* by = A.by.p;
+  const R* bz = A.bz.p;
+  const R* gamma_boris = A.gamma_boris.p;
+  const R* rho_v = A.rho_v.p;
+  R* const vx = A.vx.p;
+  R* const vy = A.vy.p;
+  R* const vz = A.vz.p;
+  R* const vx1 = A.vx1.p;
+  R* const vy1 = A.vy1.p;
+  R* const vz1 = A.vz1.p;
+  const R* fxv = A.fx_visc.p;
+  const R* fyv = A.fy_visc.p;
+  const R* fzv = A.fz_visc.p;
+  auto dxc = A.dxc, dyc = A.dyc, dzc = A.dzc, grav = A.grav;
+  LARE_BOXW(run, 17, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+    const R dt2 = (R)sc[SC_DT2];
+    const int c = ix + sx * iy + sxy * iz;
+    const int X = 1, Y = sx, Z = sxy;
+    R pp = pressure[c], ppx = pressure[c + X], ppy = pressure[c + Y];
+    R ppz = pressure[c + Z], ppxy = pressure[c + X + Y], ppxz = pressure[c + X + Z];
+    R ppyz = pressure[c + Y + Z], ppxyz = pressure[c + X + Y + Z];
+    R w1 = (pp + ppy + ppz + ppyz) * R(0.25);
+    R w2 = (ppx + ppxy + ppxz + ppxyz) * R(0.25);
+    R fx = -(w2 - w1) / dxc(ix);
+    w1 = (pp + ppx + ppz + ppxz) * R(0.25);
+    w2 = (ppy + ppxy + ppyz + ppxyz) * R(0.25);
+    R fy = -(w2 - w1) / dyc(iy);
+    w1 = (pp + ppx + ppy + ppxy) * R(0.25);
+    w2 = (ppz + ppxz + ppyz + ppxyz) * R(0.25);
+    R fz = -(w2 - w1) / dzc(iz);
+    R bxv = R(0.25) * (bx[c] + bx[c + Y] + bx[c + Z] + bx[c + Y + Z]);
+    R byv = R(0.25) * (by[c] + by[c + X] + by[c + Z] + by[c + X + Z]);
+    R bzv = R(0.25) * (bz[c] + bz[c + Y] + bz[c + X] + bz[c + X + Y]);
+    R jx, jy, jz;
+    vertex_current<R>(bx, by, bz, c, sx, sxy, dxc(ix), dyc(iy), dzc(iz), jx, jy, jz);
+    R gb = gamma_boris[c];
+    fx = fx + gb * (jy * bzv - jz * byv);
+    fy = fy + gb * (jz * bxv - jx * bzv);
+    fz = fz + gb * (jx * byv - jy * bxv);
+    R rv = rho_v[c];
+    fz = fz - rv * grav(iz);
+    vx1[c] = vx[c] + dt2 * (fxv[c] + fx) / rv;
+    vy1[c] = vy[c] + dt2 * (fyv[c] + fy) / rv;
+    vz1[c] = vz[c] + dt2 * (fzv[c] + fz) / rv;
+  });
+  // B = B0 (:389-393)
+  std::swap(A.bx.p, A.bx0.p);
+  std::swap(A.by.p, A.by0.p);
+  std::swap(A.bz.p, A.bz0.p);
+  remap_v_bcs(run);
+  // PC3: shock_heating (0:n+1) and v = 2 v1 - v (0:n) into the q buffers
+  const R* alpha1 = A.alpha1.p;
+  const R* alpha2 = A.alpha2.p;
+  const R* alpha3 = A.alpha3.p;
+  R* const vhp = A.visc_heat.p;
+  R* const nvx = A.qx.p;
+  R* const nvy = A.qy.p;
+  R* const nvz = A.qz.p;
+  auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb;
+  LARE_BOXW(run, 14, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
+    const int c = ix + sx * iy + sxy * iz;
+    const int X = 1, Y = sx, Z = sxy;
+    auto dd = [&](int p0, int p1) {
+      return (vx[p0] - vx[p1]) * (vx1[p0] - vx1[p1]) + (vy[p0] - vy[p1]) * (vy1[p0] - vy1[p1]) +
+             (vz[p0] - vz[p1]) * (vz1[p0] - vz1[p1]);
+    };
+    R a1 = dd(c - X - Y - Z, c - Y - Z);
+    R a2 = dd(c - Y - Z, c - Z);
+    R a3 = dd(c - Z, c - X - Z);
+    R a4 = dd(c - X - Z, c - X - Y - Z);
+    R a5 = dd(c - X - Y, c - Y);
+    R a6 = dd(c - Y, c);
+    R a7 = dd(c, c - X);
+    R a8 = dd(c - X, c - X - Y);
+    R a9 = dd(c - Z, c);
+    R a10 = dd(c - X - Z, c - X);
+    R a11 = dd(c - X - Y - Z, c - X - Y);
+    R a12 = dd(c - Y - Z, c - Y);
+    R ddx = dxb(ix), ddy = dyb(iy), ddz = dzb(iz);
+    R vh = -R(0.25) * ddy * ddz * alpha1[c] * a1 - R(0.25) * ddx * ddz * alpha2[c] * a2 -
+           R(0.25) * ddy * ddz * alpha1[c + Y] * a3 - R(0.25) * ddx * ddz * alpha2[c - X] * a4 -
+           R(0.25) * ddy * ddz * alpha1[c + Z] * a5 - R(0.25) * ddx * ddz * alpha2[c + Z] * a6 -
+           R(0.25) * ddy * ddz * alpha1[c + Y + Z] * a7 - R(0.25) * ddx * ddz * alpha2[c - X + Z] * a8 -
+           R(0.25) * ddx * ddy * alpha3[c] * a9 - R(0.25) * ddx * ddy * alpha3[c - X] * a10 -
+           R(0.25) * ddx * ddy * alpha3[c - X - Y] * a11 - R(0.25) * ddx * ddy * alpha3[c - Y] * a12;
+    R v = vh / cv[c];
+    vhp[c] = v > R(0) ? v : R(0);
+    if (ix <= nx && iy <= ny && iz <= nz) {
+      nvx[c] = R(2) * vx1[c] - vx[c];
+      nvy[c] = R(2) * vy1[c] - vy[c];
+      nvz[c] = R(2) * vz1[c] - vz[c];
+    }
+  });
+  std::swap(A.vx.p, A.qx.p);
+  std::swap(A.vy.p, A.qy.p);
+  std::swap(A.vz.p, A.qz.p);
+  velocity_bcs(run);
+  // PC4 (1:n): final cv1, energy, visc_dep, rho; total_visc_heating
+  R* const cv1w = A.cv1.p;
+  R* const rhow = A.rho.p;
+  R* const visc_dep = A.visc_dep.p;
+  box_sum<1>(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
+    const R dt = (R)sc[SC_DT];
+    const int c = ix + sx * iy + sxy * iz;
+    const int X = 1, Y = sx, Z = sxy;
+    R vxb = (vx1[c] + vx1[c - Y] + vx1[c - Z] + vx1[c - Y - Z]) * R(0.25);
+    R vxbm = (vx1[c - X] + vx1[c - X - Y] + vx1[c - X - Z] + vx1[c - X - Y - Z]) * R(0.25);
+    R vyb = (vy1[c] + vy1[c - X] + vy1[c - Z] + vy1[c - X - Z]) * R(0.25);
+    R vybm = (vy1[c - Y] + vy1[c - X - Y] + vy1[c - Y - Z] + vy1[c - X - Y - Z]) * R(0.25);
+    R vzb = (vz1[c] + vz1[c - X] + vz1[c - Y] + vz1[c - X - Y]) * R(0.25);
+    R vzbm = (vz1[c - Z] + vz1[c - X - Z] + vz1[c - Y - Z] + vz1[c - X - Y - Z]) * R(0.25);
+    R dv = ((vxb - vxbm) / dxb(ix) + (vyb - vybm) / dyb(iy) + (vzb - vzbm) / dzb(iz)) * dt;
+    cv1w[c] = cv[c] * (R(1) + dv);
+    R vh = vhp[c];
+    R r = rhow[c];
+    energy[c] = energy[c] + (dt * vh - dv * pressure[c]) / r;
+    visc_dep[c] = visc_dep[c] + dt * vh;
+    rhow[c] = r / (R(1) + dv);
+    v[0] = (double)(dt * vh * cv[c]);
+  }, SC_VISC_TOT, true);
+}
+
+// ---------------------------------------------------------------------
+// lagran.F90:50-200 lagrangian_step
+template <class R>
+int lagrangian_step(Run<R>& run, int step) {
+  run.cur_step = step;
+  prologue_and_shock_viscosity(run);
+  set_dt(run);
+  double* sc = run.sc;
+  run.last_substeps = 0;
+  if (run.p.resistive_mhd) {
+    launch_scalar(run.s, run.launches, [=] __device__() {
+      double dt = sc[SC_DT];
+      int substeps = (int)(dt / sc[SC_DTR]) + 1;
+      sc[SC_SUBSTEPS] = (double)substeps;
+      sc[SC_DTSUB] = dt / (double)substeps;
+    });
+    if (pull_scalars(run) != cudaSuccess) return LARE_ECUDA;
+    int substeps = (int)run.host_sc[SC_SUBSTEPS];
+    double dtv = run.host_sc[SC_DT];
+    if (!(dtv > 0.0) || !std::isfinite(dtv)) return LARE_EDT;
+    if (substeps < 1 || substeps > 1000000) return LARE_EDT;
+    if (substeps > run.peak_substeps) run.peak_substeps = substeps;
+    run.last_substeps = substeps;
+    for (int i = 1; i <= substeps; ++i) {
+      eta_and_rkstep(run, true);
+      resistive_update(run);
+    }
+    // The cell B averages recomputed at :152-163 only feed the CAUCHY branch.
+  }
+  if (run.p.conduction) {
+    copy_whole(run, run.a.energy0, run.a.energy);
+    calc_s_stages(run, SC_DT);
+    if (pull_scalars(run) != cudaSuccess) return LARE_ECUDA;
+    int ns = (int)run.host_sc[SC_STAGES];
+    if (ns < 1 || ns > 100000) return LARE_ESTAGES;
+    run.n_s_stages = ns;
+    heat_conduct_sts2(run, SC_DT);
+  }
+  predictor_corrector_step(run);
+  end_of_step_bcs(run);
+  ++run.steps_taken;
+  return LARE_OK;
+}
+
+}  // namespace lare

@@ -32,6 +32,10 @@ int lare_gpu_init(const lare_params* p, int nx, int ny, int nz, const double* dx
   const int bcs[6] = {p->xbc_min, p->xbc_max, p->ybc_min, p->ybc_max, p->zbc_min, p->zbc_max};
   for (int q = 0; q < 6; ++q)
     if (!bc_supported(bcs[q])) return LARE_EINVAL;  // BC_OPEN (openboundary.f90) is not on this path
+  // A periodic boundary needs both sides periodic: the reference leaves the
+  // ghosts of a half-periodic direction unset (mpi_routines.F90:195-210).
+  for (int d = 0; d < 3; ++d)
+    if ((bcs[2 * d] == LARE_BC_PERIODIC) != (bcs[2 * d + 1] == LARE_BC_PERIODIC)) return LARE_EINVAL;
   if (!(p->gamma > 1.0) || !(p->dt_multiplier > 0.0)) return LARE_EINVAL;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return LARE_ECUDA;
