@@ -166,6 +166,81 @@ def time_steps(sim, torch, stream, first, k):
     return e0.elapsed_time(e1) / 1000.0
 
 
+def surrogate_form(torch, cdeck, plain):
+    """The learned conduction step at 256^3 (FP32 state) against plain FP32
+    RKL2 from the same state, with the committed trained weights."""
+    import numpy as np
+    from lare3d_b200 import gpu
+    from lare3d_b200 import surrogate as S
+    if not os.path.exists(S.DEFAULT_WEIGHTS):
+        return {"unavailable": "no trained weights (python -m lare3d_b200.surrogate)"}
+    net = S.Network(seed=0)
+    net.load(S.DEFAULT_WEIGHTS)
+    dt = net.meta["dt"]
+    n = cdeck.nx
+    n3 = n ** 3
+    ref = gpu.simulation(cdeck, precision=32)
+    ref.start(cdeck.state)
+    e_start = ref.get_field("energy")
+    stages = ref.conduct_heat(dt)
+    g = (cdeck.params.gamma - 1.0) / (2.0 - cdeck.params.xi_n)
+    T_ref = g * ref.get_field("energy")[2:-2, 2:-2, 2:-2]
+    T_0 = g * e_start[2:-2, 2:-2, 2:-2]
+    # plain RKL2 at the surrogate's dt, timed the same way
+    stp = torch.cuda.ExternalStream(gpu.stream_of(ref))
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a0.record(stp)
+    for _ in range(3):
+        ref.conduct_heat(dt)
+    a1.record(stp)
+    a1.synchronize()
+    t_plain = a0.elapsed_time(a1) / 1000.0 / 3
+    ref.close()
+    sim = gpu.simulation(cdeck, precision=32)
+    sim.start(cdeck.state)
+    sc = S.SurrogateConduction(sim, cdeck, net, dt, bound=1e-3, col=64, seed=0)
+    info = sc.step()
+    T_sur = g * sim.get_field("energy")[2:-2, 2:-2, 2:-2]
+    rel = np.abs(T_sur - T_ref) / np.abs(T_ref)
+    rel0 = np.abs(T_0 - T_ref) / np.abs(T_ref)
+    st = torch.cuda.ExternalStream(sc.stream)
+    times = {}
+    for chk in (True, False):
+        sc.check = chk
+        sim.set_field("energy", e_start)
+        sim.boundary_conditions()
+        torch.cuda.synchronize()
+        a0.record(st)
+        for _ in range(3):
+            sc.step()
+        a1.record(st)
+        a1.synchronize()
+        times[chk] = a0.elapsed_time(a1) / 1000.0 / 3
+    a0.record(st)
+    net.forward(sc.bufs, sc.nb)
+    a1.record(st)
+    a1.synchronize()
+    t_fwd = a0.elapsed_time(a1) / 1000.0
+    d = sc.bufs["d"]
+    flops = sum(2 * 27 * cin * cf * d[l + 1] ** 3 * sc.nb for l, (cin, _c, _r, cf) in enumerate(S.LAYERS))
+    sc.close()
+    sim.close()
+    out = {"value": n3 / times[True], "unit": "cell-updates/s (one conduction step incl. 1/16 re-check)",
+           "ms_per_step": 1e3 * times[True], "ms_per_step_no_recheck": 1e3 * times[False],
+           "plain_rkl2_fp32_ms_same_dt": 1e3 * t_plain, "speedup_vs_plain_rkl2": t_plain / times[True],
+           "stages": stages, "network_forward_ms": 1e3 * t_fwd,
+           "network_tflops": flops / t_fwd / 1e12, "network_flops_per_step": flops,
+           "rel_T_err_vs_rkl2": {"rms": float(np.sqrt(np.mean(rel ** 2))), "max": float(rel.max()),
+                                 "frac_cells_over_1e-3": float(np.mean(rel > 1e-3))},
+           "rel_T_err_without_network": {"rms": float(np.sqrt(np.mean(rel0 ** 2))), "max": float(rel0.max()),
+                                         "frac_cells_over_1e-3": float(np.mean(rel0 > 1e-3))},
+           "recheck": {"patches": info.checked, "rejected": info.rejected, "max_err": info.max_err,
+                       "fallback": info.fallback},
+           "weights": os.path.relpath(S.DEFAULT_WEIGHTS, ROOT)}
+    return out
+
+
 def run_reference(args):
     ws, rank, _ = dist_setup(args)
     if rank != 0:
@@ -320,6 +395,7 @@ def main():
                                                   "ms_per_substep": 1e3 * elc, "stages": ns,
                                                   "dt_over_dt_parab": cdeck.info["dt_ratio"]}
             sc.close()
+        forms["surrogate_conduction"] = surrogate_form(torch, cdeck, forms.get("conduction_rkl2_fp32"))
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

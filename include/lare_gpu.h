@@ -157,6 +157,22 @@ int lare_gpu_run(lare_ctx* ctx, int first_step, int nsteps, double t_end,
 int lare_gpu_conduct_heat(lare_ctx* ctx, double dt, int* n_stages);
 
 /*
+ * The same RKL2 step with the stage count s given (s >= 2) instead of taken
+ * from calc_s_stages.  No counterpart in the reference: it lets a
+ * sub-domain copy of a grid repeat a step of the whole grid exactly (the
+ * learned-conduction re-check runs plain RKL2 on windows this way).
+ */
+int lare_gpu_conduct_heat_stages(lare_ctx* ctx, double dt, int n_stages);
+
+/*
+ * conduct.f90:56-143 calc_s_stages alone: the RKL2 stage count s that
+ * lare_gpu_conduct_heat would use for dt on the current state (it also
+ * refreshes the temperature and larsen_factor arrays).  No counterpart as a
+ * separate call in the reference.
+ */
+int lare_gpu_conduction_stages(lare_ctx* ctx, double dt, int* n_stages);
+
+/*
  * diagnostics.F90:517 energy_account: out[0..4] = en_b, en_ke, en_int,
  * total_visc_heating, total_ohmic_heating (the en.dat record, :79-83), FP64.
  */
@@ -210,6 +226,17 @@ int lare_gpu_set_field(lare_ctx* ctx, const char* name, const double* host);
 
 /* Bounds of a named array: lo[3], hi[3] (Fortran, inclusive). */
 int lare_gpu_field_bounds(lare_ctx* ctx, const char* name, int lo[3], int hi[3]);
+
+/*
+ * Device address of a named array, for kernels that work on the resident
+ * state in place (no counterpart in the reference).  Element (i, j, k), in
+ * Fortran indices from -2 up, is origin[i + sx*j + sxy*k] (origin is the
+ * address of (0, 0, 0)); elem_bytes is 8 for the FP64 engine and 4 for FP32.
+ * Some arrays are double-buffered, so the address is valid only until the
+ * next call that advances the state; after writing through it, call
+ * lare_gpu_boundary_conditions before the next step.
+ */
+int lare_gpu_field_device(lare_ctx* ctx, const char* name, void** origin, int* sx, int* sxy, int* elem_bytes);
 
 int lare_gpu_get_scalars(lare_ctx* ctx, lare_scalars* out);
 

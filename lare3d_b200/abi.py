@@ -215,6 +215,11 @@ class Binding:
         de = getattr(lib, prefix + "destroy")
         de.argtypes = [C.c_void_p]
         de.restype = None
+        if hasattr(lib, prefix + "field_device"):
+            f("conduct_heat_stages", [C.c_void_p, C.c_double, C.c_int])
+            f("conduction_stages", [C.c_void_p, C.c_double, C.POINTER(C.c_int)])
+            f("field_device", [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int),
+                               C.POINTER(C.c_int), C.POINTER(C.c_int)])
         if hasattr(lib, prefix + "run"):
             f("run", [C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_int), dp, dp])
         if hasattr(lib, prefix + "launch_count"):
@@ -329,6 +334,21 @@ class Simulation:
         s = C.c_int()
         self.b.call(self.ctx, "conduct_heat", C.c_double(dt), C.byref(s))
         return s.value
+
+    def conduct_heat_stages(self, dt, n_stages):
+        self.b.call(self.ctx, "conduct_heat_stages", C.c_double(dt), int(n_stages))
+
+    def conduction_stages(self, dt):
+        s = C.c_int()
+        self.b.call(self.ctx, "conduction_stages", C.c_double(dt), C.byref(s))
+        return s.value
+
+    def field_device(self, name):
+        """(device address of Fortran element (0,0,0), sx, sxy, element bytes)."""
+        o = C.c_void_p()
+        sx, sxy, eb = C.c_int(), C.c_int(), C.c_int()
+        self.b.call(self.ctx, "field_device", name.encode(), C.byref(o), C.byref(sx), C.byref(sxy), C.byref(eb))
+        return int(o.value or 0), sx.value, sxy.value, eb.value
 
     def energy(self):
         out = (C.c_double * 5)()

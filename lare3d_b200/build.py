@@ -1,6 +1,7 @@
 """In-tree build of the native libraries.
 
-* ``liblare_gpu.so``  - sm_100a CUDA engine + C ABI (include/lare_gpu.h)
+* ``liblare_gpu.so``  - sm_100a CUDA engine + C ABI (include/lare_gpu.h) and
+  the learned-conduction kernels (include/lare_surrogate.h)
 * ``liblare_host.so`` - host helpers of the deck layer (KISS generator)
 
 Run ``python -m lare3d_b200.build``.  Object files go to ``_build/`` and the
@@ -32,6 +33,7 @@ UNITS = [
     ("engine_f32.cu", ["--fmad=true"]),
     ("lare_gpu.cu", []),
     ("lare_noalloc.cu", ["--fmad=false"]),
+    ("surrogate.cu", []),
 ]
 
 
@@ -50,7 +52,7 @@ def _newer(target, deps):
 
 
 def _deps():
-    out = [os.path.join(ROOT, "include", "lare_gpu.h")]
+    out = [os.path.join(ROOT, "include", h) for h in ("lare_gpu.h", "lare_surrogate.h")]
     for f in os.listdir(CSRC):
         if f.endswith((".cuh", ".h", ".cu")):
             out.append(os.path.join(CSRC, f))

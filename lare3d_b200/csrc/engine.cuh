@@ -5,8 +5,10 @@
 // same index box, with the same left-to-right expression order.  Compiled
 // with --fmad=false for FP64 (engine_f64.cu) the arithmetic is then
 // bit-for-bit that of a gfortran -O3 x86-64 build of the reference, which
-// emits no FMA; pow() (conduction only) is the one call whose last bit may
-// differ.  engine_f32.cu instantiates the same code in FP32 (the FP32 form).
+// emits no FMA.  Conduction is the exception: it forms T^2.5 and T^1.5 as
+// T*T*sqrt(T) and T*sqrt(T) where the reference calls pow(), so its results
+// differ in the last bits.  engine_f32.cu instantiates the same code in FP32
+// (the FP32 form).
 //
 // All routines are free functions over Run<R>&; kernels capture only local
 // copies of array handles and scalars (a capture of `run` itself fails to
@@ -48,9 +50,11 @@ struct Arrays {
   A3<R> db1, dc1, r_rho_v, r_rho_v1, rho1, dm, cv2, flux;
   A3<R> f1, f2, rho_alt, cv1v, cv2v, dmv, mfx, mfy, mfz;
   // conduct.f90 temporaries
-  A3<R> larsen, c_flux, Y0, Y1, Y2, Y3, Lc_Y0;
+  A3<R> larsen, Y1, Y2, Y3, Lc_Y0;  // RKL2 (Y0 is read from energy itself)
   // 1-D metrics (pointers at Fortran index 0)
   A1<R> dxb, dxc, dyb, dyc, dzb, dzc, grav;
+  // reciprocals for conduction: 1/dxb, 1/dxc, 1/(dxc(i) + dxc(i-1)), per axis
+  A1<R> rdb[3], rdc[3], rdc2[3];
 };
 
 enum Stag { ST_C = 0, ST_N = 1, ST_F = 2 };
@@ -328,6 +332,14 @@ __device__ __forceinline__ R edge_viscosity(R dvdots, R r1, R r2, R c1, R c2, R 
 }
 
 // ---------------------------------------------------------------------
+// x^2.5 and x^1.5 as x*x*sqrt(x) and x*sqrt(x): within an ulp or two of
+// pow() and several times cheaper (the reference calls pow, so conduction is
+// compared with the oracle at a 1e-12 relative tolerance, not bitwise).
+template <class R>
+__device__ __forceinline__ R pow25(R x) { return x * x * sqrt(x); }
+template <class R>
+__device__ __forceinline__ R pow15(R x) { return x * sqrt(x); }
+
 // conduct.f90:56-143 calc_s_stages.  Produces larsen_factor and the stage
 // count in sc[SC_STAGES] from the dt in sc[dt_slot].
 template <class R>
@@ -345,8 +357,8 @@ void calc_s_stages(Run<R>& run, int dt_slot) {
     if (!limiter) { larsen(ix, iy, iz) = R(1); return; }
     int ixm = ix - 1, ixp = ix + 1, iym = iy - 1, iyp = iy + 1, izm = iz - 1, izp = iz + 1;
     R T = temperature(ix, iy, iz);
-    R temp = pow(T, R(2.5));
-    R q_fs = fl * R(42.85) * rho(ix, iy, iz) * pow(T, R(1.5));
+    R temp = pow25(T);
+    R q_fs = fl * R(42.85) * rho(ix, iy, iz) * pow15(T);
     R q_fs2 = q_fs * q_fs;
     R q_spx = -k0 * temp * (temperature(ixp, iy, iz) - temperature(ixm, iy, iz)) * R(0.5) / dxb(ix);
     R q_spy = -k0 * temp * (temperature(ix, iyp, iz) - temperature(ix, iym, iz)) * R(0.5) / dyb(iy);
@@ -359,7 +371,7 @@ void calc_s_stages(Run<R>& run, int dt_slot) {
   box_min<1>(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
     R kappa1 = k0 * larsen(ix, iy, iz);
     R temp = (g - R(1)) / (R(2) - xi) * (energy(ix, iy, iz) - (R(1) - xi) * ip);
-    R tp = pow(temp, R(2.5));
+    R tp = pow25(temp);
     R r = rho(ix, iy, iz);
     R dt1 = r * (dxb(ix) * dxb(ix)) / (R(2) * kappa1 * tp);
     R dt2 = r * (dyb(iy) * dyb(iy)) / (R(2) * kappa1 * tp);
@@ -388,6 +400,15 @@ void calc_s_stages(Run<R>& run, int dt_slot) {
   });
 }
 
+// Temperature of an energy-like array, conduct.f90:68 and :371-374,
+// evaluated where it is needed instead of stored.
+template <class R>
+struct TempOf {
+  A3<R> y;
+  R c, e0;  // (gamma - 1)/(2 - xi_n), (1 - xi_n)*ionise_pot
+  __device__ __forceinline__ R operator()(int i, int j, int k) const { return c * (y(i, j, k) - e0); }
+};
+
 // conduct.f90:152-291 heat_flux as a gather.  The reference scatters each
 // cell's three face fluxes into flux(c) and flux(c+e); for cell c the
 // contributions therefore arrive in loop order as
@@ -396,15 +417,20 @@ void calc_s_stages(Run<R>& run, int dt_slot) {
 // (i,j,k)), which this kernel reproduces term for term, with no atomics.
 template <class R>
 struct HeatFluxArgs {
-  A3<R> T, bx, by, bz, larsen;
-  A1<R> dxb, dyb, dzb, dxc, dyc, dzc;
+  TempOf<R> T;
+  A3<R> bx, by, bz, larsen;
+  A1<R> rdb[3], rdc[3], rdc2[3];
   R k0;
 };
 
-template <class R>
-__device__ __forceinline__ R face_flux(const HeatFluxArgs<R>& h, int axis, int ix, int iy, int iz) {
+// One face flux of conduct.f90:170-275, divided by the cell width dxb of the
+// face's index (the factor heat_flux applies when it scatters the flux).
+// Divisions by metric sums become products with reciprocals and /2 becomes
+// *0.5; only the division by |B|^2 remains.
+template <class R, class TT>
+__device__ __forceinline__ R face_flux(const HeatFluxArgs<R>& h, const TT& T, int axis, int ix, int iy, int iz) {
   const R min_b = R(1.0e-10);  // conduct.f90:28
-  const A3<R>& T = h.T;
+  const R half = R(0.5);
   int ixp = ix + 1, ixm = ix - 1, iyp = iy + 1, iym = iy - 1, izp = iz + 1, izm = iz - 1;
   R lf = h.larsen(ix, iy, iz);
   if (axis == 0) {
@@ -412,59 +438,50 @@ __device__ __forceinline__ R face_flux(const HeatFluxArgs<R>& h, int axis, int i
     R bzf = R(0.25) * (h.bz(ix, iy, iz) + h.bz(ixp, iy, iz) + h.bz(ix, iy, izm) + h.bz(ixp, iy, izm));
     R b0 = h.bx(ix, iy, iz);
     R modb = b0 * b0 + byf * byf + bzf * bzf + min_b;
-    R tb = (T(ixp, iy, iz) + T(ix, iy, iz)) / R(2);
-    R tb_p = (T(ixp, iyp, iz) + T(ix, iyp, iz)) / R(2);
-    R tb_m = (T(ixp, iym, iz) + T(ix, iym, iz)) / R(2);
-    R tg_a1 = (tb_p - tb_m) / (h.dyc(iy) + h.dyc(iym));
-    tb_p = (T(ixp, iy, izp) + T(ix, iy, izp)) / R(2);
-    tb_m = (T(ixp, iy, izm) + T(ix, iy, izm)) / R(2);
-    R tg_a2 = (tb_p - tb_m) / (h.dzc(iz) + h.dzc(izm));
-    R tg = (T(ixp, iy, iz) - T(ix, iy, iz)) / h.dxc(ix);
+    R tb = (T(ixp, iy, iz) + T(ix, iy, iz)) * half;
+    R tb_p = (T(ixp, iyp, iz) + T(ix, iyp, iz)) * half;
+    R tb_m = (T(ixp, iym, iz) + T(ix, iym, iz)) * half;
+    R tg_a1 = (tb_p - tb_m) * h.rdc2[1](iy);
+    tb_p = (T(ixp, iy, izp) + T(ix, iy, izp)) * half;
+    tb_m = (T(ixp, iy, izm) + T(ix, iy, izm)) * half;
+    R tg_a2 = (tb_p - tb_m) * h.rdc2[2](iz);
+    R tg = (T(ixp, iy, iz) - T(ix, iy, iz)) * h.rdc[0](ix);
     tb = tb > R(0) ? tb : R(0);
-    return -lf * h.k0 * pow(tb, R(2.5)) * (b0 * (tg * b0 + tg_a1 * byf + tg_a2 * bzf) + tg * min_b) / modb;
+    return -lf * h.k0 * pow25(tb) * (b0 * (tg * b0 + tg_a1 * byf + tg_a2 * bzf) + tg * min_b) / modb *
+           h.rdb[0](ix);
   } else if (axis == 1) {
     R bxf = R(0.25) * (h.bx(ix, iy, iz) + h.bx(ix, iyp, iz) + h.bx(ixm, iy, iz) + h.bx(ixm, iyp, iz));
     R bzf = R(0.25) * (h.bz(ix, iy, iz) + h.bz(ix, iyp, iz) + h.bz(ix, iy, izm) + h.bz(ix, iyp, izm));
     R b0 = h.by(ix, iy, iz);
     R modb = bxf * bxf + b0 * b0 + bzf * bzf + min_b;
-    R tb = (T(ix, iyp, iz) + T(ix, iy, iz)) / R(2);
-    R tb_p = (T(ixp, iy, iz) + T(ixp, iyp, iz)) / R(2);
-    R tb_m = (T(ixm, iyp, iz) + T(ixm, iy, iz)) / R(2);
-    R tg_a1 = (tb_p - tb_m) / (h.dxc(ix) + h.dxc(ixm));
-    tb_p = (T(ix, iyp, izp) + T(ix, iy, izp)) / R(2);
-    tb_m = (T(ix, iyp, izm) + T(ix, iy, izm)) / R(2);
-    R tg_a2 = (tb_p - tb_m) / (h.dzc(iz) + h.dzc(izm));
-    R tg = (T(ix, iyp, iz) - T(ix, iy, iz)) / h.dyc(iy);
+    R tb = (T(ix, iyp, iz) + T(ix, iy, iz)) * half;
+    R tb_p = (T(ixp, iy, iz) + T(ixp, iyp, iz)) * half;
+    R tb_m = (T(ixm, iyp, iz) + T(ixm, iy, iz)) * half;
+    R tg_a1 = (tb_p - tb_m) * h.rdc2[0](ix);
+    tb_p = (T(ix, iyp, izp) + T(ix, iy, izp)) * half;
+    tb_m = (T(ix, iyp, izm) + T(ix, iy, izm)) * half;
+    R tg_a2 = (tb_p - tb_m) * h.rdc2[2](iz);
+    R tg = (T(ix, iyp, iz) - T(ix, iy, iz)) * h.rdc[1](iy);
     tb = tb > R(0) ? tb : R(0);
-    return -lf * h.k0 * pow(tb, R(2.5)) * (b0 * (tg * b0 + tg_a1 * bxf + tg_a2 * bzf) + tg * min_b) / modb;
+    return -lf * h.k0 * pow25(tb) * (b0 * (tg * b0 + tg_a1 * bxf + tg_a2 * bzf) + tg * min_b) / modb *
+           h.rdb[1](iy);
   } else {
     R bxf = R(0.25) * (h.bx(ix, iy, iz) + h.bx(ix, iy, izp) + h.bx(ixm, iy, iz) + h.bx(ixm, iy, izp));
     R byf = R(0.25) * (h.by(ix, iy, iz) + h.by(ix, iy, izp) + h.by(ix, iym, iz) + h.by(ix, iym, izp));
     R b0 = h.bz(ix, iy, iz);
     R modb = bxf * bxf + byf * byf + b0 * b0 + min_b;
-    R tb = (T(ix, iy, izp) + T(ix, iy, iz)) / R(2);
-    R tb_p = (T(ixp, iy, izp) + T(ixp, iy, iz)) / R(2);
-    R tb_m = (T(ixm, iy, izp) + T(ixm, iy, iz)) / R(2);
-    R tg_a1 = (tb_p - tb_m) / (h.dxc(ix) + h.dxc(ixm));
-    tb_p = (T(ix, iyp, izp) + T(ix, iyp, iz)) / R(2);
-    tb_m = (T(ix, iym, izp) + T(ix, iym, iz)) / R(2);
-    R tg_a2 = (tb_p - tb_m) / (h.dyc(iy) + h.dyc(iym));
-    R tg = (T(ix, iy, izp) - T(ix, iy, iz)) / h.dzc(iz);
+    R tb = (T(ix, iy, izp) + T(ix, iy, iz)) * half;
+    R tb_p = (T(ixp, iy, izp) + T(ixp, iy, iz)) * half;
+    R tb_m = (T(ixm, iy, izp) + T(ixm, iy, iz)) * half;
+    R tg_a1 = (tb_p - tb_m) * h.rdc2[0](ix);
+    tb_p = (T(ix, iyp, izp) + T(ix, iyp, iz)) * half;
+    tb_m = (T(ix, iym, izp) + T(ix, iym, iz)) * half;
+    R tg_a2 = (tb_p - tb_m) * h.rdc2[1](iy);
+    R tg = (T(ix, iy, izp) - T(ix, iy, iz)) * h.rdc[2](iz);
     tb = tb > R(0) ? tb : R(0);
-    return -lf * h.k0 * pow(tb, R(2.5)) * (b0 * (tg * b0 + tg_a1 * bxf + tg_a2 * byf) + tg * min_b) / modb;
+    return -lf * h.k0 * pow25(tb) * (b0 * (tg * b0 + tg_a1 * bxf + tg_a2 * byf) + tg * min_b) / modb *
+           h.rdb[2](iz);
   }
-}
-
-template <class R>
-__device__ __forceinline__ R heat_flux_gather(const HeatFluxArgs<R>& h, int ix, int iy, int iz) {
-  R f = R(0);
-  f = f + face_flux(h, 2, ix, iy, iz - 1) / h.dzb(iz - 1);
-  f = f + face_flux(h, 1, ix, iy - 1, iz) / h.dyb(iy - 1);
-  f = f + face_flux(h, 0, ix - 1, iy, iz) / h.dxb(ix - 1);
-  f = f - face_flux(h, 0, ix, iy, iz) / h.dxb(ix);
-  f = f - face_flux(h, 1, ix, iy, iz) / h.dyb(iy);
-  f = f - face_flux(h, 2, ix, iy, iz) / h.dzb(iz);
-  return f;
 }
 
 template <class R>
@@ -486,8 +503,25 @@ void copy_whole(Run<R>& run, A3<R> dst, A3<R> src) {
   run.prof_end(k);
 }
 
+}  // namespace lare
+
+#include "conduct.cuh"
+
+namespace lare {
+
 // conduct.f90:299-416 heat_conduct_sts2, dt from sc[dt_slot]; the stage
 // count s must already be known on the host (run.n_s_stages).
+//
+// The reference keeps Y(0:3) and copies whole arrays between stages
+// (Y1 = Y2; energy = Y3; energy_bcs; Y2 = energy).  Here the stages rotate
+// three buffers instead, with Y0 read straight from `energy` (untouched
+// until the end), and the temperature of Y2 is formed where the flux needs
+// it.  The values are the same as the reference's, including its boundary
+// detail: the temperature ghosts of stage 2 in MPI/periodic directions come
+// from Y2's ghost cells, which still hold the energy's (temperature_bcs
+// refreshes only BC_USER faces), so Y2 starts as a whole copy of energy and
+// gets only the BC_USER fill before stage 2; from stage 3 on, Y2 is the
+// previous Y3 after the full energy boundary fill.
 template <class R>
 void heat_conduct_sts2(Run<R>& run, int dt_slot) {
   const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
@@ -510,54 +544,63 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
     gamma_tilde[j] = -1.0 * a[j - 1] * mu_tilde[j];
   }
   Arrays<R>& A = run.a;
-  auto Y0 = A.Y0, Y1 = A.Y1, Y2 = A.Y2, Y3 = A.Y3, Lc_Y0 = A.Lc_Y0, rho = A.rho, energy = A.energy;
-  HeatFluxArgs<R> h{A.temperature, A.bx, A.by, A.bz, A.larsen, A.dxb, A.dyb, A.dzb, A.dxc, A.dyc, A.dzc,
-                    (R)run.p.kappa_0};
+  auto Lc_Y0 = A.Lc_Y0, rho = A.rho, energy = A.energy;
+  const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
+  const R tc = (g - R(1)) / (R(2) - xi), te0 = (R(1) - xi) * ip;
+  auto args = [&](A3<R> y) {
+    return HeatFluxArgs<R>{TempOf<R>{y, tc, te0}, A.bx, A.by, A.bz, A.larsen, {A.rdb[0], A.rdb[1], A.rdb[2]},
+                           {A.rdc[0], A.rdc[1], A.rdc[2]}, {A.rdc2[0], A.rdc2[1], A.rdc2[2]}, (R)run.p.kappa_0};
+  };
   const double* sc = run.sc;
-  copy_whole(run, Y0, energy);
-  copy_whole(run, Y1, energy);
+  if (s < 2) {
+    // The stage loop is empty and energy(1:n) = Y(3)(1:n) = energy: the
+    // reference leaves the energy unchanged (conduct.f90:409).
+    energy_bcs(run);
+    return;
+  }
+  // rotating buffers: Y0 = energy (read only), Y1 = energy for stage 2
+  A3<R> bufs[3] = {A.Y1, A.Y2, A.Y3};
+  A3<R> Y1 = energy, Y2 = bufs[0], Y3 = bufs[1];
+  int next_free = 2;
   copy_whole(run, Y2, energy);
-  copy_whole(run, Y3, energy);
-  temperature_from(run, Y0);
-  const R mt1 = (R)mu_tilde[1];
-  LARE_BOXW(run, 10, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
-    const R dt = (R)sc[dt_slot];
-    R f = heat_flux_gather<R>(h, ix, iy, iz);
-    R lc = (R(1) / rho(ix, iy, iz)) * f;
-    Lc_Y0(ix, iy, iz) = lc;
-    R c0 = mt1 * dt * lc;
-    R y1 = Y0(ix, iy, iz) + c0;
-    // Y(2) = Y(1); Y(1) = Y(0) on 1:n (conduct.f90:366-367)
-    Y2(ix, iy, iz) = y1;
-    Y1(ix, iy, iz) = Y0(ix, iy, iz);
-  });
+  rkl2_stage<R, true>(run, __LINE__, args(energy), energy, energy, energy, Y2, dt_slot, (R)mu_tilde[1], R(0), R(0),
+                      R(0), R(0));
+  ghost(run, run.g_cell_user, Y2);
+  {
+    GhostBatch<R> bb;
+    bb.add(run.g_cell_mpi, A.rho.p);  // density_mpi of temperature_bcs (a no-op on a consistent rho)
+    ghost_flush(run, bb);
+  }
   for (int j = 2; j <= s; ++j) {
-    temperature_from(run, Y2);
-    temperature_bcs(run);
     const R gt = (R)gamma_tilde[j], mtj = (R)mu_tilde[j], mj = (R)mu[j], nj = (R)nu[j];
-    const R omn = (R)(1.0 - mu[j] - nu[j]);
     const R omn_r = R(1) - mj - nj;
-    LARE_BOXW(run, 11, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
-      const R dt = (R)sc[dt_slot];
-      (void)omn;
-      R f = heat_flux_gather<R>(h, ix, iy, iz);
-      R c0 = gt * dt * Lc_Y0(ix, iy, iz);
-      R Lc = (R(1) / rho(ix, iy, iz)) * f;
-      R c1 = mtj * dt * Lc;
-      R y3 = mj * Y2(ix, iy, iz) + nj * Y1(ix, iy, iz) + omn_r * Y0(ix, iy, iz);
-      Y3(ix, iy, iz) = y3 + c1 + c0;
-    });
+    rkl2_stage<R, false>(run, __LINE__, args(Y2), Y2, Y1, energy, Y3, dt_slot, mtj, mj, nj, omn_r, gt);
     if (j < s) {
-      copy_whole(run, Y1, Y2);
-      copy_whole(run, energy, Y3);
-      energy_bcs(run);
-      copy_whole(run, Y2, energy);
-      // Y(3)(1:n) = 0 (conduct.f90:406): every later read of Y3 on 1:n is
-      // preceded by the next stage's write, so the zeroing is not needed.
+      GhostBatch<R> bb;
+      bb.add(run.g_cell, Y3.p);  // energy_bcs on the copy of Y3
+      ghost_flush(run, bb);
+      A3<R> freed = Y1;
+      Y1 = Y2;
+      Y2 = Y3;
+      if (freed.p == energy.p) {
+        Y3 = bufs[next_free];
+      } else {
+        Y3 = freed;
+      }
     }
   }
-  if (s >= 2) {
-    LARE_BOXW(run, 3, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) { energy(ix, iy, iz) = Y3(ix, iy, iz); });
+  // The reference leaves temperature = T(Y2 of the last stage) after
+  // temperature_bcs; keep that, then energy(1:n) = Y3(1:n) and energy_bcs.
+  {
+    auto temperature = A.temperature;
+    A3<R> y2 = Y2, y3 = Y3;
+    LARE_BOXW(run, 2, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+      temperature(ix, iy, iz) = tc * (y2(ix, iy, iz) - te0);
+    });
+    GhostBatch<R> bb;
+    bb.add(run.g_cell_user, temperature.p);
+    ghost_flush(run, bb);
+    LARE_BOXW(run, 2, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) { energy(ix, iy, iz) = y3(ix, iy, iz); });
   }
   energy_bcs(run);
 }

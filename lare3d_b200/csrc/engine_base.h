@@ -17,12 +17,14 @@ class EngineBase {
   virtual int eulerian_remap(int step) = 0;
   virtual int eta_calc() = 0;
   virtual int boundary_conditions() = 0;
-  virtual int conduct_heat(double dt, int* n_stages) = 0;
+  virtual int conduct_heat(double dt, int force_stages, int* n_stages) = 0;
+  virtual int conduction_stages(double dt, int* n_stages) = 0;
   virtual int energy(double out[5]) = 0;
   virtual int download(double* const* state8) = 0;
   virtual int get_field(const char* name, double* host) = 0;
   virtual int set_field(const char* name, const double* host) = 0;
   virtual int field_bounds(const char* name, int lo[3], int hi[3]) = 0;
+  virtual int field_device(const char* name, void** origin, int* sx, int* sxy, int* elem_bytes) = 0;
   virtual int scalars(lare_scalars* out) = 0;
   virtual int profile(int enable) = 0;
   virtual int profile_report(char* buf, int len) = 0;

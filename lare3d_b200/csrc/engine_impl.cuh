@@ -191,7 +191,7 @@ class EngineT : public EngineBase {
         &run.a.r_rho_v1, &run.a.rho1, &run.a.dm, &run.a.cv2, &run.a.flux, &run.a.f1, &run.a.f2,
         &run.a.rho_alt, &run.a.cv1v, &run.a.cv2v, &run.a.dmv, &run.a.mfx, &run.a.mfy, &run.a.mfz};
     if (p.conduction) {
-      for (A3<R>* x : {&run.a.larsen, &run.a.c_flux, &run.a.Y0, &run.a.Y1, &run.a.Y2, &run.a.Y3, &run.a.Lc_Y0})
+      for (A3<R>* x : {&run.a.larsen, &run.a.Y1, &run.a.Y2, &run.a.Y3, &run.a.Lc_Y0})
         all.push_back(x);
     } else {
       // conduct_heat may still be called on its own; allocate lazily there.
@@ -219,7 +219,7 @@ class EngineT : public EngineBase {
     // 1-D metrics: dxb(-1:n+2), dxc(-1:n+1) per axis, grav(-1:nz+2).
     int nn[3] = {nx, ny, nz};
     size_t mlen = 0;
-    for (int d = 0; d < 3; ++d) mlen += (size_t)(nn[d] + 6) * 2;
+    for (int d = 0; d < 3; ++d) mlen += (size_t)(nn[d] + 6) * 5;
     mlen += nz + 6;
     metrics_dev = dalloc<R>(mlen, err);
     if (!metrics_dev) return LARE_ENOMEM;
@@ -234,6 +234,17 @@ class EngineT : public EngineBase {
       pos += nn[d] + 6;
       for (int i = -1; i <= nn[d] + 1; ++i) hm[pos + 2 + i] = (R)metrics6[2 * d + 1][i + 1];
       dc[d]->p = metrics_dev + pos + 2;
+      pos += nn[d] + 6;
+      // reciprocals used by conduction (computed in double, then rounded)
+      for (int i = -1; i <= nn[d] + 2; ++i) hm[pos + 2 + i] = (R)(1.0 / metrics6[2 * d][i + 1]);
+      run.a.rdb[d].p = metrics_dev + pos + 2;
+      pos += nn[d] + 6;
+      for (int i = -1; i <= nn[d] + 1; ++i) hm[pos + 2 + i] = (R)(1.0 / metrics6[2 * d + 1][i + 1]);
+      run.a.rdc[d].p = metrics_dev + pos + 2;
+      pos += nn[d] + 6;
+      for (int i = 0; i <= nn[d] + 1; ++i)
+        hm[pos + 2 + i] = (R)(1.0 / (metrics6[2 * d + 1][i + 1] + metrics6[2 * d + 1][i]));
+      run.a.rdc2[d].p = metrics_dev + pos + 2;
       pos += nn[d] + 6;
     }
     run.a.grav.p = metrics_dev + pos + 2;
@@ -300,10 +311,10 @@ class EngineT : public EngineBase {
   }
 
   int ensure_conduction_arrays() {
-    if (run.a.Y0.p) return LARE_OK;
+    if (run.a.Y1.p) return LARE_OK;
     std::string err;
     const long long off = 2 + 2LL * run.sx + 2LL * run.sxy;
-    for (A3<R>* x : {&run.a.larsen, &run.a.c_flux, &run.a.Y0, &run.a.Y1, &run.a.Y2, &run.a.Y3, &run.a.Lc_Y0}) {
+    for (A3<R>* x : {&run.a.larsen, &run.a.Y1, &run.a.Y2, &run.a.Y3, &run.a.Lc_Y0}) {
       R* base = dalloc<R>(run.elems, err);
       if (!base) return fail(LARE_ENOMEM, err);
       x->p = base + off;
@@ -436,13 +447,13 @@ class EngineT : public EngineBase {
     lare::boundary_conditions(run);
     return cuda_check("boundary_conditions");
   }
-  int conduct_heat(double dt, int* n_stages) override {
+  int conduct_heat(double dt, int force_stages, int* n_stages) override {
     int rc = ensure_conduction_arrays();
     if (rc) return rc;
     cudaMemcpyAsync(run.sc + SC_DTCOND, &dt, sizeof(double), cudaMemcpyHostToDevice, run.s);
     calc_s_stages(run, SC_DTCOND);
     if (pull_scalars(run) != cudaSuccess) return fail(LARE_ECUDA, "conduct_heat: sync failed");
-    int ns = (int)run.host_sc[SC_STAGES];
+    int ns = force_stages > 0 ? force_stages : (int)run.host_sc[SC_STAGES];
     if (ns < 1 || ns > 100000) return fail(LARE_ESTAGES, "RKL2 stage count out of range");
     run.n_s_stages = ns;
     heat_conduct_sts2(run, SC_DTCOND);
@@ -490,6 +501,28 @@ class EngineT : public EngineBase {
       lo[d] = it->second.second.lo[d];
       hi[d] = it->second.second.hi[d];
     }
+    return LARE_OK;
+  }
+  int conduction_stages(double dt, int* n_stages) override {
+    int rc = ensure_conduction_arrays();
+    if (rc) return rc;
+    cudaMemcpyAsync(run.sc + SC_DTCOND, &dt, sizeof(double), cudaMemcpyHostToDevice, run.s);
+    calc_s_stages(run, SC_DTCOND);
+    if (pull_scalars(run) != cudaSuccess) return fail(LARE_ECUDA, "conduction_stages: sync failed");
+    *n_stages = (int)run.host_sc[SC_STAGES];
+    return cuda_check("conduction_stages");
+  }
+  int field_device(const char* name, void** origin, int* sx, int* sxy, int* elem_bytes) override {
+    if (std::strcmp(name, "larsen_factor") == 0) {
+      int rc = ensure_conduction_arrays();
+      if (rc) return rc;
+    }
+    auto it = fields.find(name);
+    if (it == fields.end()) return fail(LARE_ENOTFOUND, std::string("unknown field ") + name);
+    *origin = (void*)it->second.first->p;
+    *sx = run.sx;
+    *sxy = run.sxy;
+    *elem_bytes = (int)sizeof(R);
     return LARE_OK;
   }
   int scalars(lare_scalars* o) override {

@@ -129,7 +129,24 @@ int lare_gpu_run(lare_ctx* c, int first_step, int nsteps, double t_end, int* ste
 int lare_gpu_conduct_heat(lare_ctx* c, double dt, int* n_stages) {
   if (guard(c)) return LARE_EINVAL;
   if (!(dt > 0.0) || !std::isfinite(dt)) return LARE_EINVAL;
-  return c->e->conduct_heat(dt, n_stages);
+  return c->e->conduct_heat(dt, 0, n_stages);
+}
+
+int lare_gpu_conduct_heat_stages(lare_ctx* c, double dt, int n_stages) {
+  if (guard(c)) return LARE_EINVAL;
+  if (!(dt > 0.0) || !std::isfinite(dt) || n_stages < 2) return LARE_EINVAL;
+  return c->e->conduct_heat(dt, n_stages, nullptr);
+}
+
+int lare_gpu_conduction_stages(lare_ctx* c, double dt, int* n_stages) {
+  if (guard(c) || !n_stages) return LARE_EINVAL;
+  if (!(dt > 0.0) || !std::isfinite(dt)) return LARE_EINVAL;
+  return c->e->conduction_stages(dt, n_stages);
+}
+
+int lare_gpu_field_device(lare_ctx* c, const char* name, void** origin, int* sx, int* sxy, int* elem_bytes) {
+  if (guard(c) || !name || !origin || !sx || !sxy || !elem_bytes) return LARE_EINVAL;
+  return c->e->field_device(name, origin, sx, sxy, elem_bytes);
 }
 
 int lare_gpu_energy(lare_ctx* c, double out[5]) {

@@ -15,7 +15,7 @@ from lare3d_b200.abi import LareParams, default_params
 
 def declared(header):
     txt = open(os.path.join(ROOT, "include", header)).read()
-    return sorted(set(re.findall(r"\b(lare_gpu_\w+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(lare_(?:gpu|sur)_\w+)\s*\(", txt)))
 
 
 def test_exports_every_declared_symbol(built):
@@ -23,8 +23,35 @@ def test_exports_every_declared_symbol(built):
     lib = gpu.library()
     names = declared("lare_gpu.h")
     assert len(names) >= 20
-    missing = [n for n in names if not hasattr(lib, n)]
+    sur = declared("lare_surrogate.h")
+    assert len(sur) == 11
+    missing = [n for n in names + sur if not hasattr(lib, n)]
     assert not missing, missing
+
+
+def test_surrogate_host_side_argument_checks(built):
+    """Bad shapes and null pointers are rejected before any launch."""
+    from lare3d_b200 import gpu
+    lib = gpu.library()
+    f = lib.lare_sur_conv
+    f.argtypes = [C.c_int] * 4 + [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                  C.c_int, C.c_void_p, C.c_void_p]
+    p = C.c_void_p(16)
+    assert f(16, 32, 1, 0, None, 24, 0, p, None, p, 22, 1, None, None) == -1      # null input
+    assert f(16, 32, 1, 0, p, 24, 0, p, None, p, 21, 1, None, None) == -1         # wrong output edge
+    assert f(16, 32, 1, 0, p, 24, 1, p, None, p, 24, 1, None, None) == -1         # pad must be 0 or 2
+    assert f(24, 32, 1, 0, p, 24, 0, p, None, p, 22, 1, None, None) == -1         # channel pair
+    assert f(32, 8, 0, 1, p, 24, 0, p, None, p, 22, 1, p, None) == -1             # mask with FP32 out
+    w = lib.lare_sur_conv_wgrad_work
+    w.argtypes = [C.c_int] * 4
+    w.restype = C.c_longlong
+    assert w(32, 32, 16, 64) == ((16 ** 3 * 64 + 2047) // 2048) * 27 * 32 * 32
+    r = lib.lare_sur_recheck
+    r.argtypes = [C.c_int, C.c_void_p] + [C.c_int] * 4 + [C.c_void_p] + [C.c_int] * 13 + [C.c_double] * 4 + \
+        [C.c_void_p] * 3
+    # window (96 columns) narrower than the checked patches (20 + 6 * 16)
+    assert r(4, p, 261, 261 * 261, 256, 256, p, 120, 120 * 101, 96, 96, 0, 0, 20, 20, 0, 6, 4, 16, 16,
+             5 / 3, 0.0, 0.0, 1e-3, p, p, None) == -1
 
 
 def test_struct_layout_matches_header():
