@@ -241,6 +241,51 @@ def surrogate_form(torch, cdeck, plain):
     return out
 
 
+def ensemble_form(torch, count=48, launches=3):
+    """48 blast / Orszag-Tang members of uneven sizes (32^3..128^3), FP32,
+    one graph launch per 6 steps of all members; block shapes from the
+    autotuner (measured at 32, 64, 96 and 128, nearest edge used)."""
+    from lare3d_b200 import ensemble as E
+    t0 = time.perf_counter()
+    reps = (32, 64, 96, 128)
+    tuned = {n: E.autotune(n, kind="blast", launches=1) for n in reps}
+    t_tune = time.perf_counter() - t0
+    specs = E.member_specs(count)
+    blocks = {sp.n: tuned[min(reps, key=lambda r: abs(r - sp.n))][0] for sp in specs}
+    ds = [E.member_deck(sp) for sp in specs]
+    ens = E.Ensemble(ds, precision=32, blocks=blocks)
+    st = torch.cuda.ExternalStream(ens.stream)
+    ens.launch(1)
+    ens.sync()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    ens.launch(launches)
+    b.record(st)
+    ens.sync()
+    el = a.elapsed_time(b) / 1000.0
+    cells = ens.cells()
+    steps = launches * E.STEPS_PER_LAUNCH
+    # the same members stepped one after another through lare_gpu_step
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for sim in ens.sims:
+        first = sim.scalars().steps_taken
+        for k in range(E.STEPS_PER_LAUNCH):
+            sim.step(first + k + 1)
+    torch.cuda.synchronize()
+    el_seq = time.perf_counter() - t1
+    ens.close()
+    return {"value": cells * steps / el, "unit": "cell-updates/s (all members)", "members": count,
+            "cells": cells, "steps": steps, "ms_per_step": 1e3 * el / steps,
+            "sizes": sorted(sp.n for sp in specs),
+            "sequential_lare_gpu_step_value": cells * E.STEPS_PER_LAUNCH / el_seq,
+            "speedup_vs_sequential": (cells * steps / el) / (cells * E.STEPS_PER_LAUNCH / el_seq),
+            "autotuned_blocks": {str(n): list(tuned[n][0]) for n in reps},
+            "autotune_ms_per_step": {str(n): {f"{k[0]}x{k[1]}": round(v, 4) for k, v in tuned[n][1].items()}
+                                     for n in reps},
+            "autotune_s": t_tune, "dtype": "f32"}
+
+
 def run_reference(args):
     ws, rank, _ = dist_setup(args)
     if rank != 0:
@@ -396,6 +441,7 @@ def main():
                                                   "dt_over_dt_parab": cdeck.info["dt_ratio"]}
             sc.close()
         forms["surrogate_conduction"] = surrogate_form(torch, cdeck, forms.get("conduction_rkl2_fp32"))
+        forms["ensemble"] = ensemble_form(torch)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -257,9 +257,40 @@ long long lare_gpu_launch_count(lare_ctx* ctx);
 /* The CUDA stream (cudaStream_t) the context launches on. */
 void* lare_gpu_stream(lare_ctx* ctx);
 
+/*
+ * Block shape (bx x by threads, bx*by a multiple of 32 up to 256) of the
+ * context's point kernels.  Results do not depend on it; the ensemble
+ * autotuner picks it per grid size.  No counterpart in the reference.
+ */
+int lare_gpu_set_block(lare_ctx* ctx, int bx, int by);
+
 const char* lare_gpu_last_error(lare_ctx* ctx);
 
 void lare_gpu_destroy(lare_ctx* ctx);
+
+/*
+ * Ensembles (no counterpart in the reference, which runs one simulation per
+ * MPI job): n independent contexts of any sizes and parameters, advanced by
+ * ONE CUDA graph launch per steps_per_launch steps of every member.  Each
+ * member must have taken at least one step through lare_gpu_step (the
+ * reference's first-call set-up), must not have conduction on (its RKL2
+ * stage count is chosen on the host), and must not be used through other
+ * calls while the ensemble exists, except after lare_ens_sync.  The
+ * resistive sub-cycles run as device-side loops inside the graph.
+ * steps_per_launch must be a multiple of 6 (the remap's sweep-order period,
+ * remap.f90), and recorded step numbers continue from each member's count.
+ *
+ * lare_ens_launch enqueues nlaunch graph launches on the ensemble's stream
+ * and returns; lare_ens_sync waits, folds the steps into every member's step
+ * counter and returns the first LARE_E* code raised on the device (a bad dt
+ * or sub-cycle count) with *first_bad its member index, or 0.
+ */
+typedef struct lare_ens lare_ens;
+int lare_ens_create(lare_ctx* const* members, int n, int steps_per_launch, lare_ens** out);
+int lare_ens_launch(lare_ens* ens, int nlaunch);
+int lare_ens_sync(lare_ens* ens, int* first_bad);
+void* lare_ens_stream(lare_ens* ens);
+void lare_ens_destroy(lare_ens* ens);
 
 #ifdef __cplusplus
 }

@@ -58,7 +58,9 @@ enum Slot {
   SC_STAGES,       // RKL2 stages (integer value)
   SC_DTPARAB,      // explicit conduction limit
   SC_EN_B, SC_EN_KE, SC_EN_INT,
-  SC_NSLOTS = 16
+  SC_ERROR,        // LARE_E* code raised on the device (0 = none)
+  SC_LOOP,         // remaining resistive sub-cycles of a captured step
+  SC_NSLOTS = 24
 };
 // Integer min-reduction targets (bit patterns of positive doubles order
 // like unsigned integers).
@@ -76,12 +78,16 @@ __global__ void __launch_bounds__(256) k_box(int i0, int j0, int k0, int ni, int
   fn(i0 + i, j0 + j, k0 + (int)blockIdx.z);
 }
 
+// Block shape bx x by (bx * by <= 256), chosen per context (the ensemble
+// autotuner sets it per grid size); every point runs the same arithmetic
+// whatever the shape.
 template <class Fn>
-inline void launch_box(cudaStream_t s, long long& count, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn) {
+inline void launch_box(cudaStream_t s, long long& count, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn,
+                       int bx = 64, int by = 4) {
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   if (ni <= 0 || nj <= 0 || nk <= 0) return;
-  dim3 blk(64, 4, 1);
-  dim3 grd((ni + 63) / 64, (nj + 3) / 4, nk);
+  dim3 blk(bx, by, 1);
+  dim3 grd((ni + bx - 1) / bx, (nj + by - 1) / by, nk);
   k_box<<<grd, blk, 0, s>>>(i0, j0, k0, ni, nj, fn);
   ++count;
 }

@@ -99,6 +99,9 @@ struct Run {
   bool gamma_boris_one = true;      // gamma_boris holds 1 everywhere
   int cur_step = 0;
   int peak_substeps = 0, last_substeps = 0, steps_taken = 0, n_s_stages = 0;
+  int blk_x = 64, blk_y = 4;            // block shape of the point kernels
+  bool capturing = false;               // recording a CUDA graph of whole steps
+  cudaStream_t s_body = nullptr;        // captures the body of the resistive sub-cycle loop
   GSpec g_cell, g_node, g_bx, g_by, g_bz, g_cell_mpi, g_cell_user, g_dm[3];
   Prof prof;
   std::string err;
@@ -160,7 +163,7 @@ inline void rbox(Run<R>& run, const char* func, int line, int words, int i0, int
                  Fn fn) {
   double pts = (double)(i1 - i0 + 1) * (double)(j1 - j0 + 1) * (double)(k1 - k0 + 1);
   int k = run.prof_begin(func, line, words, pts);
-  launch_box(run.s, run.launches, i0, i1, j0, j1, k0, k1, fn);
+  launch_box(run.s, run.launches, i0, i1, j0, j1, k0, k1, fn, run.blk_x, run.blk_y);
   run.prof_end(k);
 }
 // LARE_BOX: one kernel over an inclusive Fortran index box.  LARE_BOXW also

@@ -28,6 +28,14 @@ class EngineBase {
   virtual int scalars(lare_scalars* out) = 0;
   virtual int profile(int enable) = 0;
   virtual int profile_report(char* buf, int len) = 0;
+  // CUDA-graph recording of whole steps (the ensemble path).  The caller
+  // has put stream() into capture mode; capture_steps records nsteps steps
+  // numbered from steps_taken + 1 and leaves the host-side counters as they
+  // were; add_steps advances them once the graph has run.
+  virtual int capture_steps(int nsteps) = 0;
+  virtual void add_steps(int n) = 0;
+  virtual int set_block(int bx, int by) = 0;
+  virtual int device_error() = 0;  // syncs; LARE_E* raised on the device, 0 if none
   virtual long long launches() const = 0;
   virtual void* stream() const = 0;
   virtual const char* error() const = 0;

@@ -75,6 +75,7 @@ class EngineT : public EngineBase {
     for (void* p : run.allocations) cudaFree(p);
     if (run.host_sc) cudaFreeHost(run.host_sc);
     if (run.s) cudaStreamDestroy(run.s);
+    if (run.s_body) cudaStreamDestroy(run.s_body);
   }
 
   int fail(int code, const std::string& m) {
@@ -502,6 +503,41 @@ class EngineT : public EngineBase {
       hi[d] = it->second.second.hi[d];
     }
     return LARE_OK;
+  }
+  int capture_steps(int nsteps) override {
+    if (run.p.conduction) return fail(LARE_EINVAL, "capture: conduction steps need the host (stage count)");
+    if (run.steps_taken < 1) return fail(LARE_EINVAL, "capture: take one step first (first-call set-up)");
+    if (run.prof.on) return fail(LARE_EINVAL, "capture: profiling is on");
+    if (!run.s_body && cudaStreamCreateWithFlags(&run.s_body, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(LARE_ECUDA, "capture: stream");
+    const int first = run.steps_taken + 1;
+    const int saved_taken = run.steps_taken, saved_peak = run.peak_substeps;
+    run.capturing = true;
+    int rc = LARE_OK;
+    for (int k = 0; k < nsteps && rc == LARE_OK; ++k) {
+      rc = lare::lagrangian_step(run, first + k);
+      if (rc == LARE_OK) lare::eulerian_remap(run, first + k);
+      if (rc == LARE_OK) lare::eta_calc(run);
+    }
+    run.capturing = false;
+    run.steps_taken = saved_taken;
+    run.peak_substeps = saved_peak;
+    run.last_substeps = -1;
+    if (rc) return fail(rc, "capture: step recording failed");
+    return cuda_check("capture_steps");
+  }
+  void add_steps(int n) override { run.steps_taken += n; }
+  int set_block(int bx, int by) override {
+    if (bx < 1 || by < 1 || bx * by > 256 || (bx * by) % 32) return fail(LARE_EINVAL, "block shape");
+    run.blk_x = bx;
+    run.blk_y = by;
+    return LARE_OK;
+  }
+  int device_error() override {
+    if (pull_scalars(run) != cudaSuccess) return fail(LARE_ECUDA, "device_error: sync failed");
+    const int code = (int)run.host_sc[SC_ERROR];
+    if (code) fail(code, "raised on the device in a recorded step (bad dt or sub-cycle count)");
+    return code;
   }
   int conduction_stages(double dt, int* n_stages) override {
     int rc = ensure_conduction_arrays();

@@ -630,6 +630,67 @@ void predictor_corrector_step(Run<R>& run) {
 }
 
 // ---------------------------------------------------------------------
+// lagran.F90:135-150, the resistive sub-cycles, recorded into a CUDA graph:
+// the count is known only on the device, so the loop is a conditional WHILE
+// node whose body (eta + rkstep, bstep, ohmic heating) ends with a kernel
+// that counts down and sets the loop condition.  A bad dt sets sc[SC_ERROR]
+// and skips the loop; the host reads the flag after the graph has run.
+template <class R>
+int resistive_subcycles_captured(Run<R>& run) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  if (cudaStreamGetCaptureInfo(run.s, &st, nullptr, &g, &deps, &nd) != cudaSuccess ||
+      st != cudaStreamCaptureStatusActive)
+    return LARE_ECUDA;
+  cudaGraphConditionalHandle h;
+  if (cudaGraphConditionalHandleCreate(&h, g, 0, 0) != cudaSuccess) return LARE_ECUDA;
+  double* sc = run.sc;
+  launch_scalar(run.s, run.launches, [=] __device__() {
+    const double dt = sc[SC_DT];
+    const double q = dt / sc[SC_DTR];
+    int substeps = 0;
+    if (dt > 0.0 && isfinite(dt) && q >= 0.0 && q < 99999.0) {  // at most 1e5 device-side cycles
+      substeps = (int)q + 1;
+      sc[SC_DTSUB] = dt / (double)substeps;
+    } else {
+      sc[SC_ERROR] = (double)LARE_EDT;
+    }
+    sc[SC_SUBSTEPS] = (double)substeps;
+    sc[SC_LOOP] = (double)substeps;
+    cudaGraphSetConditional(h, substeps > 0 ? 1u : 0u);
+  });
+  if (cudaStreamGetCaptureInfo(run.s, &st, nullptr, &g, &deps, &nd) != cudaSuccess) return LARE_ECUDA;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cudaGraphAddNode(&node, g, deps, nd, &cp) != cudaSuccess) return LARE_ECUDA;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if (cudaStreamBeginCaptureToGraph(run.s_body, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+      cudaSuccess)
+    return LARE_ECUDA;
+  cudaStream_t outer = run.s;
+  run.s = run.s_body;
+  eta_and_rkstep(run, true);
+  resistive_update(run);
+  launch_scalar(run.s, run.launches, [=] __device__() {
+    const double left = sc[SC_LOOP] - 1.0;
+    sc[SC_LOOP] = left;
+    cudaGraphSetConditional(h, left > 0.5 ? 1u : 0u);
+  });
+  run.s = outer;
+  cudaGraph_t captured = nullptr;
+  if (cudaStreamEndCapture(run.s_body, &captured) != cudaSuccess) return LARE_ECUDA;
+  if (cudaStreamUpdateCaptureDependencies(run.s, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+    return LARE_ECUDA;
+  return LARE_OK;
+}
+
+// ---------------------------------------------------------------------
 // lagran.F90:50-200 lagrangian_step
 template <class R>
 int lagrangian_step(Run<R>& run, int step) {
@@ -638,7 +699,10 @@ int lagrangian_step(Run<R>& run, int step) {
   set_dt(run);
   double* sc = run.sc;
   run.last_substeps = 0;
-  if (run.p.resistive_mhd) {
+  if (run.p.resistive_mhd && run.capturing) {
+    int rc = resistive_subcycles_captured(run);
+    if (rc) return rc;
+  } else if (run.p.resistive_mhd) {
     launch_scalar(run.s, run.launches, [=] __device__() {
       double dt = sc[SC_DT];
       int substeps = (int)(dt / sc[SC_DTR]) + 1;
@@ -659,6 +723,7 @@ int lagrangian_step(Run<R>& run, int step) {
     // The cell B averages recomputed at :152-163 only feed the CAUCHY branch.
   }
   if (run.p.conduction) {
+    if (run.capturing) return LARE_EINVAL;  // the stage count and coefficients are host-side
     copy_whole(run, run.a.energy0, run.a.energy);
     calc_s_stages(run, SC_DT);
     if (pull_scalars(run) != cudaSuccess) return LARE_ECUDA;

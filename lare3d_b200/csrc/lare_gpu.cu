@@ -3,6 +3,7 @@
 
 #include <cmath>
 #include <string>
+#include <vector>
 
 #include "../../include/lare_gpu.h"
 #include "engine_base.h"
@@ -138,6 +139,11 @@ int lare_gpu_conduct_heat_stages(lare_ctx* c, double dt, int n_stages) {
   return c->e->conduct_heat(dt, n_stages, nullptr);
 }
 
+int lare_gpu_set_block(lare_ctx* c, int bx, int by) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->set_block(bx, by);
+}
+
 int lare_gpu_conduction_stages(lare_ctx* c, double dt, int* n_stages) {
   if (guard(c) || !n_stages) return LARE_EINVAL;
   if (!(dt > 0.0) || !std::isfinite(dt)) return LARE_EINVAL;
@@ -206,5 +212,119 @@ void lare_gpu_destroy(lare_ctx* c) {
   delete c->e;
   delete c;
 }
+
+// ---------------------------------------------------------------------
+// Ensembles: many independent contexts advanced by one CUDA graph launch.
+
+struct lare_ens {
+  std::vector<lare_ctx*> m;
+  int steps_per_launch = 0;
+  cudaStream_t s = nullptr;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> joins;
+  long long launched = 0;  // launches not yet folded into the members' step counters
+};
+
+namespace {
+void ens_free(lare_ens* e) {
+  if (!e) return;
+  if (e->s) cudaStreamSynchronize(e->s);
+  if (e->x) cudaGraphExecDestroy(e->x);
+  if (e->g) cudaGraphDestroy(e->g);
+  if (e->fork) cudaEventDestroy(e->fork);
+  for (cudaEvent_t j : e->joins)
+    if (j) cudaEventDestroy(j);
+  if (e->s) cudaStreamDestroy(e->s);
+  delete e;
+}
+}  // namespace
+
+int lare_ens_create(lare_ctx* const* members, int n, int steps_per_launch, lare_ens** out) {
+  if (!out) return LARE_EINVAL;
+  *out = nullptr;
+  if (!members || n < 1 || steps_per_launch < 1 || steps_per_launch % 6) return LARE_EINVAL;
+  for (int i = 0; i < n; ++i)
+    if (guard(members[i])) return LARE_EINVAL;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < i; ++j)
+      if (members[i] == members[j]) return LARE_EINVAL;
+  lare_ens* e = new lare_ens();
+  e->m.assign(members, members + n);
+  e->steps_per_launch = steps_per_launch;
+  e->joins.assign(n, nullptr);
+  int rc = LARE_OK;
+  if (cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) {
+    ens_free(e);
+    return LARE_ECUDA;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (cudaEventCreateWithFlags(&e->joins[i], cudaEventDisableTiming) != cudaSuccess) {
+      ens_free(e);
+      return LARE_ECUDA;
+    }
+  }
+  // Members may still be busy with eager work on their own streams.
+  for (int i = 0; i < n; ++i) cudaStreamSynchronize((cudaStream_t)members[i]->e->stream());
+  // One capture: fork every member's stream off the ensemble stream, record
+  // its steps there, join back.
+  if (cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    ens_free(e);
+    return LARE_ECUDA;
+  }
+  cudaEventRecord(e->fork, e->s);
+  for (int i = 0; i < n && rc == LARE_OK; ++i) {
+    cudaStream_t ms = (cudaStream_t)members[i]->e->stream();
+    cudaStreamWaitEvent(ms, e->fork, 0);
+    rc = members[i]->e->capture_steps(steps_per_launch);
+    cudaEventRecord(e->joins[i], ms);
+    cudaStreamWaitEvent(e->s, e->joins[i], 0);
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(e->s, &g);
+  e->g = g;
+  if (rc == LARE_OK && ce != cudaSuccess) rc = LARE_ECUDA;
+  if (rc == LARE_OK && cudaGraphInstantiate(&e->x, e->g, 0) != cudaSuccess) rc = LARE_ECUDA;
+  cudaGetLastError();
+  if (rc) {
+    ens_free(e);
+    return rc;
+  }
+  *out = e;
+  return LARE_OK;
+}
+
+int lare_ens_launch(lare_ens* e, int nlaunch) {
+  if (!e || !e->x || nlaunch < 0) return LARE_EINVAL;
+  for (int k = 0; k < nlaunch; ++k) {
+    if (cudaGraphLaunch(e->x, e->s) != cudaSuccess) return LARE_ECUDA;
+    ++e->launched;
+  }
+  return LARE_OK;
+}
+
+int lare_ens_sync(lare_ens* e, int* first_bad) {
+  if (!e) return LARE_EINVAL;
+  if (first_bad) *first_bad = -1;
+  if (cudaStreamSynchronize(e->s) != cudaSuccess) return LARE_ECUDA;
+  const int adv = (int)(e->launched * e->steps_per_launch);
+  e->launched = 0;
+  int rc = LARE_OK;
+  for (size_t i = 0; i < e->m.size(); ++i) {
+    e->m[i]->e->add_steps(adv);
+    const int code = e->m[i]->e->device_error();
+    if (code && rc == LARE_OK) {
+      rc = code;
+      if (first_bad) *first_bad = (int)i;
+    }
+  }
+  return rc;
+}
+
+void* lare_ens_stream(lare_ens* e) { return e ? (void*)e->s : nullptr; }
+
+void lare_ens_destroy(lare_ens* e) { ens_free(e); }
 
 }  // extern "C"

@@ -1,0 +1,79 @@
+"""GPU checks of batched ensembles: one graph launch per 6 steps of every
+member gives each member exactly the state of the same run stepped alone
+(FP32 form, bit for bit, resistive sub-cycles included), whatever block
+shape the autotuner picked; and the host-side rules of lare_ens_create."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import STATE
+
+pytestmark = pytest.mark.gpu
+
+
+def specs():
+    from lare3d_b200.ensemble import MemberSpec
+    return [MemberSpec("blast", 16, 0.5, 1e-3, 3), MemberSpec("orszag_tang", 24, 0.05, 5e-3, 4),
+            MemberSpec("blast", 20, 5.0, 1e-4, 5), MemberSpec("orszag_tang", 16, 2.0, 1e-2, 6)]
+
+
+def test_ensemble_matches_single_runs(built):
+    from lare3d_b200 import gpu
+    from lare3d_b200.ensemble import Ensemble, member_deck
+    ds = [member_deck(s) for s in specs()]
+    ens = Ensemble(ds, precision=32, blocks={16: (32, 4), 24: (128, 2), 20: (32, 8)})
+    ens.launch(2)
+    ens.sync()
+    assert ens.steps == 13
+    for i, d in enumerate(ds):
+        ref = gpu.simulation(d, precision=32)
+        ref.start(d.state)
+        for s in range(1, 14):
+            ref.step(s)
+        got = ens.sims[i]
+        for f in STATE:
+            a, b = got.get_field(f), ref.get_field(f)
+            assert np.array_equal(a, b), (i, f, float(np.abs(a - b).max()))
+        sa, sb = got.scalars(), ref.scalars()
+        assert sa.time == sb.time and sa.dt == sb.dt and sa.steps_taken == sb.steps_taken == 13
+        ref.close()
+    ens.close()
+
+
+def test_ensemble_create_rules(built):
+    from lare3d_b200 import decks, gpu
+    from lare3d_b200.ensemble import _lib
+    lib = _lib()
+    d = decks.blast(12)
+    a = gpu.simulation(d, precision=32)
+    a.start(d.state)
+    h = C.c_void_p()
+    arr = (C.c_void_p * 1)(a.ctx.value)
+    assert lib.lare_ens_create(arr, 1, 6, C.byref(h)) == -1          # no eager step yet
+    a.step(1)
+    assert lib.lare_ens_create(arr, 1, 5, C.byref(h)) == -1          # not a multiple of 6
+    two = (C.c_void_p * 2)(a.ctx.value, a.ctx.value)
+    assert lib.lare_ens_create(two, 2, 6, C.byref(h)) == -1          # the same member twice
+    c = decks.conduction(16)
+    b = gpu.simulation(c, precision=32)
+    b.start(c.state)
+    b.step(1)
+    arr = (C.c_void_p * 1)(b.ctx.value)
+    assert lib.lare_ens_create(arr, 1, 6, C.byref(h)) == -1          # conduction needs the host
+    arr = (C.c_void_p * 1)(a.ctx.value)
+    assert lib.lare_ens_create(arr, 1, 6, C.byref(h)) == 0
+    assert lib.lare_ens_launch(h, 1) == 0
+    bad = C.c_int(7)
+    assert lib.lare_ens_sync(h, C.byref(bad)) == 0 and bad.value == -1
+    lib.lare_ens_destroy(h)
+    assert a.scalars().steps_taken == 7
+    a.close()
+    b.close()
+
+
+def test_autotune_picks_a_measured_shape(built):
+    from lare3d_b200.ensemble import BLOCKS, autotune
+    best, times = autotune(16, blocks=BLOCKS[:3], launches=1, kind="blast")
+    assert best in BLOCKS[:3] and set(times) == set(BLOCKS[:3])
+    assert all(t > 0 for t in times.values())
