@@ -40,6 +40,21 @@ int lare_sur_conv(int cin, int cout, int relu, int out_f32, const void* x, int d
                   const float* bias, void* y, int dout, int nb, const void* mask, void* stream);
 
 /*
+ * Selects the convolution engine: 1 (default) = tcgen05.mma on the 5th-
+ * generation tensor cores with accumulators in tensor memory; 0 = the
+ * warp-level mma.sync kernel.  Both compute the same sums (FP32
+ * accumulation, summation order differs).  Process-wide.
+ */
+int lare_sur_set_engine(int tensor_cores);
+
+/*
+ * Sticky status of the tensor-core kernels: 0, or a bit mask of device-side
+ * failures (1 = a wait on the tensor cores ran out; the kernel skipped its
+ * remaining work).  Synchronises the device; clear != 0 resets the word.
+ */
+int lare_sur_status(int clear);
+
+/*
  * Weight and bias gradients of a valid conv (din = dout + 2):
  * dw[t][co][ci] = sum_{b,o} dy[b][o][co] * x[b][o + d(t)][ci],
  * db[co] = sum_{b,o} dy[b][o][co] (db may be NULL), FP32, deterministic

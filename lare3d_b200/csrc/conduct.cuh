@@ -1,49 +1,111 @@
-// conduct.cuh - the RKL2 stage of conduct.f90:299-416 as one tiled kernel.
+// conduct.cuh - the heat flux of conduct.f90:152-291 and the RKL2 stage of
+// conduct.f90:299-416 as tiled kernels.
 //
-// The reference's heat_flux (conduct.f90:152-291) forms every face flux
-// once and scatters it into the two cells that share the face.  A gather
-// over cells computes each face twice; this kernel computes each once per
-// stage: a CTA owns a 32 x 8 column of cells and walks up a chunk of z,
-// holding the temperature of planes z-1, z, z+1 (with a one-cell x/y halo)
-// in shared memory, the x and y face fluxes of the current plane in shared
-// memory, and the z face flux below each cell in a register carried to the
-// next plane.  The divergence adds the six scaled face fluxes of a cell in
-// the order in which the reference's scatter delivers them to that cell:
-//   +Fz(c-ez), +Fy(c-ey), +Fx(c-ex), -Fx(c), -Fy(c), -Fz(c)
-// (iteration (i,j,k-1) precedes (i,j-1,k) precedes (i-1,j,k) precedes
-// (i,j,k)).
+// Face flux (conduct.f90:170-275), x face between cells ix and ix+1:
+//   q = -L k0 T_f^{5/2} (b0 (b0 g_x + by_f g_y + bz_f g_z) + min_b g_x) / |B|^2
+// with T_f the face-mean temperature, g the temperature gradient at the
+// face (the transverse parts from the face-mean temperatures of the two
+// neighbouring rows), L the Larsen factor of cell ix and |B|^2 = b0^2 +
+// by_f^2 + bz_f^2 + min_b.  heat_flux scatters q / dxb(ix) into the two
+// cells.  Everything but T is fixed during a conduction step, so
+// face_coefficients forms, once per step, three coefficients per face
+//   k_n = L (b0^2 + min_b) / |B|^2 / dxc(ix) / dxb(ix)
+//   k_1 = L b0 by_f / |B|^2 / (2 (dyc(iy) + dyc(iy-1))) / dxb(ix)
+//   k_2 = L b0 bz_f / |B|^2 / (2 (dzc(iz) + dzc(iz-1))) / dxb(ix)
+// and the stage kernel evaluates q / dxb = -k0 T_f^{5/2} (k_n dT_n + k_1 dS_1
+// + k_2 dS_2) with dT_n = T(ix+1) - T(ix) and dS the differences of the
+// two-point temperature sums of the neighbouring rows.  The same algebra,
+// regrouped (and T^{5/2} = T^2 sqrt(T)), agrees with the reference to
+// rounding (relative 1e-12 in FP64).
+//
+// Stage kernel: a CTA owns a 32 x 8 column of cells and walks up a chunk of
+// z, holding the temperature of planes z-1, z, z+1 (one-cell x/y halo) in
+// shared memory, the x and y face fluxes of the current plane in shared
+// memory and the z face flux below each cell in a register carried to the
+// next plane, so each face flux is formed once.  A cell adds its six scaled
+// face fluxes in the order in which the reference's scatter delivers them:
+//   +Fz(c-ez), +Fy(c-ey), +Fx(c-ex), -Fx(c), -Fy(c), -Fz(c).
 #pragma once
 
 namespace lare {
 
 constexpr int kCTX = 32, kCTY = 8, kCZ = 16;  // CTA tile (x, y) and z chunk
-constexpr int kCPlane = (kCTX + 2) * (kCTY + 2);
+constexpr int kCW = kCTX + 2;                 // plane row length with halo
+constexpr int kCPlane = kCW * (kCTY + 2);
 
-// Temperature of planes iz-1, iz, iz+1 of a CTA tile in shared memory.
+// Coefficients of every face of cells 0..n (conduct.f90:170-275 regrouped).
 template <class R>
-struct PlaneT {
-  const R* pm;
-  const R* p0;
-  const R* pp;
-  int ix0, iy0, iz;
-  __device__ __forceinline__ R operator()(int i, int j, int k) const {
-    const R* p = k < iz ? pm : (k > iz ? pp : p0);
-    return p[(j - iy0 + 1) * (kCTX + 2) + (i - ix0 + 1)];
-  }
+void face_coefficients(Run<R>& run) {
+  const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
+  Arrays<R>& A = run.a;
+  auto bx = A.bx, by = A.by, bz = A.bz, larsen = A.larsen;
+  const A1<R> rdb0 = A.rdb[0], rdb1 = A.rdb[1], rdb2 = A.rdb[2];
+  const A1<R> rdc0 = A.rdc[0], rdc1 = A.rdc[1], rdc2 = A.rdc[2];
+  const A1<R> rs0 = A.rdc2[0], rs1 = A.rdc2[1], rs2 = A.rdc2[2];
+  A3<R> k[9];
+  for (int q = 0; q < 9; ++q) k[q] = A.kf[q];
+  const A3<R> k0 = k[0], k1 = k[1], k2 = k[2], k3 = k[3], k4 = k[4], k5 = k[5], k6 = k[6], k7 = k[7], k8 = k[8];
+  LARE_BOXW(run, 13, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+    const R min_b = R(1.0e-10);  // conduct.f90:28
+    const R half = R(0.5), q4 = R(0.25);
+    const int ixp = ix + 1, ixm = ix - 1, iyp = iy + 1, iym = iy - 1, izp = iz + 1, izm = iz - 1;
+    const R lf = larsen(ix, iy, iz);
+    {  // x face
+      const R byf = q4 * (by(ix, iy, iz) + by(ixp, iy, iz) + by(ix, iym, iz) + by(ixp, iym, iz));
+      const R bzf = q4 * (bz(ix, iy, iz) + bz(ixp, iy, iz) + bz(ix, iy, izm) + bz(ixp, iy, izm));
+      const R b0 = bx(ix, iy, iz);
+      const R w = lf / (b0 * b0 + byf * byf + bzf * bzf + min_b) * rdb0(ix);
+      k0(ix, iy, iz) = w * (b0 * b0 + min_b) * rdc0(ix);
+      k1(ix, iy, iz) = w * b0 * byf * half * rs1(iy);
+      k2(ix, iy, iz) = w * b0 * bzf * half * rs2(iz);
+    }
+    {  // y face
+      const R bxf = q4 * (bx(ix, iy, iz) + bx(ix, iyp, iz) + bx(ixm, iy, iz) + bx(ixm, iyp, iz));
+      const R bzf = q4 * (bz(ix, iy, iz) + bz(ix, iyp, iz) + bz(ix, iy, izm) + bz(ix, iyp, izm));
+      const R b0 = by(ix, iy, iz);
+      const R w = lf / (bxf * bxf + b0 * b0 + bzf * bzf + min_b) * rdb1(iy);
+      k3(ix, iy, iz) = w * (b0 * b0 + min_b) * rdc1(iy);
+      k4(ix, iy, iz) = w * b0 * bxf * half * rs0(ix);
+      k5(ix, iy, iz) = w * b0 * bzf * half * rs2(iz);
+    }
+    {  // z face
+      const R bxf = q4 * (bx(ix, iy, iz) + bx(ix, iy, izp) + bx(ixm, iy, iz) + bx(ixm, iy, izp));
+      const R byf = q4 * (by(ix, iy, iz) + by(ix, iy, izp) + by(ix, iym, iz) + by(ix, iym, izp));
+      const R b0 = bz(ix, iy, iz);
+      const R w = lf / (bxf * bxf + byf * byf + b0 * b0 + min_b) * rdb2(iz);
+      k6(ix, iy, iz) = w * (b0 * b0 + min_b) * rdc2(iz);
+      k7(ix, iy, iz) = w * b0 * bxf * half * rs0(ix);
+      k8(ix, iy, iz) = w * b0 * byf * half * rs1(iy);
+    }
+  });
+}
+
+template <class R>
+struct StageArgs {
+  TempOf<R> T;                      // temperature of the stage input
+  A3<R> k[9];                       // face coefficients
+  A3<R> y2, y1, y0, lc0, rho, out;  // stage arrays
+  R k0, mt, mu, nu, omn, gt;
+  int dt_slot, nx, ny, nz;
 };
 
-// FIRST: stage 1 (y_in = energy = Y0): Lc_Y0 = flux / rho and
+template <class R>
+__device__ __forceinline__ R face_q(R k0, R T0, R T1, R kn, R k1, R s1, R k2, R s2) {
+  R tb = (T1 + T0) * R(0.5);
+  tb = tb > R(0) ? tb : R(0);
+  return -k0 * pow25(tb) * (kn * (T1 - T0) + k1 * s1 + k2 * s2);
+}
+
+// FIRST: stage 1 (y2 = energy = Y0): Lc_Y0 = flux / rho and
 //        out = Y0 + mt * dt * Lc_Y0.
 // else:  stage j: out = mu Y2 + nu Y1 + (1 - mu - nu) Y0 + mt dt Lc + gt dt Lc_Y0
 //        with Lc the flux of T(Y2) / rho.
 template <class R, bool FIRST>
-__global__ void __launch_bounds__(kCTX* kCTY) k_rkl2_stage(HeatFluxArgs<R> h, A3<R> y2, A3<R> y1, A3<R> y0,
-                                                          A3<R> lc0, A3<R> rho, A3<R> out,
-                                                          const double* __restrict__ sc, int dt_slot, R mt, R mu,
-                                                          R nu, R omn, R gt, int nx, int ny, int nz) {
+__global__ void __launch_bounds__(kCTX* kCTY) k_rkl2_stage(StageArgs<R> a, const double* __restrict__ sc) {
   __shared__ R Ts[3][kCPlane];
   __shared__ R fx[kCTY][kCTX + 1];
   __shared__ R fy[kCTY + 1][kCTX];
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int tid = threadIdx.x;
   const int tx = tid % kCTX, ty = tid / kCTX;
   const int ix0 = 1 + blockIdx.x * kCTX, iy0 = 1 + blockIdx.y * kCTY;
@@ -51,15 +113,21 @@ __global__ void __launch_bounds__(kCTX* kCTY) k_rkl2_stage(HeatFluxArgs<R> h, A3
   const int iz1 = min(nz, iz0 + kCZ - 1);
   const int ix = ix0 + tx, iy = iy0 + ty;
   const bool active = ix <= nx && iy <= ny;
-  const R dt = (R)sc[dt_slot];
-  auto slot = [](int k) { return (k + 3) % 3; };
+  const R dt = (R)sc[a.dt_slot];
   auto load_plane = [&](int k) {
-    R* d = Ts[slot(k)];
+    R* d = Ts[(k + 3) % 3];
     for (int e = tid; e < kCPlane; e += kCTX * kCTY) {
-      const int jj = e / (kCTX + 2), ii = e - jj * (kCTX + 2);
+      const int jj = e / kCW, ii = e - jj * kCW;
       const int i = min(ix0 - 1 + ii, nx + 2), j = min(iy0 - 1 + jj, ny + 2);
-      d[e] = h.T(i, j, k);
+      d[e] = a.T(i, j, k);
     }
+  };
+  // z face above cell (lr, lc) of plane slots pm (lower) and pp (upper)
+  auto zface = [&](const R* pm, const R* pp, int lr, int lc, int i, int j, int k) {
+    const int e = lr * kCW + lc;
+    return face_q(a.k0, pm[e], pp[e], a.k[6](i, j, k), a.k[7](i, j, k),
+                  (pp[e + 1] + pm[e + 1]) - (pp[e - 1] + pm[e - 1]), a.k[8](i, j, k),
+                  (pp[e + kCW] + pm[e + kCW]) - (pp[e - kCW] + pm[e - kCW]));
   };
   load_plane(iz0 - 1);
   load_plane(iz0);
@@ -67,23 +135,32 @@ __global__ void __launch_bounds__(kCTX* kCTY) k_rkl2_stage(HeatFluxArgs<R> h, A3
   for (int iz = iz0; iz <= iz1; ++iz) {
     load_plane(iz + 1);
     __syncthreads();
-    const PlaneT<R> P{Ts[slot(iz - 1)], Ts[slot(iz)], Ts[slot(iz + 1)], ix0, iy0, iz};
-    if (iz == iz0 && active) {
-      const PlaneT<R> Pm{nullptr, Ts[slot(iz - 1)], Ts[slot(iz)], ix0, iy0, iz - 1};
-      fz_m = face_flux(h, Pm, 2, ix, iy, iz - 1);
-    }
+    const R* Pm = Ts[(iz + 2) % 3];
+    const R* P0 = Ts[iz % 3];
+    const R* Pp = Ts[(iz + 1) % 3];
+    if (iz == iz0 && active) fz_m = zface(Pm, P0, ty + 1, tx + 1, ix, iy, iz - 1);
     for (int f = tid; f < kCTY * (kCTX + 1); f += kCTX * kCTY) {
       const int r = f / (kCTX + 1), c = f - r * (kCTX + 1);
       const int fi = ix0 - 1 + c, fj = iy0 + r;
-      if (fi <= nx && fj <= ny) fx[r][c] = face_flux(h, P, 0, fi, fj, iz);
+      if (fi <= nx && fj <= ny) {
+        const int e = (r + 1) * kCW + c;  // cell fi of row fj
+        fx[r][c] = face_q(a.k0, P0[e], P0[e + 1], a.k[0](fi, fj, iz), a.k[1](fi, fj, iz),
+                          (P0[e + kCW + 1] + P0[e + kCW]) - (P0[e - kCW + 1] + P0[e - kCW]), a.k[2](fi, fj, iz),
+                          (Pp[e + 1] + Pp[e]) - (Pm[e + 1] + Pm[e]));
+      }
     }
     for (int f = tid; f < (kCTY + 1) * kCTX; f += kCTX * kCTY) {
       const int r = f / kCTX, c = f - r * kCTX;
       const int fi = ix0 + c, fj = iy0 - 1 + r;
-      if (fi <= nx && fj <= ny) fy[r][c] = face_flux(h, P, 1, fi, fj, iz);
+      if (fi <= nx && fj <= ny) {
+        const int e = r * kCW + c + 1;  // cell fi of row fj
+        fy[r][c] = face_q(a.k0, P0[e], P0[e + kCW], a.k[3](fi, fj, iz), a.k[4](fi, fj, iz),
+                          (P0[e + 1] + P0[e + kCW + 1]) - (P0[e - 1] + P0[e + kCW - 1]), a.k[5](fi, fj, iz),
+                          (Pp[e] + Pp[e + kCW]) - (Pm[e] + Pm[e + kCW]));
+      }
     }
     R fz_p = R(0);
-    if (active) fz_p = face_flux(h, P, 2, ix, iy, iz);
+    if (active) fz_p = zface(P0, Pp, ty + 1, tx + 1, ix, iy, iz);
     __syncthreads();
     if (active) {
       R f = R(0);
@@ -94,15 +171,15 @@ __global__ void __launch_bounds__(kCTX* kCTY) k_rkl2_stage(HeatFluxArgs<R> h, A3
       f = f - fy[ty + 1][tx];
       f = f - fz_p;
       if (FIRST) {
-        const R lc = (R(1) / rho(ix, iy, iz)) * f;
-        lc0(ix, iy, iz) = lc;
-        out(ix, iy, iz) = y0(ix, iy, iz) + mt * dt * lc;
+        const R lc = (R(1) / a.rho(ix, iy, iz)) * f;
+        a.lc0(ix, iy, iz) = lc;
+        a.out(ix, iy, iz) = a.y0(ix, iy, iz) + a.mt * dt * lc;
       } else {
-        const R c0 = gt * dt * lc0(ix, iy, iz);
-        const R Lc = (R(1) / rho(ix, iy, iz)) * f;
-        const R c1 = mt * dt * Lc;
-        const R v = mu * y2(ix, iy, iz) + nu * y1(ix, iy, iz) + omn * y0(ix, iy, iz);
-        out(ix, iy, iz) = v + c1 + c0;
+        const R c0 = a.gt * dt * a.lc0(ix, iy, iz);
+        const R Lc = (R(1) / a.rho(ix, iy, iz)) * f;
+        const R c1 = a.mt * dt * Lc;
+        const R v = a.mu * a.y2(ix, iy, iz) + a.nu * a.y1(ix, iy, iz) + a.omn * a.y0(ix, iy, iz);
+        a.out(ix, iy, iz) = v + c1 + c0;
       }
     }
     fz_m = fz_p;
@@ -110,13 +187,32 @@ __global__ void __launch_bounds__(kCTX* kCTY) k_rkl2_stage(HeatFluxArgs<R> h, A3
 }
 
 template <class R, bool FIRST>
-void rkl2_stage(Run<R>& run, int line, const HeatFluxArgs<R>& h, A3<R> y2, A3<R> y1, A3<R> y0, A3<R> out,
-                int dt_slot, R mt, R mu, R nu, R omn, R gt) {
+void rkl2_stage(Run<R>& run, int line, const TempOf<R>& T, A3<R> y2, A3<R> y1, A3<R> y0, A3<R> out, int dt_slot,
+                R mt, R mu, R nu, R omn, R gt) {
   const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
+  StageArgs<R> a;
+  a.T = T;
+  for (int q = 0; q < 9; ++q) a.k[q] = run.a.kf[q];
+  a.y2 = y2;
+  a.y1 = y1;
+  a.y0 = y0;
+  a.lc0 = run.a.Lc_Y0;
+  a.rho = run.a.rho;
+  a.out = out;
+  a.k0 = (R)run.p.kappa_0;
+  a.mt = mt;
+  a.mu = mu;
+  a.nu = nu;
+  a.omn = omn;
+  a.gt = gt;
+  a.dt_slot = dt_slot;
+  a.nx = nx;
+  a.ny = ny;
+  a.nz = nz;
   dim3 grid((nx + kCTX - 1) / kCTX, (ny + kCTY - 1) / kCTY, (nz + kCZ - 1) / kCZ);
-  const int k = run.prof_begin("rkl2_stage", line, FIRST ? 9 : 10, (double)nx * ny * nz);
-  k_rkl2_stage<R, FIRST><<<grid, kCTX * kCTY, 0, run.s>>>(h, y2, y1, y0, run.a.Lc_Y0, run.a.rho, out, run.sc,
-                                                          dt_slot, mt, mu, nu, omn, gt, nx, ny, nz);
+  // words per point: T stencil input, 9 coefficients, rho, Lc_Y0, output (+ Y1, Y0 after stage 1)
+  const int k = run.prof_begin("rkl2_stage", line, FIRST ? 13 : 15, (double)nx * ny * nz);
+  k_rkl2_stage<R, FIRST><<<grid, kCTX * kCTY, 0, run.s>>>(a, run.sc);
   run.prof_end(k);
   ++run.launches;
 }

@@ -1,0 +1,320 @@
+// conv_tc.cuh - the surrogate's 3-D convolution on the 5th-generation
+// tensor cores (tcgen05.mma, accumulators in tensor memory).
+//
+// Implicit GEMM with shifted operands.  For an output z-plane oz, output
+// voxels are numbered r = oy*D + ox with the INPUT row length D (columns
+// ox >= E = D - 2 are computed and dropped), so that for tap (dz, dy, dx)
+// the input voxel of row r is row r + dy*D + dx of input plane oz + dz: one
+// constant shift per tap.  A CTA stages the three input planes' rows
+// [r0, r0 + RS) in shared memory as [plane][channel group of 8][row][8 bf16]
+// -- the no-swizzle K-major operand layout, in which 8 consecutive rows of
+// 16 bytes form one core matrix -- so the A operand of every tap is the same
+// buffer with a different start address.  The weights stay resident as
+// [tap][channel group][cout][8].  One elected thread issues
+// T x 27 x (CIN/16) MMAs of 128 x N x 16 (N = output channels) into T
+// accumulator tiles in tensor memory, commits them to an mbarrier, and the
+// four warps read their 32 lanes back (tcgen05.ld), add the bias, apply the
+// ReLU or the mask and store bf16 or FP32.  Padding (pad = 2, the
+// backward-data convolution) is zero fill during staging.
+//
+// Every wait is bounded; a wait that runs out records kErrWait in the
+// device status word and the CTA frees its tensor memory and returns.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace {
+
+constexpr int kTcT = 4;           // accumulator tiles (128 rows each) per work item
+constexpr int kTcThreads = 128;
+constexpr int kErrWait = 1;
+
+__device__ int g_sur_status = 0;  // sticky error word of the tensor-core kernels
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// 16-byte asynchronous global -> shared copy; src_bytes = 0 writes zeros.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle: start, leading
+// (K-direction core-matrix) byte offset, stride (M/N-direction core-matrix)
+// byte offset, descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulate, bf16 A and B, both
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t umma_idesc(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[N]);
+
+template <>
+__device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+template <>
+__device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float (&v)[32]) {
+  float a[16], b[16];
+  tmem_ld<16>(taddr, a);
+  tmem_ld<16>(taddr + 16, b);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    v[i] = a[i];
+    v[16 + i] = b[i];
+  }
+}
+
+struct TcGeom {
+  int D;      // virtual (padded) input edge
+  int E;      // output edge = D - 2
+  int din;    // real input edge
+  int pad;    // 0 or 2
+  int nb;
+  int RS;     // staged rows per plane (odd multiple of 8 plus 1)
+  int NRP;    // padded rows per output plane that cover every valid voxel
+  int ntg;    // work items per output plane
+};
+
+// CIN input channels, NTC = MMA N (output channels computed), COUT = output
+// channels stored.
+template <int CIN, int NTC, int COUT>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_conv_tc(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ w,
+              const float* __restrict__ bias, void* __restrict__ y, const __nv_bfloat16* __restrict__ mask,
+              TcGeom g, int relu, int out_f32) {
+  constexpr int KG = CIN / 8;
+  constexpr int WBYTES = 27 * KG * NTC * 16;
+  constexpr int TCOLS = kTcT * NTC <= 32 ? 32 : (kTcT * NTC <= 64 ? 64 : 128);
+  extern __shared__ __align__(128) unsigned char sm[];
+  unsigned char* sw = sm;                        // weights
+  unsigned char* sx = sm + WBYTES;               // staged input
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int RS = g.RS, D = g.D;
+  const long long in_plane = (long long)g.din * g.din;
+
+  // weights: global [27][COUT][CIN] -> shared [27][KG][NTC][8] (rows >= COUT zero)
+  for (int q = tid; q < 27 * KG * NTC; q += kTcThreads) {
+    const int co = q % NTC, kg = (q / NTC) % KG, tap = q / (NTC * KG);
+    const __nv_bfloat16* src = w + ((long long)tap * COUT + (co < COUT ? co : 0)) * CIN + kg * 8;
+    cp_async16(smem_u32(sw + (size_t)q * 16), src, co < COUT ? 16u : 0u);
+  }
+  cp_async_wait_all();
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(TCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tbase = tmem_slot;
+  const uint32_t mb = smem_u32(&mbar);
+  const uint32_t sw_a = smem_u32(sw), sx_a = smem_u32(sx);
+  const uint32_t idesc = umma_idesc(NTC);
+  uint32_t phase = 0;
+  bool failed = false;
+
+  const long long items = (long long)g.nb * g.E * g.ntg;
+  for (long long it = blockIdx.x; it < items && !failed; it += gridDim.x) {
+    const int tg = (int)(it % g.ntg);
+    const int oz = (int)((it / g.ntg) % g.E);
+    const int b = (int)(it / ((long long)g.ntg * g.E));
+    const int r0 = tg * kTcT * 128;
+    // stage planes oz..oz+2 (virtual), rows r0..r0+RS-1, zero outside the real input
+    for (int q = tid; q < 3 * RS * KG; q += kTcThreads) {
+      const int kg = q % KG, v = (q / KG) % RS, p = q / (KG * RS);
+      const int vr = r0 + v;
+      const int vz = oz + p, vy = vr / D, vx = vr - (vr / D) * D;
+      const int iz = vz - g.pad, iy = vy - g.pad, ix = vx - g.pad;
+      const bool in = vy < D && (unsigned)iz < (unsigned)g.din && (unsigned)iy < (unsigned)g.din &&
+                      (unsigned)ix < (unsigned)g.din;
+      const __nv_bfloat16* src =
+          in ? x + (((long long)b * g.din + iz) * in_plane + (long long)iy * g.din + ix) * CIN + kg * 8 : x;
+      cp_async16(sx_a + (uint32_t)(((p * KG + kg) * RS + v) * 16), src, in ? 16u : 0u);
+    }
+    cp_async_wait_all();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      // the kTcT accumulator tiles are independent: interleave them so that
+      // consecutive MMAs do not wait on the same accumulator
+      for (int tap = 0; tap < 27; ++tap) {
+        const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+#pragma unroll
+        for (int kc = 0; kc < KG / 2; ++kc) {
+          const uint32_t b_addr = sw_a + (uint32_t)(((tap * KG + 2 * kc) * NTC) * 16);
+          const uint64_t bd = umma_desc(b_addr, (uint32_t)NTC * 16u, 128u);
+          const uint32_t acc = (tap > 0 || kc > 0) ? 1u : 0u;
+#pragma unroll
+          for (int t = 0; t < kTcT; ++t) {
+            const int row = t * 128 + dy * D + dx;
+            const uint32_t a_addr = sx_a + (uint32_t)(((dz * KG + 2 * kc) * RS + row) * 16);
+            const uint64_t ad = umma_desc(a_addr, (uint32_t)RS * 16u, 128u);
+            umma_f16(tbase + (uint32_t)(t * NTC), ad, bd, idesc, acc);
+          }
+        }
+      }
+      umma_commit(mb);
+    }
+    // wait for the accumulators (bounded; the outcome is made uniform over
+    // the CTA so that every thread takes the same path)
+    long long spins = 0;
+    bool timed_out = false;
+    while (!mbar_try(mb, phase)) {
+      if (++spins > (1LL << 22)) {
+        timed_out = true;
+        break;
+      }
+    }
+    phase ^= 1u;
+    failed = __syncthreads_or(timed_out) != 0;
+    if (failed) {
+      if (tid == 0) atomicOr(&g_sur_status, kErrWait);
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // epilogue: warp w owns accumulator rows 32w..32w+31 of every tile
+#pragma unroll 1
+    for (int t = 0; t < kTcT; ++t) {
+      float v[NTC];
+      tmem_ld<NTC>(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(t * NTC), v);
+      const int r = r0 + t * 128 + 32 * warp + lane;
+      const int oy = r / D, ox = r - (r / D) * D;
+      if (oy < g.E && ox < g.E) {
+        const long long o = (((long long)b * g.E + oz) * g.E + oy) * g.E + ox;
+        if (out_f32) {
+          float* yo = reinterpret_cast<float*>(y) + o * COUT;
+#pragma unroll
+          for (int c = 0; c < COUT; ++c) {
+            float a = v[c] + (bias ? bias[c] : 0.f);
+            if (relu) a = fmaxf(a, 0.f);
+            yo[c] = a;
+          }
+        } else {
+          __nv_bfloat16* yo = reinterpret_cast<__nv_bfloat16*>(y) + o * COUT;
+#pragma unroll
+          for (int c = 0; c < COUT; c += 8) {
+            float a[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              a[j] = v[c + j] + (bias ? bias[c + j] : 0.f);
+              if (relu) a[j] = fmaxf(a[j], 0.f);
+            }
+            if (mask) {
+              const uint4 mk = *reinterpret_cast<const uint4*>(mask + o * COUT + c);
+              const uint32_t mw[4] = {mk.x, mk.y, mk.z, mk.w};
+#pragma unroll
+              for (int j = 0; j < 8; ++j) {
+                const unsigned short h = (unsigned short)((mw[j >> 1] >> (16 * (j & 1))) & 0xffffu);
+                if (!(__bfloat162float(__ushort_as_bfloat16(h)) > 0.f)) a[j] = 0.f;
+              }
+            }
+            uint4 o4;
+            o4.x = pack2f(a[0], a[1]);
+            o4.y = pack2f(a[2], a[3]);
+            o4.z = pack2f(a[4], a[5]);
+            o4.w = pack2f(a[6], a[7]);
+            *reinterpret_cast<uint4*>(yo + c) = o4;
+          }
+        }
+      }
+    }
+    // every warp is done with tensor memory and the staged rows before the
+    // next item's MMAs overwrite them
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TCOLS) : "memory");
+  }
+}
+
+// Geometry of one convolution call (see the file comment).
+inline TcGeom tc_geom(int din, int pad, int nb) {
+  TcGeom g;
+  g.din = din;
+  g.pad = pad;
+  g.D = din + 2 * pad;
+  g.E = g.D - 2;
+  g.nb = nb;
+  int rs = kTcT * 128 + 2 * g.D + 2;
+  rs = (rs + 7) / 8 * 8 + 1;  // odd number of 16-byte rows per channel group: conflict-free staging stores
+  g.RS = rs;
+  g.NRP = (g.E - 1) * g.D + g.E;
+  g.ntg = (g.NRP + kTcT * 128 - 1) / (kTcT * 128);
+  return g;
+}
+
+template <int CIN, int NTC>
+constexpr size_t tc_smem_bytes(int rs) {
+  return (size_t)27 * (CIN / 8) * NTC * 16 + (size_t)3 * (CIN / 8) * rs * 16;
+}
+
+}  // namespace

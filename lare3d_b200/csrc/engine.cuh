@@ -51,6 +51,7 @@ struct Arrays {
   A3<R> f1, f2, rho_alt, cv1v, cv2v, dmv, mfx, mfy, mfz;
   // conduct.f90 temporaries
   A3<R> larsen, Y1, Y2, Y3, Lc_Y0;  // RKL2 (Y0 is read from energy itself)
+  A3<R> kf[9];                        // stage-invariant face coefficients, 3 per face direction
   // 1-D metrics (pointers at Fortran index 0)
   A1<R> dxb, dxc, dyb, dyc, dzb, dzc, grav;
   // reciprocals for conduction: 1/dxb, 1/dxc, 1/(dxc(i) + dxc(i-1)), per axis
@@ -412,81 +413,6 @@ struct TempOf {
   __device__ __forceinline__ R operator()(int i, int j, int k) const { return c * (y(i, j, k) - e0); }
 };
 
-// conduct.f90:152-291 heat_flux as a gather.  The reference scatters each
-// cell's three face fluxes into flux(c) and flux(c+e); for cell c the
-// contributions therefore arrive in loop order as
-//   +Fz(c-ez), +Fy(c-ey), +Fx(c-ex), -Fx(c), -Fy(c), -Fz(c)
-// (iteration (i,j,k-1) precedes (i,j-1,k) precedes (i-1,j,k) precedes
-// (i,j,k)), which this kernel reproduces term for term, with no atomics.
-template <class R>
-struct HeatFluxArgs {
-  TempOf<R> T;
-  A3<R> bx, by, bz, larsen;
-  A1<R> rdb[3], rdc[3], rdc2[3];
-  R k0;
-};
-
-// One face flux of conduct.f90:170-275, divided by the cell width dxb of the
-// face's index (the factor heat_flux applies when it scatters the flux).
-// Divisions by metric sums become products with reciprocals and /2 becomes
-// *0.5; only the division by |B|^2 remains.
-template <class R, class TT>
-__device__ __forceinline__ R face_flux(const HeatFluxArgs<R>& h, const TT& T, int axis, int ix, int iy, int iz) {
-  const R min_b = R(1.0e-10);  // conduct.f90:28
-  const R half = R(0.5);
-  int ixp = ix + 1, ixm = ix - 1, iyp = iy + 1, iym = iy - 1, izp = iz + 1, izm = iz - 1;
-  R lf = h.larsen(ix, iy, iz);
-  if (axis == 0) {
-    R byf = R(0.25) * (h.by(ix, iy, iz) + h.by(ixp, iy, iz) + h.by(ix, iym, iz) + h.by(ixp, iym, iz));
-    R bzf = R(0.25) * (h.bz(ix, iy, iz) + h.bz(ixp, iy, iz) + h.bz(ix, iy, izm) + h.bz(ixp, iy, izm));
-    R b0 = h.bx(ix, iy, iz);
-    R modb = b0 * b0 + byf * byf + bzf * bzf + min_b;
-    R tb = (T(ixp, iy, iz) + T(ix, iy, iz)) * half;
-    R tb_p = (T(ixp, iyp, iz) + T(ix, iyp, iz)) * half;
-    R tb_m = (T(ixp, iym, iz) + T(ix, iym, iz)) * half;
-    R tg_a1 = (tb_p - tb_m) * h.rdc2[1](iy);
-    tb_p = (T(ixp, iy, izp) + T(ix, iy, izp)) * half;
-    tb_m = (T(ixp, iy, izm) + T(ix, iy, izm)) * half;
-    R tg_a2 = (tb_p - tb_m) * h.rdc2[2](iz);
-    R tg = (T(ixp, iy, iz) - T(ix, iy, iz)) * h.rdc[0](ix);
-    tb = tb > R(0) ? tb : R(0);
-    return -lf * h.k0 * pow25(tb) * (b0 * (tg * b0 + tg_a1 * byf + tg_a2 * bzf) + tg * min_b) / modb *
-           h.rdb[0](ix);
-  } else if (axis == 1) {
-    R bxf = R(0.25) * (h.bx(ix, iy, iz) + h.bx(ix, iyp, iz) + h.bx(ixm, iy, iz) + h.bx(ixm, iyp, iz));
-    R bzf = R(0.25) * (h.bz(ix, iy, iz) + h.bz(ix, iyp, iz) + h.bz(ix, iy, izm) + h.bz(ix, iyp, izm));
-    R b0 = h.by(ix, iy, iz);
-    R modb = bxf * bxf + b0 * b0 + bzf * bzf + min_b;
-    R tb = (T(ix, iyp, iz) + T(ix, iy, iz)) * half;
-    R tb_p = (T(ixp, iy, iz) + T(ixp, iyp, iz)) * half;
-    R tb_m = (T(ixm, iyp, iz) + T(ixm, iy, iz)) * half;
-    R tg_a1 = (tb_p - tb_m) * h.rdc2[0](ix);
-    tb_p = (T(ix, iyp, izp) + T(ix, iy, izp)) * half;
-    tb_m = (T(ix, iyp, izm) + T(ix, iy, izm)) * half;
-    R tg_a2 = (tb_p - tb_m) * h.rdc2[2](iz);
-    R tg = (T(ix, iyp, iz) - T(ix, iy, iz)) * h.rdc[1](iy);
-    tb = tb > R(0) ? tb : R(0);
-    return -lf * h.k0 * pow25(tb) * (b0 * (tg * b0 + tg_a1 * bxf + tg_a2 * bzf) + tg * min_b) / modb *
-           h.rdb[1](iy);
-  } else {
-    R bxf = R(0.25) * (h.bx(ix, iy, iz) + h.bx(ix, iy, izp) + h.bx(ixm, iy, iz) + h.bx(ixm, iy, izp));
-    R byf = R(0.25) * (h.by(ix, iy, iz) + h.by(ix, iy, izp) + h.by(ix, iym, iz) + h.by(ix, iym, izp));
-    R b0 = h.bz(ix, iy, iz);
-    R modb = bxf * bxf + byf * byf + b0 * b0 + min_b;
-    R tb = (T(ix, iy, izp) + T(ix, iy, iz)) * half;
-    R tb_p = (T(ixp, iy, izp) + T(ixp, iy, iz)) * half;
-    R tb_m = (T(ixm, iy, izp) + T(ixm, iy, iz)) * half;
-    R tg_a1 = (tb_p - tb_m) * h.rdc2[0](ix);
-    tb_p = (T(ix, iyp, izp) + T(ix, iyp, iz)) * half;
-    tb_m = (T(ix, iym, izp) + T(ix, iym, iz)) * half;
-    R tg_a2 = (tb_p - tb_m) * h.rdc2[1](iy);
-    R tg = (T(ix, iy, izp) - T(ix, iy, iz)) * h.rdc[2](iz);
-    tb = tb > R(0) ? tb : R(0);
-    return -lf * h.k0 * pow25(tb) * (b0 * (tg * b0 + tg_a1 * bxf + tg_a2 * byf) + tg * min_b) / modb *
-           h.rdb[2](iz);
-  }
-}
-
 template <class R>
 void temperature_from(Run<R>& run, A3<R> e) {
   const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
@@ -547,14 +473,10 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
     gamma_tilde[j] = -1.0 * a[j - 1] * mu_tilde[j];
   }
   Arrays<R>& A = run.a;
-  auto Lc_Y0 = A.Lc_Y0, rho = A.rho, energy = A.energy;
+  auto energy = A.energy;
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
   const R tc = (g - R(1)) / (R(2) - xi), te0 = (R(1) - xi) * ip;
-  auto args = [&](A3<R> y) {
-    return HeatFluxArgs<R>{TempOf<R>{y, tc, te0}, A.bx, A.by, A.bz, A.larsen, {A.rdb[0], A.rdb[1], A.rdb[2]},
-                           {A.rdc[0], A.rdc[1], A.rdc[2]}, {A.rdc2[0], A.rdc2[1], A.rdc2[2]}, (R)run.p.kappa_0};
-  };
-  const double* sc = run.sc;
+  auto temp = [&](A3<R> y) { return TempOf<R>{y, tc, te0}; };
   if (s < 2) {
     // The stage loop is empty and energy(1:n) = Y(3)(1:n) = energy: the
     // reference leaves the energy unchanged (conduct.f90:409).
@@ -566,7 +488,8 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
   A3<R> Y1 = energy, Y2 = bufs[0], Y3 = bufs[1];
   int next_free = 2;
   copy_whole(run, Y2, energy);
-  rkl2_stage<R, true>(run, __LINE__, args(energy), energy, energy, energy, Y2, dt_slot, (R)mu_tilde[1], R(0), R(0),
+  face_coefficients(run);
+  rkl2_stage<R, true>(run, __LINE__, temp(energy), energy, energy, energy, Y2, dt_slot, (R)mu_tilde[1], R(0), R(0),
                       R(0), R(0));
   ghost(run, run.g_cell_user, Y2);
   {
@@ -577,7 +500,7 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
   for (int j = 2; j <= s; ++j) {
     const R gt = (R)gamma_tilde[j], mtj = (R)mu_tilde[j], mj = (R)mu[j], nj = (R)nu[j];
     const R omn_r = R(1) - mj - nj;
-    rkl2_stage<R, false>(run, __LINE__, args(Y2), Y2, Y1, energy, Y3, dt_slot, mtj, mj, nj, omn_r, gt);
+    rkl2_stage<R, false>(run, __LINE__, temp(Y2), Y2, Y1, energy, Y3, dt_slot, mtj, mj, nj, omn_r, gt);
     if (j < s) {
       GhostBatch<R> bb;
       bb.add(run.g_cell, Y3.p);  // energy_bcs on the copy of Y3

@@ -194,6 +194,7 @@ class EngineT : public EngineBase {
     if (p.conduction) {
       for (A3<R>* x : {&run.a.larsen, &run.a.Y1, &run.a.Y2, &run.a.Y3, &run.a.Lc_Y0})
         all.push_back(x);
+      for (int q = 0; q < 9; ++q) all.push_back(&run.a.kf[q]);
     } else {
       // conduct_heat may still be called on its own; allocate lazily there.
     }
@@ -315,7 +316,9 @@ class EngineT : public EngineBase {
     if (run.a.Y1.p) return LARE_OK;
     std::string err;
     const long long off = 2 + 2LL * run.sx + 2LL * run.sxy;
-    for (A3<R>* x : {&run.a.larsen, &run.a.Y1, &run.a.Y2, &run.a.Y3, &run.a.Lc_Y0}) {
+    std::vector<A3<R>*> list = {&run.a.larsen, &run.a.Y1, &run.a.Y2, &run.a.Y3, &run.a.Lc_Y0};
+    for (int q = 0; q < 9; ++q) list.push_back(&run.a.kf[q]);
+    for (A3<R>* x : list) {
       R* base = dalloc<R>(run.elems, err);
       if (!base) return fail(LARE_ENOMEM, err);
       x->p = base + off;

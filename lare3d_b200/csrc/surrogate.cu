@@ -43,6 +43,12 @@ __device__ __forceinline__ uint32_t pack2f(float lo, float hi) {
   return pack2(__float2bfloat16(lo), __float2bfloat16(hi));
 }
 
+}  // namespace
+
+#include "conv_tc.cuh"
+
+namespace {
+
 int current_device() {
   int d = 0;
   cudaGetDevice(&d);
@@ -177,9 +183,39 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const bf16* __restrict__ 
   }
 }
 
+bool g_use_tc = true;  // tcgen05 convolution (else the mma.sync one)
+
+template <int CIN, int NTC, int COUT>
+int launch_conv_tc(const void* x, int din, int pad, const void* w, const float* bias, void* y, int nb,
+                   const void* mask, int relu, int out_f32, cudaStream_t s) {
+  const TcGeom g = tc_geom(din, pad, nb);
+  const size_t smem = tc_smem_bytes<CIN, NTC>(g.RS);
+  if (smem > 220 * 1024) return LARE_ETOOLARGE;
+  static int attr[64] = {};
+  const int dev = current_device();
+  if (dev < 0 || dev >= 64) return LARE_ECUDA;
+  if (attr[dev] < (int)smem) {
+    if (cudaFuncSetAttribute(k_conv_tc<CIN, NTC, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return LARE_ECUDA;
+    attr[dev] = (int)smem;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long items = (long long)nb * g.E * g.ntg;
+  const unsigned blocks = (unsigned)(items < sms ? items : sms);
+  k_conv_tc<CIN, NTC, COUT><<<blocks, kTcThreads, smem, s>>>((const bf16*)x, (const bf16*)w, bias, y,
+                                                             (const bf16*)mask, g, relu, out_f32);
+  return cudaGetLastError() == cudaSuccess ? LARE_OK : LARE_ECUDA;
+}
+
 template <int CIN, int COUT>
 int launch_conv(const void* x, int din, int pad, const void* w, const float* bias, void* y, int dout, int nb,
                 const void* mask, int relu, int out_f32, cudaStream_t s) {
+  if (g_use_tc) {
+    (void)dout;
+    return launch_conv_tc<CIN, (COUT < 16 ? 16 : COUT), COUT>(x, din, pad, w, bias, y, nb, mask, relu, out_f32, s);
+  }
   constexpr size_t smem = conv_smem<CIN, COUT>();
   static bool attr[64] = {};
   const int dev = current_device();
@@ -553,6 +589,21 @@ int lare_sur_conv(int cin, int cout, int relu, int out_f32, const void* x, int d
   if (cin == 32 && cout == 32) return launch_conv<32, 32>(x, din, pad, w, bias, y, dout, nb, mask, relu, out_f32, s);
   if (cin == 32 && cout == 8) return launch_conv<32, 8>(x, din, pad, w, bias, y, dout, nb, mask, relu, out_f32, s);
   return LARE_EINVAL;
+}
+
+int lare_sur_set_engine(int tensor_cores) {
+  g_use_tc = tensor_cores != 0;
+  return LARE_OK;
+}
+
+int lare_sur_status(int clear) {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_sur_status, sizeof(int)) != cudaSuccess) return LARE_ECUDA;
+  if (clear) {
+    const int z = 0;
+    if (cudaMemcpyToSymbol(g_sur_status, &z, sizeof(int)) != cudaSuccess) return LARE_ECUDA;
+  }
+  return v;
 }
 
 long long lare_sur_conv_wgrad_work(int cin, int cout, int dout, int nb) {

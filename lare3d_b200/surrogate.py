@@ -82,6 +82,12 @@ class _Lib:
         w.argtypes = [i, i, i, i]
         w.restype = ll
         self.wgrad_work = w
+        lib.lare_sur_set_engine.argtypes = [i]
+        lib.lare_sur_set_engine.restype = i
+        lib.lare_sur_status.argtypes = [i]
+        lib.lare_sur_status.restype = i
+        self.set_engine = lambda tc: lib.lare_sur_set_engine(1 if tc else 0)
+        self.status = lambda clear=True: lib.lare_sur_status(1 if clear else 0)
 
     @staticmethod
     def _checked(fn, name):

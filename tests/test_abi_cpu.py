@@ -15,7 +15,7 @@ from lare3d_b200.abi import LareParams, default_params
 
 def declared(header):
     txt = open(os.path.join(ROOT, "include", header)).read()
-    return sorted(set(re.findall(r"\b(lare_(?:gpu|sur)_\w+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(lare_(?:gpu|sur|ens)_\w+)\s*\(", txt)))
 
 
 def test_exports_every_declared_symbol(built):
@@ -24,7 +24,8 @@ def test_exports_every_declared_symbol(built):
     names = declared("lare_gpu.h")
     assert len(names) >= 20
     sur = declared("lare_surrogate.h")
-    assert len(sur) == 11
+    assert len(sur) == 13
+    assert {"lare_ens_create", "lare_ens_launch", "lare_ens_sync", "lare_ens_destroy"} <= set(names)
     missing = [n for n in names + sur if not hasattr(lib, n)]
     assert not missing, missing
 
