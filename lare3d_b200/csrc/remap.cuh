@@ -11,6 +11,8 @@
 //                 is recomputed in the thread for dxc1.
 //   K2 B fluxes   both constrained-transport edge fluxes (:340-470); the
 //                 second does not read what the first one's updates change.
+//                 The y and z sweeps use a marching kernel (each quotient
+//                 formed once); the x sweep forms them per cell.
 //   K3 B update   the four flux-difference updates (:121-157), with each
 //                 file's own loop ranges as predicates.
 //   K4 mass flux  dm (:474-533) over the whole cell box, with dm_x_bcs
@@ -37,6 +39,123 @@ namespace lare {
 template <int A>
 __device__ __forceinline__ int acoord(int ix, int iy, int iz) {
   return A == 0 ? ix : (A == 1 ? iy : iz);
+}
+
+// K2 for the y and z sweeps as a marching kernel.  A thread owns a run of
+// kMarch consecutive cells along the sweep axis A at one (x, transverse)
+// position and walks it, keeping the quotients B/dbv, the dbv and the db1
+// and dc1 values of the four-point stencil in registers: each step loads
+// the one new stencil point instead of all four and forms one quotient per
+// flux instead of four.  Every value is the same expression of the same
+// operands as in the per-cell form, so the fluxes are identical bit for bit.
+constexpr int kMarch = 32;
+
+template <class R>
+struct BfArgs {
+  const R* va;           // velocity component along A (v1 of the reference)
+  const R* b1;           // first transported component
+  const R* b2;           // second
+  const R* db1;
+  const R* dc1;
+  R* f1;
+  R* f2;
+  const double* sc;
+  int dt_slot;
+  int SA, SB1, SB2, SO1, SO2;  // strides along A, the two components' own axes, and their remaining axes
+  int SX, SY;                  // strides of the thread grid's two axes (x and the other transverse axis)
+  int na;                      // cells along A
+  int n0, n1;                  // extents of the thread grid (-1..n+1 each)
+};
+
+template <class R>
+__device__ __forceinline__ R bf_quot(const R* Bb, const R* db1, int q, int SB, R& dbv) {
+  dbv = (db1[q] + db1[q + SB]) * R(0.5);
+  return Bb[q] / dbv;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t1 = blockIdx.y * blockDim.y + threadIdx.y;
+  if (t0 >= a.n0 || t1 >= a.n1) return;
+  const int ia0 = -1 + (int)blockIdx.z * kMarch;
+  const int ia1 = min(ia0 + kMarch - 1, a.na + 1);
+  const int SA = a.SA;
+  // cell (t0 - 1, t1 - 1, ia0) in grid / along-A coordinates
+  int c = (t0 - 1) * a.SX + (t1 - 1) * a.SY + ia0 * SA;
+  const R dt = (R)a.sc[a.dt_slot];
+  // four-point windows at cm, c, cp, cp2 (clamped as MAX(ia-1,-1), MIN(ia+2,na+2))
+  R q1m, q10, q1p, q1p2, d1m, d10, d1p, d1p2;  // flux 1: quotients, dbv
+  R q2m, q20, q2p, q2p2, d2m, d20, d2p, d2p2;  // flux 2
+  R dcm, dc0, dcp, dbc0, dbcp;                 // dc1 at cm, c, cp; db1 at c, cp
+  {
+    const int cm = ia0 > -1 ? c - SA : c;
+    const int cp = c + SA;
+    const int cp2 = ia0 + 2 <= a.na + 2 ? c + 2 * SA : cp;
+    q1m = bf_quot(a.b1, a.db1, cm, a.SB1, d1m);
+    q10 = bf_quot(a.b1, a.db1, c, a.SB1, d10);
+    q1p = bf_quot(a.b1, a.db1, cp, a.SB1, d1p);
+    q1p2 = bf_quot(a.b1, a.db1, cp2, a.SB1, d1p2);
+    q2m = bf_quot(a.b2, a.db1, cm, a.SB2, d2m);
+    q20 = bf_quot(a.b2, a.db1, c, a.SB2, d20);
+    q2p = bf_quot(a.b2, a.db1, cp, a.SB2, d2p);
+    q2p2 = bf_quot(a.b2, a.db1, cp2, a.SB2, d2p2);
+    dcm = a.dc1[cm];
+    dc0 = a.dc1[c];
+    dcp = a.dc1[cp];
+    dbc0 = a.db1[c];
+    dbcp = a.db1[cp];
+  }
+  (void)d1m;
+  (void)d2m;
+  for (int ia = ia0; ia <= ia1; ++ia) {
+    // issue the next step's loads before this step's arithmetic
+    const int cn = c + SA;
+    const bool more = ia < ia1;
+    const bool clamp = ia + 3 > a.na + 2;
+    const int qn = cn + 2 * SA;
+    const bool fetch = more && !clamp;
+    R nb1 = R(0), nb2 = R(0), nd = R(0), nd1 = R(0), nd2 = R(0), ndc = R(0), ndb = R(0);
+    if (fetch) {
+      nb1 = a.b1[qn];
+      nb2 = a.b2[qn];
+      nd = a.db1[qn];
+      nd1 = a.db1[qn + a.SB1];
+      nd2 = a.db1[qn + a.SB2];
+    }
+    if (more) {
+      ndc = a.dc1[cn + SA];
+      ndb = a.db1[cn + SA];
+    }
+    const R va0 = a.va[c], va1 = a.va[c - a.SO1], va2 = a.va[c - a.SO2];
+    {
+      const R v_advect = (va0 + va1) * R(0.5);
+      LimOut<R> L = limiter<R>(v_advect, q1m, q10, q1p, q1p2, dc0, dcm, dcp, dbc0, dbcp, d10, d1p, dt, true);
+      a.f1[c] = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
+    }
+    {
+      const R v_advect = (va0 + va2) * R(0.5);
+      LimOut<R> L = limiter<R>(v_advect, q2m, q20, q2p, q2p2, dc0, dcm, dcp, dbc0, dbcp, d20, d2p, dt, true);
+      a.f2[c] = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
+    }
+    if (!more) break;
+    q1m = q10; q10 = q1p; q1p = q1p2;
+    d10 = d1p; d1p = d1p2;
+    q2m = q20; q20 = q2p; q2p = q2p2;
+    d20 = d2p; d2p = d2p2;
+    if (clamp) {
+      q1p2 = q1p; d1p2 = d1p;
+      q2p2 = q2p; d2p2 = d2p;
+    } else {
+      d1p2 = (nd + nd1) * R(0.5);
+      q1p2 = nb1 / d1p2;
+      d2p2 = (nd + nd2) * R(0.5);
+      q2p2 = nb2 / d2p2;
+    }
+    dcm = dc0; dc0 = dcp; dcp = ndc;
+    dbc0 = dbcp; dbcp = ndb;
+    c = cn;
+  }
 }
 
 template <int A, class R>
@@ -112,7 +231,34 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   R* const Bp[3] = {Ar.bx.p, Ar.by.p, Ar.bz.p};
   R* const f1 = Ar.f1.p;
   R* const f2 = Ar.f2.p;
-  {
+  if (A != 0) {
+    BfArgs<R> ba;
+    ba.va = va;
+    ba.b1 = Bp[B1];
+    ba.b2 = Bp[B2];
+    ba.db1 = db1;
+    ba.dc1 = dc1;
+    ba.f1 = f1;
+    ba.f2 = f2;
+    ba.sc = sc;
+    ba.dt_slot = dt_slot;
+    ba.SA = SA;
+    ba.SB1 = SB1;
+    ba.SB2 = SB2;
+    ba.SO1 = SO1;
+    ba.SO2 = SO2;
+    ba.SX = 1;
+    ba.SY = A == 1 ? sxy : sx;     // the grid's second axis: z for the y sweep, y for the z sweep
+    ba.na = na;
+    ba.n0 = nx + 3;
+    ba.n1 = (A == 1 ? nz : ny) + 3;
+    const int k = run.prof_begin("remap_sweep_bflux", A, 7, (double)(nx + 3) * (ny + 3) * (nz + 3));
+    dim3 blk(64, 4, 1);
+    dim3 grd((ba.n0 + 63) / 64, (ba.n1 + 3) / 4, (na + 3 + kMarch - 1) / kMarch);
+    k_bflux_march<R><<<grd, blk, 0, run.s>>>(ba);
+    run.prof_end(k);
+    ++run.launches;
+  } else {
     R* const Bb1 = Bp[B1];
     R* const Bb2 = Bp[B2];
     LARE_BOXW(run, 7, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
@@ -296,13 +442,29 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
       R rvc = rv[c], rvp = rv[cp], dmc = dmv[c];
       const R* Vc[3] = {vxp, vyp, vzp};
       R* Fo[3] = {mfx, mfy, mfz};
+      // The upwind choice, phi and dmu depend only on v_advect and the
+      // geometry, so they are formed once for the three components (the
+      // same expressions the limiter evaluates per component).
+      const R dxci = db1[cp], dxcm = db1[c], dxcp = db1[cp2], dxbi = dc1[c], dxbp = dc1[cp];
+      const R sign_v = copysign(R(1), v_advect);
+      const R vad_p = (sign_v + R(1)) * R(0.5);
+      const R vad_m = R(1) - vad_p;
+      const R dxcu = dxcm * vad_p + dxcp * vad_m;
+      const R dxbu = dxbi * vad_p + dxbp * vad_m;
+      const R phi = fabs(v_advect) * dt / dxbu;
+      const R rhou = rvc * vad_p + rvp * vad_m;
+      const R dmu = fabs(dmc) / area / dxbu / rhou;
       for (int comp = 0; comp < 3; ++comp) {
         const R* vc = Vc[comp];
-        LimOut<R> L = limiter<R>(v_advect, vc[cm], vc[c], vc[cp], vc[cp2], db1[cp], db1[c], db1[cp2], dc1[c],
-                                 dc1[cp], R(0), R(0), dt, false);
-        R rhou = rvc * L.vad_p + rvp * L.vad_m;
-        R dmu = fabs(dmc) / area / L.dxbu / rhou;
-        R f = L.fu + L.Di * (R(1) - dmu);
+        const R fm = vc[cm], fi = vc[c], fp = vc[cp], fp2 = vc[cp2];
+        const R dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
+        const R fu = fi * vad_p + fp * vad_m;
+        const R dfu = dfm * vad_p + dfp * vad_m;
+        R Da = (R(2) - phi) * fabs(dfi) / dxci + (R(1) + phi) * fabs(dfu) / dxcu;
+        Da = Da * (R(1) / R(6));
+        const R ss = R(0.5) * (copysign(R(1), dfi) + copysign(R(1), dfu));
+        const R Di = sign_v * ss * fmin(fmin(fabs(Da) * dxbu, fabs(dfi)), fabs(dfu));
+        const R f = fu + Di * (R(1) - dmu);
         Fo[comp][c] = f * dmc;
       }
     });
