@@ -45,6 +45,11 @@ void face_coefficients(Run<R>& run) {
   A3<R> k[9];
   for (int q = 0; q < 9; ++q) k[q] = A.kf[q];
   const A3<R> k0 = k[0], k1 = k[1], k2 = k[2], k3 = k[3], k4 = k[4], k5 = k[5], k6 = k[6], k7 = k[7], k8 = k[8];
+  // Extension, not in the reference: kappa_perp = rp kappa_par adds
+  // rp (g_n - b_n (b . g) / |B|^2) to the bracket, i.e. rp (|B|^2 - b0^2)
+  // to the normal coefficient's numerator and a factor (1 - rp) to the
+  // transverse ones; rp = 0 is the reference's flux.
+  const R rp = (R)run.p.kappa_perp_ratio, orp = R(1) - rp;
   LARE_BOXW(run, 13, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     const R min_b = R(1.0e-10);  // conduct.f90:28
     const R half = R(0.5), q4 = R(0.25);
@@ -54,28 +59,31 @@ void face_coefficients(Run<R>& run) {
       const R byf = q4 * (by(ix, iy, iz) + by(ixp, iy, iz) + by(ix, iym, iz) + by(ixp, iym, iz));
       const R bzf = q4 * (bz(ix, iy, iz) + bz(ixp, iy, iz) + bz(ix, iy, izm) + bz(ixp, iy, izm));
       const R b0 = bx(ix, iy, iz);
-      const R w = lf / (b0 * b0 + byf * byf + bzf * bzf + min_b) * rdb0(ix);
-      k0(ix, iy, iz) = w * (b0 * b0 + min_b) * rdc0(ix);
-      k1(ix, iy, iz) = w * b0 * byf * half * rs1(iy);
-      k2(ix, iy, iz) = w * b0 * bzf * half * rs2(iz);
+      const R modb = b0 * b0 + byf * byf + bzf * bzf + min_b;
+      const R w = lf / modb * rdb0(ix);
+      k0(ix, iy, iz) = w * ((b0 * b0 + min_b) + rp * (modb - b0 * b0)) * rdc0(ix);
+      k1(ix, iy, iz) = w * b0 * byf * orp * half * rs1(iy);
+      k2(ix, iy, iz) = w * b0 * bzf * orp * half * rs2(iz);
     }
     {  // y face
       const R bxf = q4 * (bx(ix, iy, iz) + bx(ix, iyp, iz) + bx(ixm, iy, iz) + bx(ixm, iyp, iz));
       const R bzf = q4 * (bz(ix, iy, iz) + bz(ix, iyp, iz) + bz(ix, iy, izm) + bz(ix, iyp, izm));
       const R b0 = by(ix, iy, iz);
-      const R w = lf / (bxf * bxf + b0 * b0 + bzf * bzf + min_b) * rdb1(iy);
-      k3(ix, iy, iz) = w * (b0 * b0 + min_b) * rdc1(iy);
-      k4(ix, iy, iz) = w * b0 * bxf * half * rs0(ix);
-      k5(ix, iy, iz) = w * b0 * bzf * half * rs2(iz);
+      const R modb = bxf * bxf + b0 * b0 + bzf * bzf + min_b;
+      const R w = lf / modb * rdb1(iy);
+      k3(ix, iy, iz) = w * ((b0 * b0 + min_b) + rp * (modb - b0 * b0)) * rdc1(iy);
+      k4(ix, iy, iz) = w * b0 * bxf * orp * half * rs0(ix);
+      k5(ix, iy, iz) = w * b0 * bzf * orp * half * rs2(iz);
     }
     {  // z face
       const R bxf = q4 * (bx(ix, iy, iz) + bx(ix, iy, izp) + bx(ixm, iy, iz) + bx(ixm, iy, izp));
       const R byf = q4 * (by(ix, iy, iz) + by(ix, iy, izp) + by(ix, iym, iz) + by(ix, iym, izp));
       const R b0 = bz(ix, iy, iz);
-      const R w = lf / (bxf * bxf + byf * byf + b0 * b0 + min_b) * rdb2(iz);
-      k6(ix, iy, iz) = w * (b0 * b0 + min_b) * rdc2(iz);
-      k7(ix, iy, iz) = w * b0 * bxf * half * rs0(ix);
-      k8(ix, iy, iz) = w * b0 * byf * half * rs1(iy);
+      const R modb = bxf * bxf + byf * byf + b0 * b0 + min_b;
+      const R w = lf / modb * rdb2(iz);
+      k6(ix, iy, iz) = w * ((b0 * b0 + min_b) + rp * (modb - b0 * b0)) * rdc2(iz);
+      k7(ix, iy, iz) = w * b0 * bxf * orp * half * rs0(ix);
+      k8(ix, iy, iz) = w * b0 * byf * orp * half * rs1(iy);
     }
   });
 }

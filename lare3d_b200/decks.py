@@ -165,11 +165,14 @@ def orszag_tang(n: int = 256, seed: int = 7, amp: float = 1.0e-3, **over) -> Dec
 
 
 def conduction(n: int = 256, seed: int = 11, nspots: int = 8, T0: float = 1.0,
-               kappa_0: float = 1.0e-3, dt_ratio: float = 50.0, **over) -> Deck:
-    """Sheared-arcade conduction workload: x, y periodic; z BC_USER."""
+               kappa_0: float = 1.0e-3, dt_ratio: float = 50.0, kappa_perp_ratio: float = 1.0e-6,
+               **over) -> Deck:
+    """Sheared-arcade conduction workload: x, y periodic; z BC_USER.
+    kappa_perp_ratio = kappa_perp / kappa_par of the workload (an extension:
+    the reference has no cross-field term; 0 gives its flux exactly)."""
     g = 5.0 / 3.0
     p = default_params(gamma=g, conduction=1, heat_flux_limiter=1, flux_limiter=0.1,
-                       kappa_0=kappa_0, dt_multiplier=0.9,
+                       kappa_0=kappa_0, dt_multiplier=0.9, kappa_perp_ratio=kappa_perp_ratio,
                        zbc_min=BC_USER, zbc_max=BC_USER)
     for k, v in over.items():
         setattr(p, k, v)

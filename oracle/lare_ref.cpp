@@ -1223,6 +1223,10 @@ struct lare_ref {
   inline double face_flux(int axis, int ix, int iy, int iz) {
     F3& T = temperature;
     const double k0 = p.kappa_0;
+    // Extension, not in the reference: a cross-field conductivity
+    // kappa_perp = rp kappa_par adds rp (g_n - b_n (b . g) / |b|^2) to the
+    // bracket; rp = 0 leaves the reference's expression untouched.
+    const double rp = p.kappa_perp_ratio;
     int ixp = ix + 1, ixm = ix - 1, iyp = iy + 1, iym = iy - 1, izp = iz + 1, izm = iz - 1;
     double lf = larsen_factor(ix, iy, iz);
     if (axis == 0) {
@@ -1239,6 +1243,10 @@ struct lare_ref {
       double tg_a2 = (tb_p - tb_m) / (dzc(iz) + dzc(izm));
       double tg = (T(ixp, iy, iz) - T(ix, iy, iz)) / dxc(ix);
       tb = fmax0(tb);
+      if (rp != 0.0) {
+        double bg = b0 * (tg * b0 + tg_a1 * byf + tg_a2 * bzf);
+        return -lf * k0 * std::pow(tb, pow_c) * ((bg + tg * min_b) / modb + rp * (tg - bg / modb));
+      }
       return -lf * k0 * std::pow(tb, pow_c) * (b0 * (tg * b0 + tg_a1 * byf + tg_a2 * bzf) + tg * min_b) / modb;
     } else if (axis == 1) {
       double bxf = 0.25 * (bx(ix, iy, iz) + bx(ix, iyp, iz) + bx(ixm, iy, iz) + bx(ixm, iyp, iz));
@@ -1254,6 +1262,10 @@ struct lare_ref {
       double tg_a2 = (tb_p - tb_m) / (dzc(iz) + dzc(izm));
       double tg = (T(ix, iyp, iz) - T(ix, iy, iz)) / dyc(iy);
       tb = fmax0(tb);
+      if (rp != 0.0) {
+        double bg = b0 * (tg * b0 + tg_a1 * bxf + tg_a2 * bzf);
+        return -lf * k0 * std::pow(tb, pow_c) * ((bg + tg * min_b) / modb + rp * (tg - bg / modb));
+      }
       return -lf * k0 * std::pow(tb, pow_c) * (b0 * (tg * b0 + tg_a1 * bxf + tg_a2 * bzf) + tg * min_b) / modb;
     } else {
       double bxf = 0.25 * (bx(ix, iy, iz) + bx(ix, iy, izp) + bx(ixm, iy, iz) + bx(ixm, iy, izp));
@@ -1269,6 +1281,10 @@ struct lare_ref {
       double tg_a2 = (tb_p - tb_m) / (dyc(iy) + dyc(iym));
       double tg = (T(ix, iy, izp) - T(ix, iy, iz)) / dzc(iz);
       tb = fmax0(tb);
+      if (rp != 0.0) {
+        double bg = b0 * (tg * b0 + tg_a1 * bxf + tg_a2 * byf);
+        return -lf * k0 * std::pow(tb, pow_c) * ((bg + tg * min_b) / modb + rp * (tg - bg / modb));
+      }
       return -lf * k0 * std::pow(tb, pow_c) * (b0 * (tg * b0 + tg_a1 * bxf + tg_a2 * byf) + tg * min_b) / modb;
     }
   }

@@ -166,3 +166,39 @@ def test_invalid_arguments(built):
     s = oracle_sim(d)
     with pytest.raises(LareError):
         s.get_field("no_such_array")
+
+
+def _layered(kperp, n=12):
+    """B along x, T varying in y only: field-aligned conduction has nothing
+    to do; only a cross-field conductivity moves heat."""
+    from lare3d_b200 import decks
+    from oracle import oracle
+    d = decks.conduction(n, kappa_perp_ratio=kperp)
+    st = d.state
+    st["bx"][...] = 1.0
+    st["by"][...] = 0.0
+    st["bz"][...] = 0.0
+    y = np.arange(-1, n + 3) / n
+    T = 1.0 + 0.5 * np.sin(2 * np.pi * y)
+    g = d.params.gamma
+    st["energy"][...] = np.broadcast_to((T * 2.0 / (g - 1.0))[None, :, None], st["energy"].shape)
+    st["rho"][...] = 1.0
+    s = oracle.simulation(d)
+    s.start(st)
+    e0 = s.get_field("energy").copy()
+    s.conduct_heat(50.0 * decks.dt_parab_estimate(st, d.metrics, d.params, n))
+    return e0, s.get_field("energy")
+
+
+def test_kappa_perp_extension_moves_heat_across_the_field(built):
+    e0, e_par = _layered(0.0)
+    _, e_perp = _layered(0.05)
+    core = (slice(2, -2),) * 3
+    # field-aligned only: the min_b regulariser (1e-10 of |B|^2) is all that leaks
+    assert np.max(np.abs(e_par[core] - e0[core])) < 1e-8 * np.max(np.abs(e0[core]))
+    # with kappa_perp the y profile relaxes: peaks cool, troughs warm
+    d = e_perp[core] - e0[core]
+    assert np.max(np.abs(d)) > 1e-4 * np.max(np.abs(e0[core]))
+    dev = e0[core] - e0[core].mean()
+    assert np.corrcoef(dev.ravel(), d.ravel())[0, 1] < -0.5
+    assert d.ravel()[np.argmax(dev)] < 0 < d.ravel()[np.argmin(dev)]

@@ -124,8 +124,10 @@ def test_orszag_tang_32_50_steps(built):
         assert np.array_equal(g.get_field(f), r.get_field(f)), f
 
 
-def test_conduction_parity(built):
-    d = decks.conduction(16)
+@pytest.mark.parametrize("kperp", [0.0, 1.0e-6, 0.05])
+def test_conduction_parity(built, kperp):
+    """Reference flux (kperp = 0) and the cross-field extension."""
+    d = decks.conduction(16, kappa_perp_ratio=kperp)
     r, g = pair(d)
     for it in range(2):
         assert r.conduct_heat(d.dt_fixed) == g.conduct_heat(d.dt_fixed)
