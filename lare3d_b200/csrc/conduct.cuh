@@ -104,12 +104,22 @@ __device__ __forceinline__ R face_q(R k0, R T0, R T1, R kn, R k1, R s1, R k2, R 
   return -k0 * pow25(tb) * (kn * (T1 - T0) + k1 * s1 + k2 * s2);
 }
 
+// Per-plane operands of one thread, loaded a plane ahead.  Thread (tx, ty)
+// owns the x face below its cell (plus the last face of the row for
+// tx = 31), the y face below its cell (plus the last one for ty = 7), the z
+// face above its cell, and the cell's own stage data.
+template <class R>
+struct StagePre {
+  R kx[3], kx2[3], ky[3], ky2[3], kz[3];
+  R rho, y0, y1, y2, lc;
+};
+
 // FIRST: stage 1 (y2 = energy = Y0): Lc_Y0 = flux / rho and
 //        out = Y0 + mt * dt * Lc_Y0.
 // else:  stage j: out = mu Y2 + nu Y1 + (1 - mu - nu) Y0 + mt dt Lc + gt dt Lc_Y0
 //        with Lc the flux of T(Y2) / rho.
 template <class R, bool FIRST>
-__global__ void __launch_bounds__(kCTX* kCTY) k_rkl2_stage(StageArgs<R> a, const double* __restrict__ sc) {
+__global__ void __launch_bounds__(kCTX* kCTY, sizeof(R) == 4 ? 4 : 2) k_rkl2_stage(StageArgs<R> a, const double* __restrict__ sc) {
   __shared__ R Ts[3][kCPlane];
   __shared__ R fx[kCTY][kCTX + 1];
   __shared__ R fy[kCTY + 1][kCTX];
@@ -121,6 +131,11 @@ __global__ void __launch_bounds__(kCTX* kCTY) k_rkl2_stage(StageArgs<R> a, const
   const int iz1 = min(nz, iz0 + kCZ - 1);
   const int ix = ix0 + tx, iy = iy0 + ty;
   const bool active = ix <= nx && iy <= ny;
+  // faces owned by this thread (see StagePre)
+  const bool hx = ix - 1 <= nx && iy <= ny;                              // x face at ix - 1
+  const bool hx2 = tx == kCTX - 1 && ix <= nx && iy <= ny;               // x face at ix (row end)
+  const bool hy = ix <= nx && iy - 1 <= ny;                              // y face at iy - 1
+  const bool hy2 = ty == kCTY - 1 && ix <= nx && iy <= ny;               // y face at iy (column end)
   const R dt = (R)sc[a.dt_slot];
   auto load_plane = [&](int k) {
     R* d = Ts[(k + 3) % 3];
@@ -130,45 +145,75 @@ __global__ void __launch_bounds__(kCTX* kCTY) k_rkl2_stage(StageArgs<R> a, const
       d[e] = a.T(i, j, k);
     }
   };
+  auto fetch = [&](int k) {
+    StagePre<R> q;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      q.kx[m] = hx ? a.k[m](ix - 1, iy, k) : R(0);
+      q.kx2[m] = hx2 ? a.k[m](ix, iy, k) : R(0);
+      q.ky[m] = hy ? a.k[3 + m](ix, iy - 1, k) : R(0);
+      q.ky2[m] = hy2 ? a.k[3 + m](ix, iy, k) : R(0);
+      q.kz[m] = active ? a.k[6 + m](ix, iy, k) : R(0);
+    }
+    q.rho = active ? a.rho(ix, iy, k) : R(1);
+    q.y0 = active ? a.y0(ix, iy, k) : R(0);
+    q.y1 = (active && !FIRST) ? a.y1(ix, iy, k) : R(0);
+    q.y2 = (active && !FIRST) ? a.y2(ix, iy, k) : R(0);
+    q.lc = (active && !FIRST) ? a.lc0(ix, iy, k) : R(0);
+    return q;
+  };
   // z face above cell (lr, lc) of plane slots pm (lower) and pp (upper)
-  auto zface = [&](const R* pm, const R* pp, int lr, int lc, int i, int j, int k) {
-    const int e = lr * kCW + lc;
-    return face_q(a.k0, pm[e], pp[e], a.k[6](i, j, k), a.k[7](i, j, k),
-                  (pp[e + 1] + pm[e + 1]) - (pp[e - 1] + pm[e - 1]), a.k[8](i, j, k),
+  auto zface = [&](const R* pm, const R* pp, int e, R k6, R k7, R k8) {
+    return face_q(a.k0, pm[e], pp[e], k6, k7, (pp[e + 1] + pm[e + 1]) - (pp[e - 1] + pm[e - 1]), k8,
                   (pp[e + kCW] + pm[e + kCW]) - (pp[e - kCW] + pm[e - kCW]));
   };
+  const int ec = (ty + 1) * kCW + tx + 1;  // this thread's cell in a plane slot
   load_plane(iz0 - 1);
   load_plane(iz0);
   R fz_m = R(0);
+  R b6 = R(0), b7 = R(0), b8 = R(0);
+  if (active) {
+    b6 = a.k[6](ix, iy, iz0 - 1);
+    b7 = a.k[7](ix, iy, iz0 - 1);
+    b8 = a.k[8](ix, iy, iz0 - 1);
+  }
+  __syncthreads();
+  if (active) fz_m = zface(Ts[(iz0 + 2) % 3], Ts[iz0 % 3], ec, b6, b7, b8);
+  StagePre<R> nxt = fetch(iz0);
   for (int iz = iz0; iz <= iz1; ++iz) {
+    const StagePre<R> cur = nxt;
     load_plane(iz + 1);
+    if (iz < iz1) nxt = fetch(iz + 1);
     __syncthreads();
     const R* Pm = Ts[(iz + 2) % 3];
     const R* P0 = Ts[iz % 3];
     const R* Pp = Ts[(iz + 1) % 3];
-    if (iz == iz0 && active) fz_m = zface(Pm, P0, ty + 1, tx + 1, ix, iy, iz - 1);
-    for (int f = tid; f < kCTY * (kCTX + 1); f += kCTX * kCTY) {
-      const int r = f / (kCTX + 1), c = f - r * (kCTX + 1);
-      const int fi = ix0 - 1 + c, fj = iy0 + r;
-      if (fi <= nx && fj <= ny) {
-        const int e = (r + 1) * kCW + c;  // cell fi of row fj
-        fx[r][c] = face_q(a.k0, P0[e], P0[e + 1], a.k[0](fi, fj, iz), a.k[1](fi, fj, iz),
-                          (P0[e + kCW + 1] + P0[e + kCW]) - (P0[e - kCW + 1] + P0[e - kCW]), a.k[2](fi, fj, iz),
+    if (hx) {
+      const int e = ec - 1;  // cell ix - 1
+      fx[ty][tx] = face_q(a.k0, P0[e], P0[e + 1], cur.kx[0], cur.kx[1],
+                          (P0[e + kCW + 1] + P0[e + kCW]) - (P0[e - kCW + 1] + P0[e - kCW]), cur.kx[2],
                           (Pp[e + 1] + Pp[e]) - (Pm[e + 1] + Pm[e]));
-      }
     }
-    for (int f = tid; f < (kCTY + 1) * kCTX; f += kCTX * kCTY) {
-      const int r = f / kCTX, c = f - r * kCTX;
-      const int fi = ix0 + c, fj = iy0 - 1 + r;
-      if (fi <= nx && fj <= ny) {
-        const int e = r * kCW + c + 1;  // cell fi of row fj
-        fy[r][c] = face_q(a.k0, P0[e], P0[e + kCW], a.k[3](fi, fj, iz), a.k[4](fi, fj, iz),
-                          (P0[e + 1] + P0[e + kCW + 1]) - (P0[e - 1] + P0[e + kCW - 1]), a.k[5](fi, fj, iz),
+    if (hx2) {
+      const int e = ec;
+      fx[ty][kCTX] = face_q(a.k0, P0[e], P0[e + 1], cur.kx2[0], cur.kx2[1],
+                            (P0[e + kCW + 1] + P0[e + kCW]) - (P0[e - kCW + 1] + P0[e - kCW]), cur.kx2[2],
+                            (Pp[e + 1] + Pp[e]) - (Pm[e + 1] + Pm[e]));
+    }
+    if (hy) {
+      const int e = ec - kCW;  // cell iy - 1
+      fy[ty][tx] = face_q(a.k0, P0[e], P0[e + kCW], cur.ky[0], cur.ky[1],
+                          (P0[e + 1] + P0[e + kCW + 1]) - (P0[e - 1] + P0[e + kCW - 1]), cur.ky[2],
                           (Pp[e] + Pp[e + kCW]) - (Pm[e] + Pm[e + kCW]));
-      }
+    }
+    if (hy2) {
+      const int e = ec;
+      fy[kCTY][tx] = face_q(a.k0, P0[e], P0[e + kCW], cur.ky2[0], cur.ky2[1],
+                            (P0[e + 1] + P0[e + kCW + 1]) - (P0[e - 1] + P0[e + kCW - 1]), cur.ky2[2],
+                            (Pp[e] + Pp[e + kCW]) - (Pm[e] + Pm[e + kCW]));
     }
     R fz_p = R(0);
-    if (active) fz_p = zface(P0, Pp, ty + 1, tx + 1, ix, iy, iz);
+    if (active) fz_p = zface(P0, Pp, ec, cur.kz[0], cur.kz[1], cur.kz[2]);
     __syncthreads();
     if (active) {
       R f = R(0);
@@ -179,14 +224,14 @@ __global__ void __launch_bounds__(kCTX* kCTY) k_rkl2_stage(StageArgs<R> a, const
       f = f - fy[ty + 1][tx];
       f = f - fz_p;
       if (FIRST) {
-        const R lc = (R(1) / a.rho(ix, iy, iz)) * f;
+        const R lc = (R(1) / cur.rho) * f;
         a.lc0(ix, iy, iz) = lc;
-        a.out(ix, iy, iz) = a.y0(ix, iy, iz) + a.mt * dt * lc;
+        a.out(ix, iy, iz) = cur.y0 + a.mt * dt * lc;
       } else {
-        const R c0 = a.gt * dt * a.lc0(ix, iy, iz);
-        const R Lc = (R(1) / a.rho(ix, iy, iz)) * f;
+        const R c0 = a.gt * dt * cur.lc;
+        const R Lc = (R(1) / cur.rho) * f;
         const R c1 = a.mt * dt * Lc;
-        const R v = a.mu * a.y2(ix, iy, iz) + a.nu * a.y1(ix, iy, iz) + a.omn * a.y0(ix, iy, iz);
+        const R v = a.mu * cur.y2 + a.nu * cur.y1 + a.omn * cur.y0;
         a.out(ix, iy, iz) = v + c1 + c0;
       }
     }

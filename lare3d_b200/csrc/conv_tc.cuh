@@ -5,8 +5,11 @@
 // voxels are numbered r = oy*D + ox with the INPUT row length D (columns
 // ox >= E = D - 2 are computed and dropped), so that for tap (dz, dy, dx)
 // the input voxel of row r is row r + dy*D + dx of input plane oz + dz: one
-// constant shift per tap.  A CTA stages the three input planes' rows
-// [r0, r0 + RS) in shared memory as [plane][channel group of 8][row][8 bf16]
+// constant shift per tap.  A work item is NY whole output rows of one plane;
+// the tensor memory accelerator (cp.async.bulk.tensor, one 5-D box per input
+// plane and channel group, zero fill outside the input, which also provides
+// the padding of the backward-data convolution) stages the three input
+// planes' rows in shared memory as [plane][channel group of 8][row][8 bf16]
 // -- the no-swizzle K-major operand layout, in which 8 consecutive rows of
 // 16 bytes form one core matrix -- so the A operand of every tap is the same
 // buffer with a different start address.  The weights stay resident as
@@ -15,7 +18,7 @@
 // accumulator tiles in tensor memory, commits them to an mbarrier, and the
 // four warps read their 32 lanes back (tcgen05.ld), add the bias, apply the
 // ReLU or the mask and store bf16 or FP32.  Padding (pad = 2, the
-// backward-data convolution) is zero fill during staging.
+// backward-data convolution) comes from the zero fill of the staging.
 //
 // Every wait is bounded; a wait that runs out records kErrWait in the
 // device status word and the CTA frees its tensor memory and returns.
@@ -123,29 +126,46 @@ struct TcGeom {
   int din;    // real input edge
   int pad;    // 0 or 2
   int nb;
-  int RS;     // staged rows per plane (odd multiple of 8 plus 1)
-  int NRP;    // padded rows per output plane that cover every valid voxel
+  int NY;     // output rows per work item (NY * D <= 128 * kTcT)
+  int nyb;    // input rows staged per plane (covers every MMA row's taps)
+  int RS;     // staged voxels per plane and channel group = nyb * D
+  int SS;     // slab stride in voxels: RS rounded up to 8 (128-byte TMA destinations)
   int ntg;    // work items per output plane
 };
+
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            int c4, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+      "[%7];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(mbar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
 
 // CIN input channels, NTC = MMA N (output channels computed), COUT = output
 // channels stored.
 template <int CIN, int NTC, int COUT>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    k_conv_tc(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ w,
+    k_conv_tc(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16* __restrict__ w,
               const float* __restrict__ bias, void* __restrict__ y, const __nv_bfloat16* __restrict__ mask,
               TcGeom g, int relu, int out_f32) {
   constexpr int KG = CIN / 8;
   constexpr int WBYTES = 27 * KG * NTC * 16;
   constexpr int TCOLS = kTcT * NTC <= 32 ? 32 : (kTcT * NTC <= 64 ? 64 : 128);
-  extern __shared__ __align__(128) unsigned char sm[];
+  extern __shared__ __align__(128) unsigned char sm_raw[];
+  // 128-byte aligned base: TMA destinations must be 128-byte aligned
+  unsigned char* sm = sm_raw + ((128u - (smem_u32(sm_raw) & 127u)) & 127u);
   unsigned char* sw = sm;                        // weights
   unsigned char* sx = sm + WBYTES;               // staged input
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar;   // MMA completion
+  __shared__ __align__(8) uint64_t tbar;   // staging (TMA) completion
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int RS = g.RS, D = g.D;
-  const long long in_plane = (long long)g.din * g.din;
+  const int SS = g.SS, D = g.D;
 
   // weights: global [27][COUT][CIN] -> shared [27][KG][NTC][8] (rows >= COUT zero)
   for (int q = tid; q < 27 * KG * NTC; q += kTcThreads) {
@@ -156,6 +176,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   cp_async_wait_all();
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&tbar)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -171,32 +192,48 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t tbase = tmem_slot;
   const uint32_t mb = smem_u32(&mbar);
   const uint32_t sw_a = smem_u32(sw), sx_a = smem_u32(sx);
+  const uint32_t tb = smem_u32(&tbar);
   const uint32_t idesc = umma_idesc(NTC);
-  uint32_t phase = 0;
+  uint32_t phase = 0, tphase = 0;
   bool failed = false;
+  auto wait_bar = [&](uint32_t bar, uint32_t& ph) -> bool {
+    long long spins = 0;
+    bool timed_out = false;
+    while (!mbar_try(bar, ph)) {
+      if (++spins > (1LL << 22)) {
+        timed_out = true;
+        break;
+      }
+    }
+    ph ^= 1u;
+    return __syncthreads_or(timed_out) != 0;
+  };
 
   const long long items = (long long)g.nb * g.E * g.ntg;
+  // stage item `it` (three input planes, every channel group) with the TMA
+  auto stage = [&](long long it) {
+    const int tg = (int)(it % g.ntg);
+    const int oz = (int)((it / g.ntg) % g.E);
+    const int b = (int)(it / ((long long)g.ntg * g.E));
+    const int y0 = tg * g.NY;
+    mbar_expect_tx(tb, (uint32_t)(3 * KG * g.RS * 16));
+    for (int p = 0; p < 3; ++p)
+      for (int kg = 0; kg < KG; ++kg)
+        tma_load_5d(sx_a + (uint32_t)((p * KG + kg) * SS * 16), &xmap, kg * 8, -g.pad, y0 - g.pad, oz + p - g.pad, b,
+                    tb);
+  };
+  // descriptors advance by the operand offset in 16-byte units (the start
+  // address field holds address >> 4 and shared memory is < 256 KB)
+  const uint64_t ad0 = umma_desc(sx_a, (uint32_t)SS * 16u, 128u);
+  const uint64_t bd0 = umma_desc(sw_a, (uint32_t)NTC * 16u, 128u);
+  if (tid == 0 && (long long)blockIdx.x < items) stage(blockIdx.x);
   for (long long it = blockIdx.x; it < items && !failed; it += gridDim.x) {
     const int tg = (int)(it % g.ntg);
     const int oz = (int)((it / g.ntg) % g.E);
     const int b = (int)(it / ((long long)g.ntg * g.E));
-    const int r0 = tg * kTcT * 128;
-    // stage planes oz..oz+2 (virtual), rows r0..r0+RS-1, zero outside the real input
-    for (int q = tid; q < 3 * RS * KG; q += kTcThreads) {
-      const int kg = q % KG, v = (q / KG) % RS, p = q / (KG * RS);
-      const int vr = r0 + v;
-      const int vz = oz + p, vy = vr / D, vx = vr - (vr / D) * D;
-      const int iz = vz - g.pad, iy = vy - g.pad, ix = vx - g.pad;
-      const bool in = vy < D && (unsigned)iz < (unsigned)g.din && (unsigned)iy < (unsigned)g.din &&
-                      (unsigned)ix < (unsigned)g.din;
-      const __nv_bfloat16* src =
-          in ? x + (((long long)b * g.din + iz) * in_plane + (long long)iy * g.din + ix) * CIN + kg * 8 : x;
-      cp_async16(sx_a + (uint32_t)(((p * KG + kg) * RS + v) * 16), src, in ? 16u : 0u);
-    }
-    cp_async_wait_all();
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
+    const int y0 = tg * g.NY;
+    const int r0 = y0 * D;
+    if ((failed = wait_bar(tb, tphase))) break;  // this item's planes have landed
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (tid == 0) {
       // the kTcT accumulator tiles are independent: interleave them so that
@@ -205,37 +242,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
 #pragma unroll
         for (int kc = 0; kc < KG / 2; ++kc) {
-          const uint32_t b_addr = sw_a + (uint32_t)(((tap * KG + 2 * kc) * NTC) * 16);
-          const uint64_t bd = umma_desc(b_addr, (uint32_t)NTC * 16u, 128u);
+          const uint64_t bd = bd0 + (uint64_t)((tap * KG + 2 * kc) * NTC);
           const uint32_t acc = (tap > 0 || kc > 0) ? 1u : 0u;
+          const uint64_t adk = ad0 + (uint64_t)((dz * KG + 2 * kc) * SS + dy * D + dx);
 #pragma unroll
-          for (int t = 0; t < kTcT; ++t) {
-            const int row = t * 128 + dy * D + dx;
-            const uint32_t a_addr = sx_a + (uint32_t)(((dz * KG + 2 * kc) * RS + row) * 16);
-            const uint64_t ad = umma_desc(a_addr, (uint32_t)RS * 16u, 128u);
-            umma_f16(tbase + (uint32_t)(t * NTC), ad, bd, idesc, acc);
-          }
+          for (int t = 0; t < kTcT; ++t) umma_f16(tbase + (uint32_t)(t * NTC), adk + (uint64_t)(t * 128), bd, idesc, acc);
         }
       }
       umma_commit(mb);
     }
-    // wait for the accumulators (bounded; the outcome is made uniform over
-    // the CTA so that every thread takes the same path)
-    long long spins = 0;
-    bool timed_out = false;
-    while (!mbar_try(mb, phase)) {
-      if (++spins > (1LL << 22)) {
-        timed_out = true;
-        break;
-      }
-    }
-    phase ^= 1u;
-    failed = __syncthreads_or(timed_out) != 0;
-    if (failed) {
-      if (tid == 0) atomicOr(&g_sur_status, kErrWait);
-      break;
-    }
+    // wait for the accumulators (bounded; uniform over the CTA)
+    if ((failed = wait_bar(mb, phase))) break;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // the staged planes are free again: fetch the next item while this
+    // item's accumulators drain
+    const long long nxt = it + gridDim.x;
+    if (tid == 0 && nxt < items) stage(nxt);
     // epilogue: warp w owns accumulator rows 32w..32w+31 of every tile
 #pragma unroll 1
     for (int t = 0; t < kTcT; ++t) {
@@ -243,7 +265,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tmem_ld<NTC>(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(t * NTC), v);
       const int r = r0 + t * 128 + 32 * warp + lane;
       const int oy = r / D, ox = r - (r / D) * D;
-      if (oy < g.E && ox < g.E) {
+      if (oy < g.E && oy < y0 + g.NY && ox < g.E) {
         const long long o = (((long long)b * g.E + oz) * g.E + oy) * g.E + ox;
         if (out_f32) {
           float* yo = reinterpret_cast<float*>(y) + o * COUT;
@@ -282,12 +304,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
       }
     }
-    // every warp is done with tensor memory and the staged rows before the
-    // next item's MMAs overwrite them
+    // every warp has read the accumulators before the next item's MMAs
+    // overwrite them
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
+  if (failed && tid == 0) atomicOr(&g_sur_status, kErrWait);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -304,17 +327,20 @@ inline TcGeom tc_geom(int din, int pad, int nb) {
   g.D = din + 2 * pad;
   g.E = g.D - 2;
   g.nb = nb;
-  int rs = kTcT * 128 + 2 * g.D + 2;
-  rs = (rs + 7) / 8 * 8 + 1;  // odd number of 16-byte rows per channel group: conflict-free staging stores
-  g.RS = rs;
-  g.NRP = (g.E - 1) * g.D + g.E;
-  g.ntg = (g.NRP + kTcT * 128 - 1) / (kTcT * 128);
+  g.NY = (kTcT * 128) / g.D;
+  if (g.NY > g.E) g.NY = g.E;
+  // the last MMA row of the last tile reads row index kTcT*128 - 1 + 2D + 2
+  g.nyb = (kTcT * 128 + 2 * g.D + 2 + g.D - 1) / g.D;
+  g.RS = g.nyb * g.D;
+  g.SS = (g.RS + 7) / 8 * 8;
+  g.ntg = (g.E + g.NY - 1) / g.NY;
   return g;
 }
 
 template <int CIN, int NTC>
-constexpr size_t tc_smem_bytes(int rs) {
-  return (size_t)27 * (CIN / 8) * NTC * 16 + (size_t)3 * (CIN / 8) * rs * 16;
+constexpr size_t tc_smem_bytes(int ss) {
+  // 128 bytes of alignment slack + weights + 3 planes x channel groups of slabs
+  return 128 + (size_t)27 * (CIN / 8) * NTC * 16 + (size_t)3 * (CIN / 8) * ss * 16;
 }
 
 }  // namespace

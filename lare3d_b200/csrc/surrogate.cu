@@ -12,8 +12,10 @@
 // warp.  The weight gradient is the transposed GEMM (rows = output channels,
 // columns = input channels, reduction = voxels) with per-chunk partials
 // summed in a fixed order, so training is deterministic.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstdint>
@@ -185,12 +187,40 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const bf16* __restrict__ 
 
 bool g_use_tc = true;  // tcgen05 convolution (else the mma.sync one)
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
 template <int CIN, int NTC, int COUT>
 int launch_conv_tc(const void* x, int din, int pad, const void* w, const float* bias, void* y, int nb,
                    const void* mask, int relu, int out_f32, cudaStream_t s) {
   const TcGeom g = tc_geom(din, pad, nb);
-  const size_t smem = tc_smem_bytes<CIN, NTC>(g.RS);
-  if (smem > 220 * 1024) return LARE_ETOOLARGE;
+  const size_t smem = tc_smem_bytes<CIN, NTC>(g.SS);
+  if (smem > 220 * 1024 || g.D > 256 || g.nyb > 256 || g.NY < 1) return LARE_ETOOLARGE;
+  if (((uintptr_t)x & 15u) != 0) return LARE_EINVAL;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return LARE_ECUDA;
+  // activations [nb][din][din][din][CIN] bf16 as a 5-D tensor, channels innermost
+  CUtensorMap xmap;
+  const cuuint64_t e = 2ull * CIN;
+  const cuuint64_t dims[5] = {(cuuint64_t)CIN, (cuuint64_t)din, (cuuint64_t)din, (cuuint64_t)din, (cuuint64_t)nb};
+  const cuuint64_t strides[4] = {e, e * din, e * din * din, e * din * din * din};
+  const cuuint32_t box[5] = {8u, (cuuint32_t)g.D, (cuuint32_t)g.nyb, 1u, 1u};
+  const cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
+  if (enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(x), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return LARE_ECUDA;
   static int attr[64] = {};
   const int dev = current_device();
   if (dev < 0 || dev >= 64) return LARE_ECUDA;
@@ -204,8 +234,8 @@ int launch_conv_tc(const void* x, int din, int pad, const void* w, const float* 
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long long items = (long long)nb * g.E * g.ntg;
   const unsigned blocks = (unsigned)(items < sms ? items : sms);
-  k_conv_tc<CIN, NTC, COUT><<<blocks, kTcThreads, smem, s>>>((const bf16*)x, (const bf16*)w, bias, y,
-                                                             (const bf16*)mask, g, relu, out_f32);
+  k_conv_tc<CIN, NTC, COUT><<<blocks, kTcThreads, smem, s>>>(xmap, (const bf16*)w, bias, y, (const bf16*)mask, g,
+                                                             relu, out_f32);
   return cudaGetLastError() == cudaSuccess ? LARE_OK : LARE_ECUDA;
 }
 
