@@ -34,7 +34,9 @@ extern "C" {
  * multiplied by (mask > 0) (the ReLU derivative, for the backward pass).
  * bias may be NULL.  Backward-data is this call with pad = 2 on the output
  * gradient and the tap-flipped, transposed weights of lare_sur_pack.
- * (cin, cout) in {(16,32), (32,32), (32,8)}.
+ * (cin, cout) in {(16,32), (32,32), (32,8), (32,1)}; (32,1) is the
+ * network's output layer (FP32 output, no mask), computed with the nine
+ * in-plane taps in the MMA's N dimension.
  */
 int lare_sur_conv(int cin, int cout, int relu, int out_f32, const void* x, int din, int pad, const void* w,
                   const float* bias, void* y, int dout, int nb, const void* mask, void* stream);

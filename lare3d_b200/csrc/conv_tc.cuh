@@ -319,6 +319,148 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
+// Single output channel (the network's last layer, dT): the nine (dy, dx)
+// taps of a plane share one shift-free operand, so the MMA's N dimension
+// holds the taps instead of output channels:
+//   P[u][j] = sum_{dz, ci} X[plane oz+dz][row u][ci] W[dz*9 + j][ci]   (j = dy*3 + dx)
+// accumulated over the three planes and both channel halves in tensor
+// memory (N = 16, taps 9..15 zero), and out[v] = bias + sum_j P[v + dy*D + dx][j]
+// is formed in the epilogue from a shared-memory copy of P.  36 MMAs per
+// work item instead of 216.
+template <int CIN>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_conv_tc_c1(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16* __restrict__ w,
+                 const float* __restrict__ bias, float* __restrict__ y, TcGeom g, int relu) {
+  constexpr int KG = CIN / 8;
+  constexpr int NJ = 16;                         // taps per plane (9) padded to the MMA's N
+  constexpr int WBYTES = 3 * KG * NJ * 16;       // weights [plane][kg][j][8]
+  constexpr int NUT = (kTcT * 128 + 2 * 76 + 2 + 127) / 128 + 1;  // u tiles (bounded by D <= 76)
+  constexpr int TCOLS = NUT * NJ <= 32 ? 32 : (NUT * NJ <= 64 ? 64 : 128);
+  extern __shared__ __align__(128) unsigned char sm_raw[];
+  unsigned char* sm = sm_raw + ((128u - (smem_u32(sm_raw) & 127u)) & 127u);
+  unsigned char* sw = sm;
+  unsigned char* sx = sm + WBYTES;
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t tbar;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int SS = g.SS, D = g.D;
+  float* Psm = reinterpret_cast<float*>(sx + (size_t)3 * KG * SS * 16);  // [u][NJ]
+  // weights: global [27][1][CIN] -> shared [3][KG][NJ][8], j >= 9 zero
+  for (int q = tid; q < 3 * KG * NJ; q += kTcThreads) {
+    const int j = q % NJ, kg = (q / NJ) % KG, p = q / (NJ * KG);
+    const __nv_bfloat16* src = w + ((long long)(p * 9 + (j < 9 ? j : 0))) * CIN + kg * 8;
+    cp_async16(smem_u32(sw + (size_t)q * 16), src, j < 9 ? 16u : 0u);
+  }
+  cp_async_wait_all();
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&tbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(TCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tbase = tmem_slot;
+  const uint32_t mb = smem_u32(&mbar), tb = smem_u32(&tbar);
+  const uint32_t sw_a = smem_u32(sw), sx_a = smem_u32(sx);
+  const uint32_t idesc = umma_idesc(NJ);
+  uint32_t phase = 0, tphase = 0;
+  bool failed = false;
+  auto wait_bar = [&](uint32_t bar, uint32_t& ph) -> bool {
+    long long spins = 0;
+    bool timed_out = false;
+    while (!mbar_try(bar, ph)) {
+      if (++spins > (1LL << 22)) {
+        timed_out = true;
+        break;
+      }
+    }
+    ph ^= 1u;
+    return __syncthreads_or(timed_out) != 0;
+  };
+  const int nrow = g.NY * D;                       // output rows of an item (padded numbering)
+  const int nu = nrow + 2 * D + 2;                 // P rows an item needs
+  const int nut = (nu + 127) / 128;
+  const long long items = (long long)g.nb * g.E * g.ntg;
+  auto stage = [&](long long it) {
+    const int tg = (int)(it % g.ntg);
+    const int oz = (int)((it / g.ntg) % g.E);
+    const int b = (int)(it / ((long long)g.ntg * g.E));
+    mbar_expect_tx(tb, (uint32_t)(3 * KG * g.RS * 16));
+    for (int p = 0; p < 3; ++p)
+      for (int kg = 0; kg < KG; ++kg)
+        tma_load_5d(sx_a + (uint32_t)((p * KG + kg) * SS * 16), &xmap, kg * 8, -g.pad, tg * g.NY - g.pad,
+                    oz + p - g.pad, b, tb);
+  };
+  const uint64_t ad0 = umma_desc(sx_a, (uint32_t)SS * 16u, 128u);
+  const uint64_t bd0 = umma_desc(sw_a, (uint32_t)NJ * 16u, 128u);
+  const float b0 = bias ? bias[0] : 0.f;
+  if (tid == 0 && (long long)blockIdx.x < items) stage(blockIdx.x);
+  for (long long it = blockIdx.x; it < items && !failed; it += gridDim.x) {
+    const int tg = (int)(it % g.ntg);
+    const int oz = (int)((it / g.ntg) % g.E);
+    const int b = (int)(it / ((long long)g.ntg * g.E));
+    const int y0 = tg * g.NY;
+    if ((failed = wait_bar(tb, tphase))) break;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      for (int p = 0; p < 3; ++p) {
+#pragma unroll
+        for (int kc = 0; kc < KG / 2; ++kc) {
+          const uint64_t bd = bd0 + (uint64_t)((p * KG + 2 * kc) * NJ);
+          const uint64_t adk = ad0 + (uint64_t)((p * KG + 2 * kc) * SS);
+          const uint32_t acc = (p > 0 || kc > 0) ? 1u : 0u;
+          for (int ut = 0; ut < nut; ++ut)
+            umma_f16(tbase + (uint32_t)(ut * NJ), adk + (uint64_t)(ut * 128), bd, idesc, acc);
+        }
+      }
+      umma_commit(mb);
+    }
+    if ((failed = wait_bar(mb, phase))) break;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const long long nxt = it + gridDim.x;
+    if (tid == 0 && nxt < items) stage(nxt);
+    // P to shared memory: warp w writes rows ut*128 + 32w + lane
+    for (int ut = 0; ut < nut; ++ut) {
+      float v[NJ];
+      tmem_ld<NJ>(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(ut * NJ), v);
+      const int u = ut * 128 + 32 * warp + lane;
+      float4* dst = reinterpret_cast<float4*>(Psm + (size_t)u * NJ);
+#pragma unroll
+      for (int q = 0; q < NJ / 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    for (int r = tid; r < nrow; r += kTcThreads) {
+      const int oy = y0 + r / D, ox = r - (r / D) * D;
+      if (oy >= g.E || ox >= g.E) continue;
+      float a = 0.f;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) a += Psm[(size_t)(r + (j / 3) * D + (j % 3)) * NJ + j];
+      a += b0;
+      if (relu) a = fmaxf(a, 0.f);
+      y[(((long long)b * g.E + oz) * g.E + oy) * g.E + ox] = a;
+    }
+    __syncthreads();
+  }
+  if (failed && tid == 0) atomicOr(&g_sur_status, kErrWait);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TCOLS) : "memory");
+  }
+}
+
 // Geometry of one convolution call (see the file comment).
 inline TcGeom tc_geom(int din, int pad, int nb) {
   TcGeom g;

@@ -239,6 +239,72 @@ int launch_conv_tc(const void* x, int din, int pad, const void* w, const float* 
   return cudaGetLastError() == cudaSuccess ? LARE_OK : LARE_ECUDA;
 }
 
+// Single-output-channel convolution (the network's last layer).
+template <int CIN>
+int launch_conv_tc_c1(const void* x, int din, int pad, const void* w, const float* bias, float* y, int nb, int relu,
+                      cudaStream_t s) {
+  TcGeom g = tc_geom(din, pad, nb);
+  const int nu = g.NY * g.D + 2 * g.D + 2, nut = (nu + 127) / 128;
+  if (g.D > 76 || nut > (kTcT * 128 + 2 * 76 + 2 + 127) / 128 + 1) return LARE_ETOOLARGE;
+  if (g.SS < nut * 128) g.SS = nut * 128;  // every MMA row stays inside the staged slabs
+  const size_t smem = 128 + (size_t)3 * (CIN / 8) * 16 * 16 + (size_t)3 * (CIN / 8) * g.SS * 16 +
+                      (size_t)nut * 128 * 16 * sizeof(float);
+  if (smem > 220 * 1024 || g.nyb > 256 || g.NY < 1) return LARE_ETOOLARGE;
+  if (((uintptr_t)x & 15u) != 0) return LARE_EINVAL;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return LARE_ECUDA;
+  CUtensorMap xmap;
+  const cuuint64_t e = 2ull * CIN;
+  const cuuint64_t dims[5] = {(cuuint64_t)CIN, (cuuint64_t)din, (cuuint64_t)din, (cuuint64_t)din, (cuuint64_t)nb};
+  const cuuint64_t strides[4] = {e, e * din, e * din * din, e * din * din * din};
+  const cuuint32_t box[5] = {8u, (cuuint32_t)g.D, (cuuint32_t)g.nyb, 1u, 1u};
+  const cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
+  if (enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(x), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return LARE_ECUDA;
+  static int attr[64] = {};
+  const int dev = current_device();
+  if (dev < 0 || dev >= 64) return LARE_ECUDA;
+  if (attr[dev] < (int)smem) {
+    if (cudaFuncSetAttribute(k_conv_tc_c1<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return LARE_ECUDA;
+    attr[dev] = (int)smem;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long items = (long long)nb * g.E * g.ntg;
+  const unsigned blocks = (unsigned)(items < sms ? items : sms);
+  k_conv_tc_c1<CIN><<<blocks, kTcThreads, smem, s>>>(xmap, (const bf16*)w, bias, y, g, relu);
+  return cudaGetLastError() == cudaSuccess ? LARE_OK : LARE_ECUDA;
+}
+
+// Single output channel on the CUDA cores (the alternative engine): one
+// thread per output voxel, taps and channels in the forward conv's order.
+template <int CIN>
+__global__ void k_conv_c1(const bf16* __restrict__ x, int din, int pad, const bf16* __restrict__ w,
+                          const float* __restrict__ bias, float* __restrict__ y, int dout, int nb, int relu) {
+  const long long n = (long long)dout * dout * dout * nb;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long vox = (long long)dout * dout * dout;
+  const int b = (int)(i / vox);
+  const long long v = i - (long long)b * vox;
+  const int ox = (int)(v % dout), oy = (int)((v / dout) % dout), oz = (int)(v / ((long long)dout * dout));
+  float a = 0.f;
+  for (int tap = 0; tap < 27; ++tap) {
+    const int iz = oz + tap / 9 - pad, iy = oy + (tap / 3) % 3 - pad, ix = ox + tap % 3 - pad;
+    if ((unsigned)iz >= (unsigned)din || (unsigned)iy >= (unsigned)din || (unsigned)ix >= (unsigned)din) continue;
+    const bf16* xp = x + ((((long long)b * din + iz) * din + iy) * din + ix) * CIN;
+    const bf16* wp = w + (long long)tap * CIN;
+#pragma unroll
+    for (int c = 0; c < CIN; ++c) a += __bfloat162float(xp[c]) * __bfloat162float(wp[c]);
+  }
+  a += bias ? bias[0] : 0.f;
+  if (relu) a = fmaxf(a, 0.f);
+  y[i] = a;
+}
+
 template <int CIN, int COUT>
 int launch_conv(const void* x, int din, int pad, const void* w, const float* bias, void* y, int dout, int nb,
                 const void* mask, int relu, int out_f32, cudaStream_t s) {
@@ -618,6 +684,14 @@ int lare_sur_conv(int cin, int cout, int relu, int out_f32, const void* x, int d
   if (cin == 16 && cout == 32) return launch_conv<16, 32>(x, din, pad, w, bias, y, dout, nb, mask, relu, out_f32, s);
   if (cin == 32 && cout == 32) return launch_conv<32, 32>(x, din, pad, w, bias, y, dout, nb, mask, relu, out_f32, s);
   if (cin == 32 && cout == 8) return launch_conv<32, 8>(x, din, pad, w, bias, y, dout, nb, mask, relu, out_f32, s);
+  if (cin == 32 && cout == 1) {
+    if (!out_f32 || mask) return LARE_EINVAL;
+    if (g_use_tc) return launch_conv_tc_c1<32>(x, din, pad, w, bias, (float*)y, nb, relu, s);
+    const long long n = (long long)dout * dout * dout * nb;
+    k_conv_c1<32><<<(unsigned)((n + 255) / 256), 256, 0, s>>>((const bf16*)x, din, pad, (const bf16*)w, bias,
+                                                             (float*)y, dout, nb, relu);
+    return cudaGetLastError() == cudaSuccess ? LARE_OK : LARE_ECUDA;
+  }
   return LARE_EINVAL;
 }
 

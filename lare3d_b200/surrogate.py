@@ -39,7 +39,7 @@ from . import gpu
 from .abi import BC_USER, LARE_OK, LareError
 
 # (cin padded, cout of the master weights, cin used, cout used by the forward)
-LAYERS = ((16, 32, 7, 32), (32, 32, 32, 32), (32, 32, 32, 32), (32, 16, 32, 8))
+LAYERS = ((16, 32, 7, 32), (32, 32, 32, 32), (32, 32, 32, 32), (32, 16, 32, 1))
 HALO = 4                 # cells trimmed per face by the four valid convolutions
 PATCH = 16               # edge of a re-check / rejection patch
 TRAIN_WIN = PATCH + 2 * HALO

@@ -18,7 +18,7 @@ from __future__ import annotations
 import numpy as np
 
 # (cin padded, cout of the master weights, cin used, cout used by the forward)
-LAYERS = ((16, 32, 7, 32), (32, 32, 32, 32), (32, 32, 32, 32), (32, 16, 32, 8))
+LAYERS = ((16, 32, 7, 32), (32, 32, 32, 32), (32, 32, 32, 32), (32, 16, 32, 1))
 TAPS = [(t // 9, (t // 3) % 3, t % 3) for t in range(27)]   # t = (dz*3 + dy)*3 + dx
 
 

@@ -38,7 +38,7 @@ def engine(request, built):
 
 
 @pytest.mark.parametrize("cin,cout,pad,masked", [(16, 32, 0, False), (32, 32, 0, False), (32, 8, 0, False),
-                                                 (16, 32, 2, True), (32, 32, 2, True)])
+                                                 (32, 1, 0, False), (16, 32, 2, True), (32, 32, 2, True)])
 @pytest.mark.parametrize("din", [9, 24])
 def test_conv_kernel_fp32_output(engine, cin, cout, pad, masked, din):
     """lare_sur_conv with FP32 output against float64 on bf16 operands
