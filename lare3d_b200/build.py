@@ -30,7 +30,7 @@ NVCC_COMMON = [
 # (--fmad=false) to reproduce the reference's x86-64 arithmetic bit for bit.
 UNITS = [
     ("engine_f64.cu", ["--fmad=false"]),
-    ("engine_f32.cu", ["--fmad=true"]),
+    ("engine_f32.cu", ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"]),
     ("lare_gpu.cu", []),
     ("lare_noalloc.cu", ["--fmad=false"]),
     ("surrogate.cu", []),
