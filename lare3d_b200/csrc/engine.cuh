@@ -100,7 +100,7 @@ struct Run {
   bool gamma_boris_one = true;      // gamma_boris holds 1 everywhere
   int cur_step = 0;
   int peak_substeps = 0, last_substeps = 0, steps_taken = 0, n_s_stages = 0;
-  int blk_x = 64, blk_y = 4;            // block shape of the point kernels
+  int blk_x = 32, blk_y = 4;            // block shape of the point kernels (measured best at 256^3)
   bool capturing = false;               // recording a CUDA graph of whole steps
   cudaStream_t s_body = nullptr;        // captures the body of the resistive sub-cycle loop
   GSpec g_cell, g_node, g_bx, g_by, g_bz, g_cell_mpi, g_cell_user, g_dm[3];

@@ -568,7 +568,7 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--steps", type=int, default=4, help="RKL2 steps per seed")
     ap.add_argument("--seeds", type=int, default=len(TRAIN_SEEDS))
-    ap.add_argument("--iters", type=int, default=20000)
+    ap.add_argument("--iters", type=int, default=60000)
     ap.add_argument("--nb", type=int, default=64)
     ap.add_argument("--lr", type=float, default=5e-4)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
