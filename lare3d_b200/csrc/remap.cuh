@@ -253,8 +253,8 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     ba.n0 = nx + 3;
     ba.n1 = (A == 1 ? nz : ny) + 3;
     const int k = run.prof_begin("remap_sweep_bflux", A, 7, (double)(nx + 3) * (ny + 3) * (nz + 3));
-    dim3 blk(64, 4, 1);
-    dim3 grd((ba.n0 + 63) / 64, (ba.n1 + 3) / 4, (na + 3 + kMarch - 1) / kMarch);
+    dim3 blk(32, 4, 1);
+    dim3 grd((ba.n0 + 31) / 32, (ba.n1 + 3) / 4, (na + 3 + kMarch - 1) / kMarch);
     k_bflux_march<R><<<grd, blk, 0, run.s>>>(ba);
     run.prof_end(k);
     ++run.launches;
