@@ -70,6 +70,11 @@ class Clocks:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
+            # nvidia-smi takes a while to start: wait for its first sample so
+            # that the samples cover the timed region
+            t0 = time.time()
+            while time.time() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception:
             self.p = None
 
