@@ -379,7 +379,10 @@ def main():
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(top["site"])
+        # measured DRAM bytes per launch, keyed by routine, word count and grid
+        for t in json.load(open(tpath)):
+            if (t["routine"], t["words"], t["grid"]) == (top["site"].split(":")[0], top["words"], n):
+                traffic = t["bytes_per_launch"]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": traffic, "kernel": top["site"], "share": top["ms"] / total_ms,
                 "peak_kind": peak_kind, "algorithmic_bytes_per_launch": per_launch_bytes}

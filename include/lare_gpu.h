@@ -266,6 +266,15 @@ int lare_gpu_set_block(lare_ctx* ctx, int bx, int by);
 
 const char* lare_gpu_last_error(lare_ctx* ctx);
 
+/*
+ * Self-check of the exact division the FP64 kernels use for divisions by
+ * the 1-D grid metrics (a quotient corrected from the divisor's precomputed
+ * reciprocal): out[i] = a[i] / b[i] computed that way, on the device
+ * pointers a, b, out, enqueued on the given CUDA stream.  Every result must
+ * equal the IEEE quotient bit for bit.  No counterpart in the reference.
+ */
+int lare_gpu_check_division(const double* a, const double* b, long long n, double* out, void* stream);
+
 void lare_gpu_destroy(lare_ctx* ctx);
 
 /*

@@ -42,6 +42,28 @@ struct Num<float> {
   static __host__ __device__ constexpr float huge() { return FLT_MAX; }
 };
 
+// a / b given rb = RN(1/b), bitwise equal to the IEEE quotient, for divisors
+// with a precomputed reciprocal (the 1-D grid metrics).  q0 = RN(a*rb) is
+// within 1.5 ulp of a/b; one correction q + (a - b*q)*rb makes it faithful,
+// and a second is correctly rounded by Markstein's theorem (P. Markstein,
+// IBM J. Res. Dev. 34(1), 1990: with y = RN(1/b) and q within one ulp of
+// a/b, RN(q + (a - b*q)*y) = RN(a/b); the FMA remainder is exact).  The
+// theorem needs exact remainders, so non-finite values and |a| or |b|
+// outside [2^-500, 2^500] take the plain division, except a zero a over such
+// a b, whose quotient a*rb is exact (a signed zero).  FP32 keeps the build's
+// division.
+__device__ __forceinline__ double div_rcp(double a, double b, double rb) {
+  const unsigned ea = ((unsigned)__double2hiint(a) >> 20) & 0x7ffu;
+  const unsigned eb = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
+  if (ea - 523u > 1000u || eb - 523u > 1000u) return (a == 0.0 && eb - 523u <= 1000u) ? a * rb : a / b;
+  double q = a * rb;
+  double r = fma(-b, q, a);
+  q = fma(r, rb, q);
+  r = fma(-b, q, a);
+  return fma(r, rb, q);
+}
+__device__ __forceinline__ float div_rcp(float a, float b, float) { return a / b; }
+
 // Scalar slots kept in device memory so that a whole step can run (and be
 // captured in a CUDA graph) without the host knowing dt.
 enum Slot {
@@ -77,18 +99,28 @@ __global__ void __launch_bounds__(256) k_box(int i0, int j0, int k0, int ni, int
   if (i >= ni || j >= nj) return;
   fn(i0 + i, j0 + j, k0 + (int)blockIdx.z);
 }
+// The same with an occupancy hint: MINB blocks of 256 threads must fit on
+// one SM, which caps the registers per thread.
+template <int MINB, class Fn>
+__global__ void __launch_bounds__(256, MINB) k_box_mb(int i0, int j0, int k0, int ni, int nj, Fn fn) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= ni || j >= nj) return;
+  fn(i0 + i, j0 + j, k0 + (int)blockIdx.z);
+}
 
 // Block shape bx x by (bx * by <= 256), chosen per context (the ensemble
 // autotuner sets it per grid size); every point runs the same arithmetic
 // whatever the shape.
-template <class Fn>
+template <int MINB = 0, class Fn>
 inline void launch_box(cudaStream_t s, long long& count, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn,
                        int bx = 64, int by = 4) {
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   if (ni <= 0 || nj <= 0 || nk <= 0) return;
   dim3 blk(bx, by, 1);
   dim3 grd((ni + bx - 1) / bx, (nj + by - 1) / by, nk);
-  k_box<<<grd, blk, 0, s>>>(i0, j0, k0, ni, nj, fn);
+  if constexpr (MINB > 0) k_box_mb<MINB><<<grd, blk, 0, s>>>(i0, j0, k0, ni, nj, fn);
+  else k_box<<<grd, blk, 0, s>>>(i0, j0, k0, ni, nj, fn);
   ++count;
 }
 

@@ -159,21 +159,26 @@ struct Run {
 
 // ---------------------------------------------------------------------
 // Launch shorthands
-template <class R, class Fn>
+template <int MINB64 = 0, class R, class Fn>
 inline void rbox(Run<R>& run, const char* func, int line, int words, int i0, int i1, int j0, int j1, int k0, int k1,
                  Fn fn) {
   double pts = (double)(i1 - i0 + 1) * (double)(j1 - j0 + 1) * (double)(k1 - k0 + 1);
   int k = run.prof_begin(func, line, words, pts);
-  launch_box(run.s, run.launches, i0, i1, j0, j1, k0, k1, fn, run.blk_x, run.blk_y);
+  launch_box<sizeof(R) == 8 ? MINB64 : 0>(run.s, run.launches, i0, i1, j0, j1, k0, k1, fn, run.blk_x, run.blk_y);
   run.prof_end(k);
 }
 // LARE_BOX: one kernel over an inclusive Fortran index box.  LARE_BOXW also
 // states the kernel's algorithmic word count per point (arrays read +
-// written), used for the roofline of profiled launches.
+// written), used for the roofline of profiled launches.  LARE_BOXWB adds an
+// occupancy hint for the FP64 build (k_box_mb's MINB): latency-bound stencils
+// with many live values run faster with a register cap that lets more
+// blocks share an SM (measured per kernel at 256^3; FP32 keeps the default).
 #define LARE_BOX(run, i0, i1, j0, j1, k0, k1, ...) \
   rbox((run), __func__, __LINE__, 0, (i0), (i1), (j0), (j1), (k0), (k1), __VA_ARGS__)
 #define LARE_BOXW(run, words, i0, i1, j0, j1, k0, k1, ...) \
   rbox((run), __func__, __LINE__, (words), (i0), (i1), (j0), (j1), (k0), (k1), __VA_ARGS__)
+#define LARE_BOXWB(run, minb, words, i0, i1, j0, j1, k0, k1, ...) \
+  rbox<minb>((run), __func__, __LINE__, (words), (i0), (i1), (j0), (j1), (k0), (k1), __VA_ARGS__)
 
 template <class R>
 inline void ghost(Run<R>& run, const GSpec& g, A3<R> a, A3<R>* b = nullptr, A3<R>* c = nullptr) {
@@ -599,11 +604,12 @@ void eulerian_remap(Run<R>& run, int step) {
   R* const qx = run.a.bx.p;
   R* const qy = run.a.by.p;
   R* const qz = run.a.bz.p;
+  const auto rbx = run.a.rdb[0], rby = run.a.rdb[1], rbz = run.a.rdb[2];
   LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
-    if (iy >= -1 && iz >= -1) qx[c] = qx[c] / dyb(iy) / dzb(iz);
-    if (ix >= -1 && iz >= -1) qy[c] = qy[c] / dxb(ix) / dzb(iz);
-    if (ix >= -1 && iy >= -1) qz[c] = qz[c] / dxb(ix) / dyb(iy);
+    if (iy >= -1 && iz >= -1) qx[c] = div_rcp(div_rcp(qx[c], dyb(iy), rby(iy)), dzb(iz), rbz(iz));
+    if (ix >= -1 && iz >= -1) qy[c] = div_rcp(div_rcp(qy[c], dxb(ix), rbx(ix)), dzb(iz), rbz(iz));
+    if (ix >= -1 && iy >= -1) qz[c] = div_rcp(div_rcp(qz[c], dxb(ix), rbx(ix)), dyb(iy), rby(iy));
   });
   bfield_bcs(run);
 }

@@ -35,16 +35,18 @@ namespace lare {
 
 // Vertex current of eta_calc (lagran.F90:1190-1216), rkstep (:1479-1494)
 // and the predictor force (:358-373): the three places use the same
-// expressions, evaluated here once.
+// expressions, evaluated here once.  The divisions by the cell widths use
+// their reciprocals (rx, ry, rz) through div_rcp, which returns the same
+// quotients.
 template <class R>
 __device__ __forceinline__ void vertex_current(const R* bx, const R* by, const R* bz, int c, int sx, int sxy,
-                                               R dxc, R dyc, R dzc, R& jx, R& jy, R& jz) {
-  R jx1 = (bz[c + sx] - bz[c]) / dyc - (by[c + sxy] - by[c]) / dzc;
-  R jx2 = (bz[c + 1 + sx] - bz[c + 1]) / dyc - (by[c + 1 + sxy] - by[c + 1]) / dzc;
-  R jy1 = (bx[c + sxy] - bx[c]) / dzc - (bz[c + 1] - bz[c]) / dxc;
-  R jy2 = (bx[c + sx + sxy] - bx[c + sx]) / dzc - (bz[c + 1 + sx] - bz[c + sx]) / dxc;
-  R jz1 = (by[c + 1] - by[c]) / dxc - (bx[c + sx] - bx[c]) / dyc;
-  R jz2 = (by[c + 1 + sxy] - by[c + sxy]) / dxc - (bx[c + sx + sxy] - bx[c + sxy]) / dyc;
+                                               R dxc, R dyc, R dzc, R rx, R ry, R rz, R& jx, R& jy, R& jz) {
+  R jx1 = div_rcp(bz[c + sx] - bz[c], dyc, ry) - div_rcp(by[c + sxy] - by[c], dzc, rz);
+  R jx2 = div_rcp(bz[c + 1 + sx] - bz[c + 1], dyc, ry) - div_rcp(by[c + 1 + sxy] - by[c + 1], dzc, rz);
+  R jy1 = div_rcp(bx[c + sxy] - bx[c], dzc, rz) - div_rcp(bz[c + 1] - bz[c], dxc, rx);
+  R jy2 = div_rcp(bx[c + sx + sxy] - bx[c + sx], dzc, rz) - div_rcp(bz[c + 1 + sx] - bz[c + sx], dxc, rx);
+  R jz1 = div_rcp(by[c + 1] - by[c], dxc, rx) - div_rcp(bx[c + sx] - bx[c], dyc, ry);
+  R jz2 = div_rcp(by[c + 1 + sxy] - by[c + sxy], dxc, rx) - div_rcp(bx[c + sx + sxy] - bx[c + sxy], dyc, ry);
   jx = (jx1 + jx2) * R(0.5);
   jy = (jy1 + jy2) * R(0.5);
   jz = (jz1 + jz2) * R(0.5);
@@ -70,11 +72,13 @@ void eta_and_rkstep(Run<R>& run, bool with_rkstep) {
   R* const fzp = run.a.flux_z.p;
   R* const curlb = run.a.curlb.p;
   auto dxc = run.a.dxc, dyc = run.a.dyc, dzc = run.a.dzc;
+  auto rdcx = run.a.rdc[0], rdcy = run.a.rdc[1], rdcz = run.a.rdc[2];
   const R jmax = (R)run.p.j_max, eb = (R)run.p.eta_background, e0 = (R)run.p.eta0;
-  LARE_BOXW(run, with_rkstep ? 8 : 4, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWB(run, 5, with_rkstep ? 8 : 4, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     R jx, jy, jz;
-    vertex_current<R>(bx, by, bz, c, sx, sxy, dxc(ix), dyc(iy), dzc(iz), jx, jy, jz);
+    vertex_current<R>(bx, by, bz, c, sx, sxy, dxc(ix), dyc(iy), dzc(iz), rdcx(ix), rdcy(iy), rdcz(iz), jx, jy,
+                      jz);
     R j2 = jx * jx + jy * jy + jz * jz;
     R e = sqrt(j2) > jmax ? eb + e0 : eb;
     eta[c] = e;
@@ -112,7 +116,7 @@ void resistive_update(Run<R>& run) {
   auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb, dxc = A.dxc, dyc = A.dyc, dzc = A.dzc;
   const double* sc = run.sc;
   // RS2: bstep (:1588-1631) into the second buffers
-  LARE_BOXW(run, 9, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWB(run, 4, 9, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DTSUB];
     const int c = ix + sx * iy + sxy * iz;
     if (iy >= 1 && iz >= 1) {
@@ -236,7 +240,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
   auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb, dxc = A.dxc, dyc = A.dyc, dzc = A.dzc;
   const R visc1 = (R)run.p.visc1;
   const double* sc = run.sc;
-  LARE_BOXW(run, 8, -1, nx + 1, -1, ny + 2, 0, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWB(run, 4, 8, -1, nx + 1, -1, ny + 2, 0, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DT], v2n = (R)sc[SC_VISC2N];
     const int c = ix + sx * iy + sxy * iz;
     auto edge = [&](const R* vcomp, int i1, int i2, R dx) {
@@ -456,11 +460,12 @@ void predictor_remap(Run<R>& run, int step) {
   R* const qx = A.bx.p;
   R* const qy = A.by.p;
   R* const qz = A.bz.p;
+  const auto rbx = run.a.rdb[0], rby = run.a.rdb[1], rbz = run.a.rdb[2];
   LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
-    if (iy >= -1 && iz >= -1) qx[c] = qx[c] / dyb(iy) / dzb(iz);
-    if (ix >= -1 && iz >= -1) qy[c] = qy[c] / dxb(ix) / dzb(iz);
-    if (ix >= -1 && iy >= -1) qz[c] = qz[c] / dxb(ix) / dyb(iy);
+    if (iy >= -1 && iz >= -1) qx[c] = div_rcp(div_rcp(qx[c], dyb(iy), rby(iy)), dzb(iz), rbz(iz));
+    if (ix >= -1 && iz >= -1) qy[c] = div_rcp(div_rcp(qy[c], dxb(ix), rbx(ix)), dzb(iz), rbz(iz));
+    if (ix >= -1 && iy >= -1) qz[c] = div_rcp(div_rcp(qz[c], dxb(ix), rbx(ix)), dyb(iy), rby(iy));
   });
   bfield_bcs(run);
 }
@@ -521,7 +526,8 @@ void predictor_corrector_step(Run<R>& run) {
   const R* fyv = A.fy_visc.p;
   const R* fzv = A.fz_visc.p;
   auto dxc = A.dxc, dyc = A.dyc, dzc = A.dzc, grav = A.grav;
-  LARE_BOXW(run, 17, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  auto rdcx = A.rdc[0], rdcy = A.rdc[1], rdcz = A.rdc[2];
+  LARE_BOXWB(run, 5, 17, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt2 = (R)sc[SC_DT2];
     const int c = ix + sx * iy + sxy * iz;
     const int X = 1, Y = sx, Z = sxy;
@@ -530,18 +536,19 @@ void predictor_corrector_step(Run<R>& run) {
     R ppyz = pressure[c + Y + Z], ppxyz = pressure[c + X + Y + Z];
     R w1 = (pp + ppy + ppz + ppyz) * R(0.25);
     R w2 = (ppx + ppxy + ppxz + ppxyz) * R(0.25);
-    R fx = -(w2 - w1) / dxc(ix);
+    R fx = -div_rcp(w2 - w1, dxc(ix), rdcx(ix));
     w1 = (pp + ppx + ppz + ppxz) * R(0.25);
     w2 = (ppy + ppxy + ppyz + ppxyz) * R(0.25);
-    R fy = -(w2 - w1) / dyc(iy);
+    R fy = -div_rcp(w2 - w1, dyc(iy), rdcy(iy));
     w1 = (pp + ppx + ppy + ppxy) * R(0.25);
     w2 = (ppz + ppxz + ppyz + ppxyz) * R(0.25);
-    R fz = -(w2 - w1) / dzc(iz);
+    R fz = -div_rcp(w2 - w1, dzc(iz), rdcz(iz));
     R bxv = R(0.25) * (bx[c] + bx[c + Y] + bx[c + Z] + bx[c + Y + Z]);
     R byv = R(0.25) * (by[c] + by[c + X] + by[c + Z] + by[c + X + Z]);
     R bzv = R(0.25) * (bz[c] + bz[c + Y] + bz[c + X] + bz[c + X + Y]);
     R jx, jy, jz;
-    vertex_current<R>(bx, by, bz, c, sx, sxy, dxc(ix), dyc(iy), dzc(iz), jx, jy, jz);
+    vertex_current<R>(bx, by, bz, c, sx, sxy, dxc(ix), dyc(iy), dzc(iz), rdcx(ix), rdcy(iy), rdcz(iz), jx, jy,
+                      jz);
     R gb = gamma_boris[c];
     fx = fx + gb * (jy * bzv - jz * byv);
     fy = fy + gb * (jz * bxv - jx * bzv);
@@ -608,6 +615,7 @@ void predictor_corrector_step(Run<R>& run) {
   R* const cv1w = A.cv1.p;
   R* const rhow = A.rho.p;
   R* const visc_dep = A.visc_dep.p;
+  const auto rbx = A.rdb[0], rby = A.rdb[1], rbz = A.rdb[2];
   box_sum<1>(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
     const R dt = (R)sc[SC_DT];
     const int c = ix + sx * iy + sxy * iz;
@@ -618,7 +626,8 @@ void predictor_corrector_step(Run<R>& run) {
     R vybm = (vy1[c - Y] + vy1[c - X - Y] + vy1[c - Y - Z] + vy1[c - X - Y - Z]) * R(0.25);
     R vzb = (vz1[c] + vz1[c - X] + vz1[c - Y] + vz1[c - X - Y]) * R(0.25);
     R vzbm = (vz1[c - Z] + vz1[c - X - Z] + vz1[c - Y - Z] + vz1[c - X - Y - Z]) * R(0.25);
-    R dv = ((vxb - vxbm) / dxb(ix) + (vyb - vybm) / dyb(iy) + (vzb - vzbm) / dzb(iz)) * dt;
+    R dv = (div_rcp(vxb - vxbm, dxb(ix), rbx(ix)) + div_rcp(vyb - vybm, dyb(iy), rby(iy)) +
+            div_rcp(vzb - vzbm, dzb(iz), rbz(iz))) * dt;
     cv1w[c] = cv[c] * (R(1) + dv);
     R vh = vhp[c];
     R r = rhow[c];

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "../../include/lare_gpu.h"
+#include "common.cuh"
 #include "engine_base.h"
 
 struct lare_ctx {
@@ -18,6 +19,13 @@ namespace {
 bool bc_supported(int c) { return c == LARE_BC_PERIODIC || c == LARE_BC_USER; }
 
 int guard(lare_ctx* c) { return (c && c->e) ? LARE_OK : LARE_EINVAL; }
+
+__global__ void k_check_division(const double* a, const double* b, long long n, double* out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double rb = 1.0 / b[i];
+    out[i] = lare::div_rcp(a[i], b[i], rb);
+  }
+}
 }  // namespace
 
 extern "C" {
@@ -198,6 +206,14 @@ int lare_gpu_profile_report(lare_ctx* c, char* buf, int len) {
 }
 
 long long lare_gpu_launch_count(lare_ctx* c) { return (c && c->e) ? c->e->launches() : -1; }
+
+int lare_gpu_check_division(const double* a, const double* b, long long n, double* out, void* stream) {
+  if (n < 0 || (n > 0 && (!a || !b || !out))) return LARE_EINVAL;
+  if (n == 0) return LARE_OK;
+  const long long blocks = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
+  k_check_division<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(a, b, n, out);
+  return cudaGetLastError() == cudaSuccess ? LARE_OK : LARE_ECUDA;
+}
 
 void* lare_gpu_stream(lare_ctx* c) { return (c && c->e) ? c->e->stream() : nullptr; }
 

@@ -11,8 +11,8 @@
 //                 is recomputed in the thread for dxc1.
 //   K2 B fluxes   both constrained-transport edge fluxes (:340-470); the
 //                 second does not read what the first one's updates change.
-//                 The y and z sweeps use a marching kernel (each quotient
-//                 formed once); the x sweep forms them per cell.
+//                 The y and z sweeps use a marching kernel and the x sweep
+//                 a warp-shuffle kernel; both form each quotient once.
 //   K3 B update   the four flux-difference updates (:121-157), with each
 //                 file's own loop ranges as predicates.
 //   K4 mass flux  dm (:474-533) over the whole cell box, with dm_x_bcs
@@ -158,6 +158,52 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
   }
 }
 
+// K2 for the x sweep: the lanes of a warp hold consecutive x positions, and
+// the stencil neighbours along x (one to the left, two to the right) come
+// from the neighbouring lanes by shuffles, so a lane loads its own point
+// once and forms one quotient per flux.  A warp spans 32 positions and
+// writes the kXOut = 29 whose whole stencil lies inside it; warps overlap by
+// three positions.  Same expressions, same operands, same results bit for
+// bit as the per-cell form.
+constexpr int kXOut = 29;
+
+template <class R>
+__global__ void __launch_bounds__(128) k_bflux_x(BfArgs<R> a, int sx, int sxy, int nx, int ny) {
+  const int lane = (int)threadIdx.x;                           // blockDim.x == 32: one warp per row
+  const int ix = -2 + (int)blockIdx.x * kXOut + lane;          // this lane's x position
+  const int iy = -1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int iz = -1 + (int)blockIdx.z;
+  if (iy > ny + 1) return;                                      // uniform over the warp
+  const int c = min(ix, nx + 2) + sx * iy + sxy * iz;           // positions past n+2 load n+2 (unused)
+  R d1, d2;
+  const R q1 = bf_quot(a.b1, a.db1, c, a.SB1, d1);
+  const R q2 = bf_quot(a.b2, a.db1, c, a.SB2, d2);
+  const R dc = a.dc1[c], db = a.db1[c];
+  const unsigned all = 0xffffffffu;
+  const R q1m = __shfl_up_sync(all, q1, 1), q1p = __shfl_down_sync(all, q1, 1), q1p2 = __shfl_down_sync(all, q1, 2);
+  const R q2m = __shfl_up_sync(all, q2, 1), q2p = __shfl_down_sync(all, q2, 1), q2p2 = __shfl_down_sync(all, q2, 2);
+  const R d1p = __shfl_down_sync(all, d1, 1), d2p = __shfl_down_sync(all, d2, 1);
+  const R dcm = __shfl_up_sync(all, dc, 1), dcp = __shfl_down_sync(all, dc, 1);
+  const R dbp = __shfl_down_sync(all, db, 1);
+  if (lane < 1 || lane > kXOut || ix > nx + 1) return;
+  const bool left = ix > -1;            // cm = MAX(ix - 1, -1)
+  const bool right = ix + 2 <= nx + 2;  // cp2 = MIN(ix + 2, n + 2)
+  const R dt = (R)a.sc[a.dt_slot];
+  const R va0 = a.va[c], va1 = a.va[c - a.SO1], va2 = a.va[c - a.SO2];
+  {
+    const R v_advect = (va0 + va1) * R(0.5);
+    LimOut<R> L = limiter<R>(v_advect, left ? q1m : q1, q1, q1p, right ? q1p2 : q1p, dc, left ? dcm : dc, dcp, db,
+                             dbp, d1, d1p, dt, true);
+    a.f1[c] = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
+  }
+  {
+    const R v_advect = (va0 + va2) * R(0.5);
+    LimOut<R> L = limiter<R>(v_advect, left ? q2m : q2, q2, q2p, right ? q2p2 : q2p, dc, left ? dcm : dc, dcp, db,
+                             dbp, d2, d2p, dt, true);
+    a.f2[c] = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
+  }
+}
+
 // K1 as a z-marching kernel: a thread owns an (x, y) column and walks a
 // chunk of z.  Each face average (xremap.f90:64-86) sums two values of its
 // own plane and two of the plane below in that order, so the lower pair is
@@ -177,6 +223,7 @@ struct GeomArgs {
   R* db1;
   R* dc1;
   A1<R> dbm[3];
+  A1<R> rdbm[3];  // reciprocals of dbm, for div_rcp
   R pass_t1, pass_t2;
   const double* sc;
   int dt_slot, nx, ny, nz, sx, sxy;
@@ -247,9 +294,9 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
     if (A == 2 && iz < g.nz + 2) vz_next = vzf(c + sxy);
     const R dvv[3] = {vxb - vxbm, vyb - vybm, vzb - vzbm};
     const int pp[3] = {ix, iy, iz};
-    const R term_t1 = g.pass_t1 * dvv[T1] / g.dbm[T1](pp[T1]);
-    const R term_t2 = g.pass_t2 * dvv[T2] / g.dbm[T2](pp[T2]);
-    const R term_a = dvv[A] / g.dbm[A](pp[A]);
+    const R term_t1 = div_rcp(g.pass_t1 * dvv[T1], g.dbm[T1](pp[T1]), g.rdbm[T1](pp[T1]));
+    const R term_t2 = div_rcp(g.pass_t2 * dvv[T2], g.dbm[T2](pp[T2]), g.rdbm[T2](pp[T2]));
+    const R term_a = div_rcp(dvv[A], g.dbm[A](pp[A]), g.rdbm[A](pp[A]));
     R dv = (term_t1 + term_t2 + term_a) * dt;
     const R cvc = g.cv[c];
     g.cv1[c] = cvc * (R(1) + dv);
@@ -301,6 +348,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   const A1<R> dbm[3] = {Ar.dxb, Ar.dyb, Ar.dzb};
   const A1<R> dcm[3] = {Ar.dxc, Ar.dyc, Ar.dzc};
   const A1<R> dba = dbm[A], dbt1 = dbm[T1], dbt2 = dbm[T2], dct1 = dcm[T1], dct2 = dcm[T2];
+  const A1<R> rdba = Ar.rdb[A], rdbt1 = Ar.rdb[T1], rdbt2 = Ar.rdb[T2];
   const R pass_t1 = (R)pass[T1], pass_t2 = (R)pass[T2];
   const double* sc = run.sc;
   const bool write_cv2 = !predictor;
@@ -320,6 +368,9 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     ga.dbm[0] = Ar.dxb;
     ga.dbm[1] = Ar.dyb;
     ga.dbm[2] = Ar.dzb;
+    ga.rdbm[0] = Ar.rdb[0];
+    ga.rdbm[1] = Ar.rdb[1];
+    ga.rdbm[2] = Ar.rdb[2];
     ga.pass_t1 = pass_t1;
     ga.pass_t2 = pass_t2;
     ga.sc = sc;
@@ -349,9 +400,9 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
       R vzb = vzf(c), vzbm = vzf(c - sxy);
       R dvv[3] = {vxb - vxbm, vyb - vybm, vzb - vzbm};
       const int pp[3] = {ix, iy, iz};
-      R term_t1 = pass_t1 * dvv[T1] / dbt1(pp[T1]);
-      R term_t2 = pass_t2 * dvv[T2] / dbt2(pp[T2]);
-      R term_a = dvv[A] / dba(pp[A]);
+      R term_t1 = div_rcp(pass_t1 * dvv[T1], dbt1(pp[T1]), rdbt1(pp[T1]));
+      R term_t2 = div_rcp(pass_t2 * dvv[T2], dbt2(pp[T2]), rdbt2(pp[T2]));
+      R term_a = div_rcp(dvv[A], dba(pp[A]), rdba(pp[A]));
       R dv = (term_t1 + term_t2 + term_a) * dt;
       cv1[c] = cv[c] * (R(1) + dv);
       if (write_cv2) {
@@ -376,7 +427,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   R* const Bp[3] = {Ar.bx.p, Ar.by.p, Ar.bz.p};
   R* const f1 = Ar.f1.p;
   R* const f2 = Ar.f2.p;
-  if (A != 0) {
+  {
     BfArgs<R> ba;
     ba.va = va;
     ba.b1 = Bp[B1];
@@ -398,36 +449,17 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     ba.n0 = nx + 3;
     ba.n1 = (A == 1 ? nz : ny) + 3;
     const int k = run.prof_begin("remap_sweep_bflux", A, 7, (double)(nx + 3) * (ny + 3) * (nz + 3));
-    dim3 blk(32, 4, 1);
-    dim3 grd((ba.n0 + 31) / 32, (ba.n1 + 3) / 4, (na + 3 + kMarch - 1) / kMarch);
-    k_bflux_march<R><<<grd, blk, 0, run.s>>>(ba);
+    if (A != 0) {
+      dim3 blk(32, 4, 1);
+      dim3 grd((ba.n0 + 31) / 32, (ba.n1 + 3) / 4, (na + 3 + kMarch - 1) / kMarch);
+      k_bflux_march<R><<<grd, blk, 0, run.s>>>(ba);
+    } else {
+      dim3 blk(32, 4, 1);
+      dim3 grd((nx + 3 + kXOut - 1) / kXOut, (ny + 3 + 3) / 4, nz + 3);
+      k_bflux_x<R><<<grd, blk, 0, run.s>>>(ba, sx, sxy, nx, ny);
+    }
     run.prof_end(k);
     ++run.launches;
-  } else {
-    R* const Bb1 = Bp[B1];
-    R* const Bb2 = Bp[B2];
-    LARE_BOXW(run, 7, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
-      const R dt = (R)sc[dt_slot];
-      const int c = ix + sx * iy + sxy * iz;
-      const int ia = acoord<A>(ix, iy, iz);
-      const int cm = ia > -1 ? c - SA : c;             // MAX(ix - 1, -1)
-      const int cp = c + SA;
-      const int cp2 = ia + 2 <= na + 2 ? c + 2 * SA : cp;  // MIN(ix + 2, n + 2)
-      auto one = [&](const R* Bb, int SB, int SO) {
-        R v_advect = (va[c] + va[c - SO]) * R(0.5);
-        auto dbv = [&](int q) { return (db1[q] + db1[q + SB]) * R(0.5); };
-        R dbx = dbv(c), dbxp = dbv(cp), dbxp2 = dbv(cp2), dbxm = dbv(cm);
-        R fm = Bb[cm] / dbxm;
-        R fi = Bb[c] / dbx;
-        R fp = Bb[cp] / dbxp;
-        R fp2 = Bb[cp2] / dbxp2;
-        LimOut<R> L = limiter<R>(v_advect, fm, fi, fp, fp2, dc1[c], dc1[cm], dc1[cp], db1[c], db1[cp], dbx, dbxp,
-                                 dt, true);
-        return (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
-      };
-      f1[c] = one(Bb1, SB1, SO1);
-      f2[c] = one(Bb2, SB2, SO2);
-    });
   }
 
   // ---- K3: the four updates, each over its file's range
@@ -496,7 +528,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   });
 
   // ---- K5: new rho (second buffer) and the energy flux (0:n)
-  LARE_BOXW(run, 10, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWB(run, 6, 10, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     const bool in0 = ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz;
     const bool in1 = ix >= 1 && iy >= 1 && iz >= 1 && in0;
@@ -577,7 +609,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     int lo[3] = {0, 0, 0}, hi[3] = {nx, ny, nz};
     lo[A] = -1;
     hi[A] = na;
-    LARE_BOXW(run, 11, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
+    LARE_BOXWB(run, 6, 11, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
       const R dt = (R)sc[dt_slot];
       const int c = ix + sx * iy + sxy * iz;
       const int pp[3] = {ix, iy, iz};

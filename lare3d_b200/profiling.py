@@ -22,7 +22,7 @@ import sys
 
 
 def _short(name: str) -> str:
-    m = re.search(r"k_box<void (?:lare::)?(\w+)<([^>]*)>\(.*?\)::\[lambda\(int, int, int\) \(instance (\d+)\)\]>", name)
+    m = re.search(r"k_box(?:_mb<\d+, |<)void (?:lare::)?(\w+)<([^>]*)>\(.*?\)::\[lambda\(int, int, int\) \(instance (\d+)\)\]>", name)
     if m:
         return f"{m.group(1)}<{m.group(2)}> lambda {m.group(3)}"
     m = re.search(r"k_box_(sum|min)<\d+, void (?:lare::)?(\w+)<", name)

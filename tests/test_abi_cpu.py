@@ -55,6 +55,19 @@ def test_surrogate_host_side_argument_checks(built):
              5 / 3, 0.0, 0.0, 1e-3, p, p, None) == -1
 
 
+def test_division_check_argument_checks(built):
+    from lare3d_b200 import gpu
+    lib = gpu.library()
+    f = lib.lare_gpu_check_division
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    p = C.c_void_p(16)
+    assert f(p, p, -1, p, None) == -1
+    assert f(None, p, 4, p, None) == -1
+    assert f(p, p, 4, None, None) == -1
+    assert f(None, None, 0, None, None) == 0     # nothing to do, nothing launched
+
+
 def test_struct_layout_matches_header():
     txt = open(os.path.join(ROOT, "include", "lare_gpu.h")).read()
     body = txt[txt.index("typedef struct lare_params"):txt.index("} lare_params;")]
