@@ -163,21 +163,22 @@ __device__ __forceinline__ void block_sum_write(double (&v)[NV], double* partial
   }
 }
 
-// Each block covers kSumPlanes consecutive planes (fewer partials for the
-// final pass); a thread adds its points plane by plane, so the order of
-// every sum is fixed.
+// Each block covers `planes` consecutive planes (kSumPlanes by default:
+// fewer partials for the final pass; 1 for heavy point functions, whose
+// planes would otherwise run one after another); a thread adds its points
+// plane by plane, so the order of every sum is fixed.
 constexpr int kSumPlanes = 4;
 
 template <int NV, class Fn>
-__global__ void __launch_bounds__(256) k_box_sum(int i0, int j0, int k0, int ni, int nj, int nk, Fn fn,
+__global__ void __launch_bounds__(256) k_box_sum(int i0, int j0, int k0, int ni, int nj, int nk, int planes, Fn fn,
                                                  double* partial) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   double v[NV];
   for (int q = 0; q < NV; ++q) v[q] = 0.0;
   if (i < ni && j < nj) {
-    const int kb = (int)blockIdx.z * kSumPlanes;
-    for (int kk = kb; kk < kb + kSumPlanes && kk < nk; ++kk) {
+    const int kb = (int)blockIdx.z * planes;
+    for (int kk = kb; kk < kb + planes && kk < nk; ++kk) {
       double w[NV];
       for (int q = 0; q < NV; ++q) w[q] = 0.0;
       fn(i0 + i, j0 + j, k0 + kk, w);

@@ -194,13 +194,14 @@ inline void ghost(Run<R>& run, const GSpec& g, A3<R> a, A3<R>* b = nullptr, A3<R
 
 // Deterministic sum of NV values over a box, into sc[slot..] (+=).
 template <int NV, class R, class Fn>
-inline void box_sum(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn, int slot, bool acc) {
+inline void box_sum(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn, int slot, bool acc,
+                    int planes = kSumPlanes) {
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   dim3 blk(64, 4, 1);
-  dim3 grd((ni + 63) / 64, (nj + 3) / 4, (nk + kSumPlanes - 1) / kSumPlanes);
+  dim3 grd((ni + 63) / 64, (nj + 3) / 4, (nk + planes - 1) / planes);
   int nb = grd.x * grd.y * grd.z;
   int k = run.prof_begin("box_sum", 0, 0, (double)ni * nj * nk);
-  k_box_sum<NV><<<grd, blk, 0, run.s>>>(i0, j0, k0, ni, nj, nk, fn, run.partial);
+  k_box_sum<NV><<<grd, blk, 0, run.s>>>(i0, j0, k0, ni, nj, nk, planes, fn, run.partial);
   k_sum_partials<NV><<<1, 1024, 0, run.s>>>(run.partial, nb, run.sc + slot, acc ? 1 : 0);
   run.prof_end(k);
   run.launches += 2;

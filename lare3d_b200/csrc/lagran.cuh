@@ -35,12 +35,14 @@ namespace lare {
 
 // Vertex current of eta_calc (lagran.F90:1190-1216), rkstep (:1479-1494)
 // and the predictor force (:358-373): the three places use the same
-// expressions, evaluated here once.  The divisions by the cell widths use
-// their reciprocals (rx, ry, rz) through div_rcp, which returns the same
-// quotients.
-template <class R>
+// expressions, evaluated here once.  With RCP the divisions by the cell
+// widths go through their reciprocals (rx, ry, rz) and div_rcp, which
+// returns the same quotients; which form runs faster depends on the kernel
+// around it (measured: the predictor force takes RCP, eta_calc does not).
+template <class R, bool RCP>
 __device__ __forceinline__ void vertex_current(const R* bx, const R* by, const R* bz, int c, int sx, int sxy,
                                                R dxc, R dyc, R dzc, R rx, R ry, R rz, R& jx, R& jy, R& jz) {
+  auto div_rcp = [](R a, R b, R r) { return RCP ? lare::div_rcp(a, b, r) : a / b; };
   R jx1 = div_rcp(bz[c + sx] - bz[c], dyc, ry) - div_rcp(by[c + sxy] - by[c], dzc, rz);
   R jx2 = div_rcp(bz[c + 1 + sx] - bz[c + 1], dyc, ry) - div_rcp(by[c + 1 + sxy] - by[c + 1], dzc, rz);
   R jy1 = div_rcp(bx[c + sxy] - bx[c], dzc, rz) - div_rcp(bz[c + 1] - bz[c], dxc, rx);
@@ -77,8 +79,8 @@ void eta_and_rkstep(Run<R>& run, bool with_rkstep) {
   LARE_BOXWB(run, 5, with_rkstep ? 8 : 4, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     R jx, jy, jz;
-    vertex_current<R>(bx, by, bz, c, sx, sxy, dxc(ix), dyc(iy), dzc(iz), rdcx(ix), rdcy(iy), rdcz(iz), jx, jy,
-                      jz);
+    vertex_current<R, false>(bx, by, bz, c, sx, sxy, dxc(ix), dyc(iy), dzc(iz), rdcx(ix), rdcy(iy), rdcz(iz), jx,
+                             jy, jz);
     R j2 = jx * jx + jy * jy + jz * jz;
     R e = sqrt(j2) > jmax ? eb + e0 : eb;
     eta[c] = e;
@@ -547,8 +549,8 @@ void predictor_corrector_step(Run<R>& run) {
     R byv = R(0.25) * (by[c] + by[c + X] + by[c + Z] + by[c + X + Z]);
     R bzv = R(0.25) * (bz[c] + bz[c + Y] + bz[c + X] + bz[c + X + Y]);
     R jx, jy, jz;
-    vertex_current<R>(bx, by, bz, c, sx, sxy, dxc(ix), dyc(iy), dzc(iz), rdcx(ix), rdcy(iy), rdcz(iz), jx, jy,
-                      jz);
+    vertex_current<R, true>(bx, by, bz, c, sx, sxy, dxc(ix), dyc(iy), dzc(iz), rdcx(ix), rdcy(iy), rdcz(iz), jx,
+                            jy, jz);
     R gb = gamma_boris[c];
     fx = fx + gb * (jy * bzv - jz * byv);
     fy = fy + gb * (jz * bxv - jx * bzv);
@@ -615,7 +617,6 @@ void predictor_corrector_step(Run<R>& run) {
   R* const cv1w = A.cv1.p;
   R* const rhow = A.rho.p;
   R* const visc_dep = A.visc_dep.p;
-  const auto rbx = A.rdb[0], rby = A.rdb[1], rbz = A.rdb[2];
   box_sum<1>(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
     const R dt = (R)sc[SC_DT];
     const int c = ix + sx * iy + sxy * iz;
@@ -626,8 +627,7 @@ void predictor_corrector_step(Run<R>& run) {
     R vybm = (vy1[c - Y] + vy1[c - X - Y] + vy1[c - Y - Z] + vy1[c - X - Y - Z]) * R(0.25);
     R vzb = (vz1[c] + vz1[c - X] + vz1[c - Y] + vz1[c - X - Y]) * R(0.25);
     R vzbm = (vz1[c - Z] + vz1[c - X - Z] + vz1[c - Y - Z] + vz1[c - X - Y - Z]) * R(0.25);
-    R dv = (div_rcp(vxb - vxbm, dxb(ix), rbx(ix)) + div_rcp(vyb - vybm, dyb(iy), rby(iy)) +
-            div_rcp(vzb - vzbm, dzb(iz), rbz(iz))) * dt;
+    R dv = ((vxb - vxbm) / dxb(ix) + (vyb - vybm) / dyb(iy) + (vzb - vzbm) / dzb(iz)) * dt;
     cv1w[c] = cv[c] * (R(1) + dv);
     R vh = vhp[c];
     R r = rhow[c];

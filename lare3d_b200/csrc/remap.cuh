@@ -164,11 +164,13 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
 // once and forms one quotient per flux.  A warp spans 32 positions and
 // writes the kXOut = 29 whose whole stencil lies inside it; warps overlap by
 // three positions.  Same expressions, same operands, same results bit for
-// bit as the per-cell form.
+// bit as the per-cell form.  The launch bounds cap the FP64 form at 48
+// registers: it is latency-bound, and the extra resident warps outweigh the
+// few spills (measured at 256^3).
 constexpr int kXOut = 29;
 
 template <class R>
-__global__ void __launch_bounds__(128) k_bflux_x(BfArgs<R> a, int sx, int sxy, int nx, int ny) {
+__global__ void __launch_bounds__(128, 10) k_bflux_x(BfArgs<R> a, int sx, int sxy, int nx, int ny) {
   const int lane = (int)threadIdx.x;                           // blockDim.x == 32: one warp per row
   const int ix = -2 + (int)blockIdx.x * kXOut + lane;          // this lane's x position
   const int iy = -1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
@@ -294,9 +296,14 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
     if (A == 2 && iz < g.nz + 2) vz_next = vzf(c + sxy);
     const R dvv[3] = {vxb - vxbm, vyb - vybm, vzb - vzbm};
     const int pp[3] = {ix, iy, iz};
-    const R term_t1 = div_rcp(g.pass_t1 * dvv[T1], g.dbm[T1](pp[T1]), g.rdbm[T1](pp[T1]));
-    const R term_t2 = div_rcp(g.pass_t2 * dvv[T2], g.dbm[T2](pp[T2]), g.rdbm[T2](pp[T2]));
-    const R term_a = div_rcp(dvv[A], g.dbm[A](pp[A]), g.rdbm[A](pp[A]));
+    // quotients by the metrics: through their reciprocals for the z sweep;
+    // the x sweep's form (three x faces live) is faster with plain division
+    auto quot = [&](R a, int d) {
+      return A == 0 ? a / g.dbm[d](pp[d]) : div_rcp(a, g.dbm[d](pp[d]), g.rdbm[d](pp[d]));
+    };
+    const R term_t1 = quot(g.pass_t1 * dvv[T1], T1);
+    const R term_t2 = quot(g.pass_t2 * dvv[T2], T2);
+    const R term_a = quot(dvv[A], A);
     R dv = (term_t1 + term_t2 + term_a) * dt;
     const R cvc = g.cv[c];
     g.cv1[c] = cvc * (R(1) + dv);
