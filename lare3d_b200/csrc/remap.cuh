@@ -325,6 +325,127 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
   }
 }
 
+// K7 as a z-marching kernel: a thread owns an (x, y) column of vertices and
+// walks a chunk of z.  The eight cells around vertex (x, y, z) are the
+// (x..x+1, y..y+1) quads of planes z and z+1, summed lower quad first in
+// the reference's order, so each step loads the upper quad of each input
+// and carries it down as the next vertex's lower quad: 18 to 20 loads per
+// vertex instead of 40, the same sums in the same order, the same results
+// bit for bit.  dm around c - e_A needs the quads of planes z-1 and z (A = z,
+// one more plane carried) or the quads shifted by one cell in x or y (two
+// more loads per plane).
+constexpr int kVertZ = 32;
+
+template <class R>
+struct VertArgs {
+  const R* rho;
+  const R* cv1;
+  const R* cv2;
+  const R* dm;
+  R* rv;
+  R* rv1;
+  R* cv1v;
+  R* cv2v;
+  R* dmv;
+  int lo[3], hi[3];
+  int na, sx, sxy;
+};
+
+template <int A, class R>
+__global__ void __launch_bounds__(128) k_vert_march(VertArgs<R> g) {
+  const int ix = g.lo[0] + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int iy = g.lo[1] + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  if (ix > g.hi[0] || iy > g.hi[1]) return;
+  const int z0 = g.lo[2] + (int)blockIdx.z * kVertZ;
+  const int z1 = min(z0 + kVertZ - 1, g.hi[2]);
+  const int sx = g.sx, sxy = g.sxy, na = g.na;
+  const int q1 = 1, q2 = sx, q3 = 1 + sx;                     // quad offsets after 0
+  const int e0 = A == 0 ? -1 : -sx, e1 = A == 0 ? -1 + sx : 1 - sx;  // shifted-quad cells not in the quad
+  int c = ix + sx * iy + sxy * z0;
+  // lower quads (plane z0)
+  R pr[4], c1[4], c2[4], d[4], dx[2], dz[4];
+  auto load = [&](int b, R (&p)[4], R (&w1)[4], R (&w2)[4], R (&m)[4], R (&mx)[2]) {
+    const int o[4] = {0, q1, q2, q3};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      w1[q] = g.cv1[b + o[q]];
+      p[q] = g.rho[b + o[q]] * w1[q];
+      w2[q] = g.cv2[b + o[q]];
+      m[q] = g.dm[b + o[q]];
+    }
+    if (A != 2) {
+      mx[0] = g.dm[b + e0];
+      mx[1] = g.dm[b + e1];
+    }
+  };
+  load(c, pr, c1, c2, d, dx);
+  if (A == 2) {
+    const int b = c - sxy;
+    dz[0] = g.dm[b];
+    dz[1] = g.dm[b + q1];
+    dz[2] = g.dm[b + q2];
+    dz[3] = g.dm[b + q3];
+  }
+  for (int iz = z0; iz <= z1; ++iz, c += sxy) {
+    R pu[4], cu1[4], cu2[4], du[4], dxu[2];
+    load(c + sxy, pu, cu1, cu2, du, dxu);
+    const int ia = A == 0 ? ix : (A == 1 ? iy : iz);
+    R s = pr[0], w = c1[0];
+#pragma unroll
+    for (int q = 1; q < 4; ++q) {
+      s = s + pr[q];
+      w = w + c1[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      s = s + pu[q];
+      w = w + cu1[q];
+    }
+    const R rvc = s / w;
+    g.rv[c] = rvc;
+    R tp = d[0];
+#pragma unroll
+    for (int q = 1; q < 4; ++q) tp = tp + d[q];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) tp = tp + du[q];
+    if (ia <= na) g.dmv[c] = tp * R(0.125);
+    if (ia >= 0 && ia <= na) {
+      R w2 = c2[0];
+#pragma unroll
+      for (int q = 1; q < 4; ++q) w2 = w2 + c2[q];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w2 = w2 + cu2[q];
+      const R cc1 = w * R(0.125), cc2 = w2 * R(0.125);
+      g.cv1v[c] = cc1;
+      g.cv2v[c] = cc2;
+      // dm summed over the cells around c - e_A, lower quad first
+      R tm;
+      if (A == 2) {
+        tm = dz[0] + dz[1] + dz[2] + dz[3] + d[0] + d[1] + d[2] + d[3];
+      } else if (A == 0) {  // quad cells (x-1, y), (x, y), (x-1, y+1), (x, y+1)
+        tm = dx[0] + d[0] + dx[1] + d[2] + dxu[0] + du[0] + dxu[1] + du[2];
+      } else {              // quad cells (x, y-1), (x+1, y-1), (x, y), (x+1, y)
+        tm = dx[0] + dx[1] + d[0] + d[1] + dxu[0] + dxu[1] + du[0] + du[1];
+      }
+      const R dmm = tm * R(0.125);
+      const R dmp = tp * R(0.125);
+      g.rv1[c] = (rvc * cc1 + dmm - dmp) / cc2;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (A == 2) dz[q] = d[q];
+      pr[q] = pu[q];
+      c1[q] = cu1[q];
+      c2[q] = cu2[q];
+      d[q] = du[q];
+    }
+    if (A != 2) {
+      dx[0] = dxu[0];
+      dx[1] = dxu[1];
+    }
+  }
+}
+
 template <int A, class R>
 void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   constexpr int T1 = A == 0 ? 1 : 0, T2 = A == 2 ? 1 : 2;  // transverse axes, T1 < T2
@@ -572,36 +693,30 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     int lo[3] = {0, 0, 0}, hi[3] = {nx, ny, nz};
     lo[A] = -1;
     hi[A] = na + 1;
-    LARE_BOXW(run, 9, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
-      const int c = ix + sx * iy + sxy * iz;
-      const int ia = acoord<A>(ix, iy, iz);
-      // the eight cells around vertex c, in the reference's summation order
-      const int o[8] = {0, 1, sx, 1 + sx, sxy, 1 + sxy, sx + sxy, 1 + sx + sxy};
-      R s = rho[c + o[0]] * cv1[c + o[0]];
-      R w = cv1[c + o[0]];
-      for (int q = 1; q < 8; ++q) {
-        s = s + rho[c + o[q]] * cv1[c + o[q]];
-        w = w + cv1[c + o[q]];
-      }
-      R rvc = s / w;
-      rv[c] = rvc;
-      auto avg_dm = [&](int b) {
-        R t = dm[b + o[0]];
-        for (int q = 1; q < 8; ++q) t = t + dm[b + o[q]];
-        return t;
-      };
-      if (ia <= na) dmv[c] = avg_dm(c) * R(0.125);
-      if (ia >= 0 && ia <= na) {
-        R w2 = cv2[c + o[0]];
-        for (int q = 1; q < 8; ++q) w2 = w2 + cv2[c + o[q]];
-        R c1 = w * R(0.125), c2 = w2 * R(0.125);
-        cv1v[c] = c1;
-        cv2v[c] = c2;
-        R dmm = avg_dm(c - SA) * R(0.125);
-        R dmp = avg_dm(c) * R(0.125);
-        rv1[c] = (rvc * c1 + dmm - dmp) / c2;
-      }
-    });
+    VertArgs<R> va7;
+    va7.rho = rho;
+    va7.cv1 = cv1;
+    va7.cv2 = cv2;
+    va7.dm = dm;
+    va7.rv = rv;
+    va7.rv1 = rv1;
+    va7.cv1v = cv1v;
+    va7.cv2v = cv2v;
+    va7.dmv = dmv;
+    for (int d = 0; d < 3; ++d) {
+      va7.lo[d] = lo[d];
+      va7.hi[d] = hi[d];
+    }
+    va7.na = na;
+    va7.sx = sx;
+    va7.sxy = sxy;
+    dim3 blk(32, 4, 1);
+    dim3 grd((hi[0] - lo[0] + 32) / 32, (hi[1] - lo[1] + 4) / 4, (hi[2] - lo[2] + kVertZ) / kVertZ);
+    const int k = run.prof_begin("remap_sweep_vert", A, 9,
+                                 (double)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1));
+    k_vert_march<A, R><<<grd, blk, 0, run.s>>>(va7);
+    run.prof_end(k);
+    ++run.launches;
   }
 
   // ---- K8: momentum fluxes at vertex faces a -1:n, transverse 0:n
