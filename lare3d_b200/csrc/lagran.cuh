@@ -472,6 +472,99 @@ void predictor_remap(Run<R>& run, int step) {
   bfield_bcs(run);
 }
 
+// PC3 (shock_heating, lagran.F90:396-458, and v = 2 v1 - v) as a
+// z-marching kernel: a thread owns an (x, y) column of cells and walks a
+// chunk of z.  The twelve edge terms of cell (x, y, z) join the four
+// corners of plane z-1 (c-Z, c-X-Z, c-Y-Z, c-X-Y-Z) and of plane z (c,
+// c-X, c-Y, c-X-Y); the plane z-1 edges are the previous cell's plane z
+// edges, and the plane z-1 corner values are the previous step's, so a step
+// loads the four new corners and forms eight edge terms instead of twelve.
+// alpha1 and alpha2 at c+Z, c+Y+Z, c-X+Z are the next cell's c, c+Y, c-X.
+// Same expressions, same operands, same results bit for bit.
+constexpr int kShockZ = 32;
+
+template <class R>
+struct ShockArgs {
+  const R* v[6];  // vx, vy, vz, vx1, vy1, vz1
+  const R* alpha1;
+  const R* alpha2;
+  const R* alpha3;
+  const R* cv;
+  R* vhp;
+  R* nv[3];
+  A1<R> dxb, dyb, dzb;
+  int nx, ny, nz, sx, sxy;
+};
+
+template <class R>
+__global__ void __launch_bounds__(128) k_shock_march(ShockArgs<R> g) {
+  const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  if (ix > g.nx + 1 || iy > g.ny + 1) return;
+  const int z0 = (int)blockIdx.z * kShockZ;
+  const int z1 = min(z0 + kShockZ - 1, g.nz + 1);
+  const int sx = g.sx, sxy = g.sxy;
+  const int X = 1, Y = sx;
+  const int off[4] = {0, -X, -Y, -X - Y};  // corners c, c-X, c-Y, c-X-Y of a plane
+  R lo[6][4];
+  int c = ix + sx * iy + sxy * z0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) lo[k][q] = g.v[k][c - sxy + off[q]];
+  // dd of two corners: sum over the components of dv * dv1
+  auto dd = [](const R (&p)[6][4], int i, const R (&r)[6][4], int j) {
+    return (p[0][i] - r[0][j]) * (p[3][i] - r[3][j]) + (p[1][i] - r[1][j]) * (p[4][i] - r[4][j]) +
+           (p[2][i] - r[2][j]) * (p[5][i] - r[5][j]);
+  };
+  // plane z0-1 edges: a1 = (c-X-Y-Z, c-Y-Z), a2 = (c-Y-Z, c-Z), a3 = (c-Z, c-X-Z), a4 = (c-X-Z, c-X-Y-Z)
+  R a1 = dd(lo, 3, lo, 2), a2 = dd(lo, 2, lo, 0), a3 = dd(lo, 0, lo, 1), a4 = dd(lo, 1, lo, 3);
+  R al1 = g.alpha1[c], al1y = g.alpha1[c + Y], al2 = g.alpha2[c], al2x = g.alpha2[c - X];
+  const R ddx = g.dxb(ix), ddy = g.dyb(iy);
+  for (int iz = z0; iz <= z1; ++iz, c += sxy) {
+    R up[6][4];
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) up[k][q] = g.v[k][c + off[q]];
+    const R a5 = dd(up, 3, up, 2);   // (c-X-Y, c-Y)
+    const R a6 = dd(up, 2, up, 0);   // (c-Y, c)
+    const R a7 = dd(up, 0, up, 1);   // (c, c-X)
+    const R a8 = dd(up, 1, up, 3);   // (c-X, c-X-Y)
+    const R a9 = dd(lo, 0, up, 0);   // (c-Z, c)
+    const R a10 = dd(lo, 1, up, 1);  // (c-X-Z, c-X)
+    const R a11 = dd(lo, 3, up, 3);  // (c-X-Y-Z, c-X-Y)
+    const R a12 = dd(lo, 2, up, 2);  // (c-Y-Z, c-Y)
+    const R al1z = g.alpha1[c + sxy], al1yz = g.alpha1[c + Y + sxy];
+    const R al2z = g.alpha2[c + sxy], al2xz = g.alpha2[c - X + sxy];
+    const R ddz = g.dzb(iz);
+    R vh = -R(0.25) * ddy * ddz * al1 * a1 - R(0.25) * ddx * ddz * al2 * a2 -
+           R(0.25) * ddy * ddz * al1y * a3 - R(0.25) * ddx * ddz * al2x * a4 -
+           R(0.25) * ddy * ddz * al1z * a5 - R(0.25) * ddx * ddz * al2z * a6 -
+           R(0.25) * ddy * ddz * al1yz * a7 - R(0.25) * ddx * ddz * al2xz * a8 -
+           R(0.25) * ddx * ddy * g.alpha3[c] * a9 - R(0.25) * ddx * ddy * g.alpha3[c - X] * a10 -
+           R(0.25) * ddx * ddy * g.alpha3[c - X - Y] * a11 - R(0.25) * ddx * ddy * g.alpha3[c - Y] * a12;
+    R v = vh / g.cv[c];
+    g.vhp[c] = v > R(0) ? v : R(0);
+    if (ix <= g.nx && iy <= g.ny && iz <= g.nz) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) g.nv[k][c] = R(2) * up[k + 3][0] - up[k][0];
+    }
+    a1 = a5;
+    a2 = a6;
+    a3 = a7;
+    a4 = a8;
+    al1 = al1z;
+    al1y = al1yz;
+    al2 = al2z;
+    al2x = al2xz;
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) lo[k][q] = up[k][q];
+  }
+}
+
 // ---------------------------------------------------------------------
 // lagran.F90:208-478 predictor_corrector_step (non-CAUCHY, no cooling),
 // including the energy0 + delta_energy / MAX(energy, 0) of :180-181.
@@ -575,40 +668,33 @@ void predictor_corrector_step(Run<R>& run) {
   R* const nvy = A.qy.p;
   R* const nvz = A.qz.p;
   auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb;
-  LARE_BOXW(run, 14, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
-    const int c = ix + sx * iy + sxy * iz;
-    const int X = 1, Y = sx, Z = sxy;
-    auto dd = [&](int p0, int p1) {
-      return (vx[p0] - vx[p1]) * (vx1[p0] - vx1[p1]) + (vy[p0] - vy[p1]) * (vy1[p0] - vy1[p1]) +
-             (vz[p0] - vz[p1]) * (vz1[p0] - vz1[p1]);
-    };
-    R a1 = dd(c - X - Y - Z, c - Y - Z);
-    R a2 = dd(c - Y - Z, c - Z);
-    R a3 = dd(c - Z, c - X - Z);
-    R a4 = dd(c - X - Z, c - X - Y - Z);
-    R a5 = dd(c - X - Y, c - Y);
-    R a6 = dd(c - Y, c);
-    R a7 = dd(c, c - X);
-    R a8 = dd(c - X, c - X - Y);
-    R a9 = dd(c - Z, c);
-    R a10 = dd(c - X - Z, c - X);
-    R a11 = dd(c - X - Y - Z, c - X - Y);
-    R a12 = dd(c - Y - Z, c - Y);
-    R ddx = dxb(ix), ddy = dyb(iy), ddz = dzb(iz);
-    R vh = -R(0.25) * ddy * ddz * alpha1[c] * a1 - R(0.25) * ddx * ddz * alpha2[c] * a2 -
-           R(0.25) * ddy * ddz * alpha1[c + Y] * a3 - R(0.25) * ddx * ddz * alpha2[c - X] * a4 -
-           R(0.25) * ddy * ddz * alpha1[c + Z] * a5 - R(0.25) * ddx * ddz * alpha2[c + Z] * a6 -
-           R(0.25) * ddy * ddz * alpha1[c + Y + Z] * a7 - R(0.25) * ddx * ddz * alpha2[c - X + Z] * a8 -
-           R(0.25) * ddx * ddy * alpha3[c] * a9 - R(0.25) * ddx * ddy * alpha3[c - X] * a10 -
-           R(0.25) * ddx * ddy * alpha3[c - X - Y] * a11 - R(0.25) * ddx * ddy * alpha3[c - Y] * a12;
-    R v = vh / cv[c];
-    vhp[c] = v > R(0) ? v : R(0);
-    if (ix <= nx && iy <= ny && iz <= nz) {
-      nvx[c] = R(2) * vx1[c] - vx[c];
-      nvy[c] = R(2) * vy1[c] - vy[c];
-      nvz[c] = R(2) * vz1[c] - vz[c];
-    }
-  });
+  {
+    ShockArgs<R> ga;
+    const R* vs[6] = {vx, vy, vz, vx1, vy1, vz1};
+    for (int k = 0; k < 6; ++k) ga.v[k] = vs[k];
+    ga.alpha1 = alpha1;
+    ga.alpha2 = alpha2;
+    ga.alpha3 = alpha3;
+    ga.cv = cv;
+    ga.vhp = vhp;
+    ga.nv[0] = nvx;
+    ga.nv[1] = nvy;
+    ga.nv[2] = nvz;
+    ga.dxb = dxb;
+    ga.dyb = dyb;
+    ga.dzb = dzb;
+    ga.nx = nx;
+    ga.ny = ny;
+    ga.nz = nz;
+    ga.sx = sx;
+    ga.sxy = sxy;
+    dim3 blk(32, 4, 1);
+    dim3 grd((nx + 2 + 31) / 32, (ny + 2 + 3) / 4, (nz + 2 + kShockZ - 1) / kShockZ);
+    const int k = run.prof_begin("shock_heating", 0, 14, (double)(nx + 2) * (ny + 2) * (nz + 2));
+    k_shock_march<R><<<grd, blk, 0, run.s>>>(ga);
+    run.prof_end(k);
+    ++run.launches;
+  }
   std::swap(A.vx.p, A.qx.p);
   std::swap(A.vy.p, A.qy.p);
   std::swap(A.vz.p, A.qz.p);
