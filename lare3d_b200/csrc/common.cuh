@@ -299,32 +299,38 @@ __global__ void __launch_bounds__(256) k_ghost(GSpec s, R* p0, R* p1, R* p2, int
 }
 
 template <class R>
-__device__ __forceinline__ void ghost_point(const GSpec& s, R* p0, R* p1, R* p2, int sx, int sxy, long long t) {
+__device__ __forceinline__ void ghost_point(const GSpec& s, R* p0, R* p1, R* p2, int sx, int sxy, long long t64) {
   const GDim &X = s.d[0], &Y = s.d[1], &Z = s.d[2];
+  // 32-bit index arithmetic (the host keeps c0 + c1 + c2 below 2^31): a
+  // 64-bit division costs several times a 32-bit one, and these kernels
+  // are dominated by it
+  const unsigned c0 = (unsigned)s.c0, c1 = (unsigned)s.c1, c2 = (unsigned)s.c2;
+  unsigned t = (unsigned)t64;
+  if (t64 >= (long long)c0 + c1 + c2) return;
   int i, j, k;
-  if (t < s.c0) {
-    int iw = (int)(t % X.nw);
-    long long r = t / X.nw;
-    int ey = Y.hi - Y.lo + 1;
-    i = X.widx[iw];
-    j = Y.lo + (int)(r % ey);
-    k = Z.lo + (int)(r / ey);
-  } else if (t < s.c0 + s.c1) {
-    t -= s.c0;
-    int ex = X.b - X.a + 1;
-    i = X.a + (int)(t % ex);
-    long long r = t / ex;
-    j = Y.widx[(int)(r % Y.nw)];
-    k = Z.lo + (int)(r / Y.nw);
-  } else if (t < s.c0 + s.c1 + s.c2) {
-    t -= s.c0 + s.c1;
-    int ex = X.b - X.a + 1, ey = Y.b - Y.a + 1;
-    i = X.a + (int)(t % ex);
-    long long r = t / ex;
-    j = Y.a + (int)(r % ey);
-    k = Z.widx[(int)(r / ey)];
+  if (t < c0) {
+    const unsigned nw = (unsigned)X.nw, ey = (unsigned)(Y.hi - Y.lo + 1);
+    const unsigned r = t / nw;
+    i = X.widx[t - r * nw];
+    const unsigned rk = r / ey;
+    j = Y.lo + (int)(r - rk * ey);
+    k = Z.lo + (int)rk;
+  } else if (t < c0 + c1) {
+    t -= c0;
+    const unsigned ex = (unsigned)(X.b - X.a + 1), nw = (unsigned)Y.nw;
+    const unsigned r = t / ex;
+    i = X.a + (int)(t - r * ex);
+    const unsigned rk = r / nw;
+    j = Y.widx[r - rk * nw];
+    k = Z.lo + (int)rk;
   } else {
-    return;
+    t -= c0 + c1;
+    const unsigned ex = (unsigned)(X.b - X.a + 1), ey = (unsigned)(Y.b - Y.a + 1);
+    const unsigned r = t / ex;
+    i = X.a + (int)(t - r * ex);
+    const unsigned rk = r / ey;
+    j = Y.a + (int)(r - rk * ey);
+    k = Z.widx[rk];
   }
   bool zero = false;
   int si = gmap(X, i, zero), sj = gmap(Y, j, zero), sk = gmap(Z, k, zero);

@@ -268,6 +268,10 @@ class EngineT : public EngineBase {
     run.g_cell_mpi = spec(sc3, true, false);
     run.g_cell_user = spec(sc3, false, true);
     for (int d = 0; d < 3; ++d) run.g_dm[d] = spec(sc3, true, false, d);
+    // the fill kernels index a job's points in 32 bits
+    for (const GSpec* g : {&run.g_cell, &run.g_node, &run.g_bx, &run.g_by, &run.g_bz, &run.g_cell_mpi,
+                           &run.g_cell_user, &run.g_dm[0], &run.g_dm[1], &run.g_dm[2]})
+      if (g->c0 + g->c1 + g->c2 >= (1LL << 31)) return fail(LARE_EINVAL, "grid too large for the ghost fills");
 
     auto add = [&](const char* name, A3<R>* a, int l0, int h0, int l1, int h1, int l2, int h2) {
       FieldDesc f{{l0, l1, l2}, {h0, h1, h2}};
