@@ -22,8 +22,9 @@
 //                 readable as rho1) and the energy flux (:539-601).
 //   K6 energy     energy update (:187-196).
 //   K7 vertex     vertex rho_v, cv1, cv2, dm averages and rho_v1 (:201-290).
-//   K8 momentum   the three momentum fluxes (:605-895), each times dm.
-//   K9 velocity   the three velocity updates (:292-329).
+//   K8 momentum   the three momentum fluxes (:605-895), each times dm, and
+//   K9 velocity   the three velocity updates (:292-329), fused into one
+//                 kernel that writes the new velocities to second buffers.
 // The face-averaged vx1 written back at :265 is only read again as
 // REAL(xpass)*(...) with xpass = 0, so it is formed in K8 and not stored.
 // Predictor sweeps (predictor_step = .TRUE.) stop after K3.
@@ -446,6 +447,162 @@ __global__ void __launch_bounds__(128) k_vert_march(VertArgs<R> g) {
   }
 }
 
+// K8 + K9 fused: the momentum fluxes (xremap.f90:605-895, each times dm)
+// and the velocity updates that consume them (:292-329).  K9 updates v in
+// place while K8's stencil reads v around each face, so the fused kernel
+// writes the new velocities to a second set of buffers (swapped in by the
+// caller; their ghosts are refilled by boundary_conditions right after) and
+// never stores the fluxes: the update at c needs the fluxes at faces c-e_A
+// and c.  x sweep: the lanes of a warp hold consecutive faces and pass the
+// flux one lane up (31 updates per 32 lanes).  y and z sweeps: a thread
+// walks kMomA faces along A, carrying the stencil windows (one new point
+// per step) and the flux of the face behind; its register cap (launch
+// bounds) is the measured best per precision.  Every flux and update is the
+// reference's expression over the same operands, so the results are
+// identical bit for bit.
+constexpr int kMomA = 32;
+
+template <class R>
+struct MomArgs {
+  const R* va;  // v1 along A
+  const R* rv;
+  const R* dmv;
+  const R* db1;
+  const R* dc1;
+  const R* v[3];
+  R* vn[3];
+  const R* cv1v;
+  const R* cv2v;
+  const R* rv1;
+  A1<R> dct1, dct2;
+  const double* sc;
+  int dt_slot, nx, ny, nz, na, n3, sx, sxy, SA, S3;
+};
+
+// the three momentum fluxes through a face (K8's body) from its stencil
+// values: w[comp] = v at c-e_A, c, c+e_A, c+2e_A; db1 at c, c+e_A, c+2e_A;
+// dc1 at c, c+e_A; v1 (va), rho_v (rv) at c, c+e_A; dm at c
+template <class R>
+__device__ __forceinline__ void mom_flux_vals(R area, R va0, R va1, R rvc, R rvp, R dmc, R db0, R db1, R db2, R dc0,
+                                              R dc1, const R (&w)[3][4], R dt, R (&F)[3]) {
+  const R v_advect = (va0 + va1) * R(0.5);  // the face-averaged v1 of xremap.f90:257-265
+  // The upwind choice, phi and dmu depend only on v_advect and the
+  // geometry, so they are formed once for the three components (the same
+  // expressions the limiter evaluates per component).
+  const R dxci = db1, dxcm = db0, dxcp = db2, dxbi = dc0, dxbp = dc1;
+  const R sign_v = copysign(R(1), v_advect);
+  const R vad_p = (sign_v + R(1)) * R(0.5);
+  const R vad_m = R(1) - vad_p;
+  const R dxcu = dxcm * vad_p + dxcp * vad_m;
+  const R dxbu = dxbi * vad_p + dxbp * vad_m;
+  const R phi = fabs(v_advect) * dt / dxbu;
+  const R rhou = rvc * vad_p + rvp * vad_m;
+  const R dmu = fabs(dmc) / area / dxbu / rhou;
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+    const R fm = w[comp][0], fi = w[comp][1], fp = w[comp][2], fp2 = w[comp][3];
+    const R dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
+    const R fu = fi * vad_p + fp * vad_m;
+    const R dfu = dfm * vad_p + dfp * vad_m;
+    R Da = (R(2) - phi) * fabs(dfi) / dxci + (R(1) + phi) * fabs(dfu) / dxcu;
+    Da = Da * (R(1) / R(6));
+    const R ss = R(0.5) * (copysign(R(1), dfi) + copysign(R(1), dfu));
+    const R Di = sign_v * ss * fmin(fmin(fabs(Da) * dxbu, fabs(dfi)), fabs(dfu));
+    const R f = fu + Di * (R(1) - dmu);
+    F[comp] = f * dmc;
+  }
+}
+
+// the same, loading the stencil of face c
+template <class R>
+__device__ __forceinline__ void mom_flux(const MomArgs<R>& g, int c, int i1, int i2, R dt, R (&F)[3]) {
+  const int SA = g.SA;
+  R w[3][4];
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[comp][q] = g.v[comp][c + (q - 1) * SA];
+  mom_flux_vals(g.dct1(i1) * g.dct2(i2), g.va[c], g.va[c + SA], g.rv[c], g.rv[c + SA], g.dmv[c], g.db1[c],
+                g.db1[c + SA], g.db1[c + 2 * SA], g.dc1[c], g.dc1[c + SA], w, dt, F);
+}
+
+// K9's update at c from the fluxes at faces c - e_A (Fm) and c (F)
+template <class R>
+__device__ __forceinline__ void mom_update(const MomArgs<R>& g, int c, const R (&Fm)[3], const R (&F)[3]) {
+  const R rvc = g.rv[c], c1 = g.cv1v[c], den = g.cv2v[c] * g.rv1[c];
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) g.vn[comp][c] = (rvc * g.v[comp][c] * c1 + Fm[comp] - F[comp]) / den;
+}
+
+template <class R>
+__global__ void __launch_bounds__(128) k_mom_x(MomArgs<R> g) {
+  const int lane = (int)threadIdx.x;                        // blockDim.x == 32: one warp per row
+  const int ix = -1 + (int)blockIdx.x * 31 + lane;          // face / vertex x position
+  const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int iz = (int)blockIdx.z;
+  if (iy > g.ny) return;                                    // uniform over the warp
+  const R dt = (R)g.sc[g.dt_slot];
+  const int c = ix + g.sx * iy + g.sxy * iz;
+  R F[3] = {R(0), R(0), R(0)};
+  if (ix <= g.nx) mom_flux(g, c, iy, iz, dt, F);            // faces -1..n
+  R Fm[3];
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) Fm[comp] = __shfl_up_sync(0xffffffffu, F[comp], 1);
+  if (lane >= 1 && ix >= 0 && ix <= g.nx) mom_update(g, c, Fm, F);
+}
+
+template <class R>
+__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 6 : 8) k_mom_march(MomArgs<R> g) {
+  const int t0 = (int)(blockIdx.x * blockDim.x + threadIdx.x);  // x, 0..nx
+  const int t1 = (int)(blockIdx.y * blockDim.y + threadIdx.y);  // the third axis, 0..n3
+  if (t0 > g.nx || t1 > g.n3) return;
+  const int ia0 = (int)blockIdx.z * kMomA;
+  const int ia1 = min(ia0 + kMomA - 1, g.na);
+  const R dt = (R)g.sc[g.dt_slot];
+  const int SA = g.SA;
+  const R area = g.dct1(t0) * g.dct2(t1);
+  // stencil window of face ia0 - 1; each step shifts it by one and loads
+  // the new far point
+  int c = t0 + t1 * g.S3 + (ia0 - 1) * SA;
+  R w[3][4];
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[comp][q] = g.v[comp][c + (q - 1) * SA];
+  R va0 = g.va[c], va1 = g.va[c + SA], rvc = g.rv[c], rvn = g.rv[c + SA];
+  R dbw0 = g.db1[c], dbw1 = g.db1[c + SA], dbw2 = g.db1[c + 2 * SA], dcw0 = g.dc1[c], dcw1 = g.dc1[c + SA];
+  R Fm[3];
+  mom_flux_vals(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, Fm);
+  for (int ia = ia0; ia <= ia1; ++ia) {
+    c += SA;
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      w[comp][0] = w[comp][1];
+      w[comp][1] = w[comp][2];
+      w[comp][2] = w[comp][3];
+      w[comp][3] = g.v[comp][c + 2 * SA];
+    }
+    va0 = va1;
+    va1 = g.va[c + SA];
+    rvc = rvn;
+    rvn = g.rv[c + SA];
+    dbw0 = dbw1;
+    dbw1 = dbw2;
+    dbw2 = g.db1[c + 2 * SA];
+    dcw0 = dcw1;
+    dcw1 = g.dc1[c + SA];
+    R F[3];
+    mom_flux_vals(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, F);
+    // K9's update at c: fluxes at faces c - e_A and c
+    const R c1 = g.cv1v[c], den = g.cv2v[c] * g.rv1[c];
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      g.vn[comp][c] = (rvc * w[comp][1] * c1 + Fm[comp] - F[comp]) / den;
+      Fm[comp] = F[comp];
+    }
+  }
+}
+
 template <int A, class R>
 void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   constexpr int T1 = A == 0 ? 1 : 0, T2 = A == 2 ? 1 : 2;  // transverse axes, T1 < T2
@@ -719,64 +876,51 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     ++run.launches;
   }
 
-  // ---- K8: momentum fluxes at vertex faces a -1:n, transverse 0:n
-  R* const Vp[3] = {Ar.vx.p, Ar.vy.p, Ar.vz.p};
-  R* const vxp = Vp[0];
-  R* const vyp = Vp[1];
-  R* const vzp = Vp[2];
-  R* const mfx = Ar.mfx.p;
-  R* const mfy = Ar.mfy.p;
-  R* const mfz = Ar.mfz.p;
+  // ---- K8 + K9: momentum fluxes (faces a -1:n, transverse 0:n) and the
+  // velocity updates (0:n) in one kernel, new velocities into the q buffers
   {
-    int lo[3] = {0, 0, 0}, hi[3] = {nx, ny, nz};
-    lo[A] = -1;
-    hi[A] = na;
-    LARE_BOXWB(run, 6, 11, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
-      const R dt = (R)sc[dt_slot];
-      const int c = ix + sx * iy + sxy * iz;
-      const int pp[3] = {ix, iy, iz};
-      const int cm = c - SA, cp = c + SA, cp2 = c + 2 * SA;
-      R area = dct1(pp[T1]) * dct2(pp[T2]);
-      R v_advect = (va[c] + va[cp]) * R(0.5);  // the face-averaged v1 of xremap.f90:257-265
-      R rvc = rv[c], rvp = rv[cp], dmc = dmv[c];
-      const R* Vc[3] = {vxp, vyp, vzp};
-      R* Fo[3] = {mfx, mfy, mfz};
-      // The upwind choice, phi and dmu depend only on v_advect and the
-      // geometry, so they are formed once for the three components (the
-      // same expressions the limiter evaluates per component).
-      const R dxci = db1[cp], dxcm = db1[c], dxcp = db1[cp2], dxbi = dc1[c], dxbp = dc1[cp];
-      const R sign_v = copysign(R(1), v_advect);
-      const R vad_p = (sign_v + R(1)) * R(0.5);
-      const R vad_m = R(1) - vad_p;
-      const R dxcu = dxcm * vad_p + dxcp * vad_m;
-      const R dxbu = dxbi * vad_p + dxbp * vad_m;
-      const R phi = fabs(v_advect) * dt / dxbu;
-      const R rhou = rvc * vad_p + rvp * vad_m;
-      const R dmu = fabs(dmc) / area / dxbu / rhou;
-      for (int comp = 0; comp < 3; ++comp) {
-        const R* vc = Vc[comp];
-        const R fm = vc[cm], fi = vc[c], fp = vc[cp], fp2 = vc[cp2];
-        const R dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
-        const R fu = fi * vad_p + fp * vad_m;
-        const R dfu = dfm * vad_p + dfp * vad_m;
-        R Da = (R(2) - phi) * fabs(dfi) / dxci + (R(1) + phi) * fabs(dfu) / dxcu;
-        Da = Da * (R(1) / R(6));
-        const R ss = R(0.5) * (copysign(R(1), dfi) + copysign(R(1), dfu));
-        const R Di = sign_v * ss * fmin(fmin(fabs(Da) * dxbu, fabs(dfi)), fabs(dfu));
-        const R f = fu + Di * (R(1) - dmu);
-        Fo[comp][c] = f * dmc;
-      }
-    });
+    MomArgs<R> gm;
+    gm.va = va;
+    gm.rv = rv;
+    gm.dmv = dmv;
+    gm.db1 = db1;
+    gm.dc1 = dc1;
+    gm.v[0] = Ar.vx.p;
+    gm.v[1] = Ar.vy.p;
+    gm.v[2] = Ar.vz.p;
+    gm.vn[0] = Ar.qx.p;
+    gm.vn[1] = Ar.qy.p;
+    gm.vn[2] = Ar.qz.p;
+    gm.cv1v = cv1v;
+    gm.cv2v = cv2v;
+    gm.rv1 = rv1;
+    gm.dct1 = dct1;
+    gm.dct2 = dct2;
+    gm.sc = sc;
+    gm.dt_slot = dt_slot;
+    gm.nx = nx;
+    gm.ny = ny;
+    gm.nz = nz;
+    gm.na = na;
+    gm.n3 = A == 1 ? nz : ny;
+    gm.sx = sx;
+    gm.sxy = sxy;
+    gm.SA = SA;
+    gm.S3 = A == 1 ? sxy : sx;
+    const int k = run.prof_begin("remap_sweep_mom", A, 14, (double)(nx + 1) * (ny + 1) * (nz + 1));
+    if (A == 0) {
+      dim3 grd((nx + 1 + 30) / 31, (ny + 1 + 3) / 4, nz + 1);
+      k_mom_x<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gm);
+    } else {
+      dim3 grd((nx + 1 + 31) / 32, (gm.n3 + 1 + 3) / 4, (na + 1 + kMomA - 1) / kMomA);
+      k_mom_march<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gm);
+    }
+    run.prof_end(k);
+    ++run.launches;
   }
-
-  // ---- K9: velocity updates (0:n)
-  LARE_BOXW(run, 13, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
-    const int c = ix + sx * iy + sxy * iz;
-    R rvc = rv[c], c1 = cv1v[c], den = cv2v[c] * rv1[c];
-    vxp[c] = (rvc * vxp[c] * c1 + mfx[c - SA] - mfx[c]) / den;
-    vyp[c] = (rvc * vyp[c] * c1 + mfy[c - SA] - mfy[c]) / den;
-    vzp[c] = (rvc * vzp[c] * c1 + mfz[c - SA] - mfz[c]) / den;
-  });
+  std::swap(Ar.vx.p, Ar.qx.p);
+  std::swap(Ar.vy.p, Ar.qy.p);
+  std::swap(Ar.vz.p, Ar.qz.p);
 
   // The new density becomes rho; the old buffer is scratch again.
   std::swap(Ar.rho.p, Ar.rho_alt.p);
