@@ -381,7 +381,8 @@ def main():
     if os.path.exists(tpath):
         # measured DRAM bytes per launch, keyed by routine, word count and grid
         for t in json.load(open(tpath)):
-            if (t["routine"], t["words"], t["grid"]) == (top["site"].split(":")[0], top["words"], n):
+            if (t["routine"], t["words"], t["launches"], t["grid"]) == (top["site"].split(":")[0], top["words"],
+                                                                         top["launches"], n):
                 traffic = t["bytes_per_launch"]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": traffic, "kernel": top["site"], "share": top["ms"] / total_ms,
