@@ -639,8 +639,9 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   const bool write_cv2 = !predictor;
 
   // ---- K1: cv1, cv2, db1, dc1 over the whole cell box -1..n+2 (z-marching for the
-  // x and z sweeps; per cell for the y sweep, where the marching form measured slower)
-  if (A != 1) {
+  // z sweep and the FP64 x sweep; per cell for the y sweep and the FP32 x sweep,
+  // where the marching form measured slower)
+  if (A == 2 || (A == 0 && sizeof(R) == 8)) {
     GeomArgs<R> ga;
     ga.vx1 = vx1;
     ga.vy1 = Ar.vy1.p;
