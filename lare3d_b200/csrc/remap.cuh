@@ -50,6 +50,7 @@ __device__ __forceinline__ int acoord(int ix, int iy, int iz) {
 // flux instead of four.  Every value is the same expression of the same
 // operands as in the per-cell form, so the fluxes are identical bit for bit.
 constexpr int kMarch = 32;
+constexpr int kBUpdZ32 = 4, kBUpdZ64 = 1;  // z-points per thread of the B updates (measured)
 
 template <class R>
 struct BfArgs {
@@ -673,6 +674,66 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 6 : 8) k_mom_march(MomAr
   }
 }
 
+// K3 with kBUpdZ z-points per thread: every load of all the thread's
+// points is issued before any store (a point reads and writes B only at
+// itself), so each thread keeps several independent loads in flight; the
+// FP32 form, 4 bytes a word, is otherwise latency-bound well below HBM
+// speed.  Same expressions and predicates as the per-point form.
+template <class R>
+struct BUpdArgs {
+  const R* f1;
+  const R* f2;
+  R* Ba;
+  R* Bb1;
+  R* Bb2;
+  int nx, ny, nz, sx, sxy, SA, SB1, SB2;
+};
+
+template <int A, int PTS, class R>
+__global__ void __launch_bounds__(128) k_bupdate(BUpdArgs<R> g) {
+  const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  if (ix > g.nx + 1 || iy > g.ny + 1) return;
+  const int z0 = (int)blockIdx.z * PTS;
+  R b1[PTS], f1c[PTS], f1a[PTS], ba[PTS], f1b[PTS], b2[PTS], f2c[PTS], f2a[PTS], f2b[PTS];
+  bool ok[PTS];
+#pragma unroll
+  for (int p = 0; p < PTS; ++p) {
+    const int iz = z0 + p;
+    ok[p] = iz <= g.nz + 1;
+    const int c = ix + g.sx * iy + g.sxy * (ok[p] ? iz : z0);
+    b1[p] = g.Bb1[c];
+    f1c[p] = g.f1[c];
+    f1a[p] = g.f1[c - g.SA];
+    ba[p] = g.Ba[c];
+    f1b[p] = g.f1[c - g.SB1];
+    b2[p] = g.Bb2[c];
+    f2c[p] = g.f2[c];
+    f2a[p] = g.f2[c - g.SA];
+    f2b[p] = g.f2[c - g.SB2];
+  }
+#pragma unroll
+  for (int p = 0; p < PTS; ++p) {
+    if (!ok[p]) continue;
+    const int iz = z0 + p;
+    const int c = ix + g.sx * iy + g.sxy * iz;
+    // first flux: b1 over 0:n+1 all, a-component over 0:n+1 all
+    g.Bb1[c] = b1[p] - f1c[p] + f1a[p];
+    R b = ba[p] + f1c[p] - f1b[p];
+    // second flux ranges (xremap.f90:141-157; yremap.f90:142-158)
+    bool r2a = true, r2b = true;
+    if (A == 0) {
+      r2a = ix >= 1 && ix <= g.nx && iy >= 1 && iy <= g.ny && iz <= g.nz;
+      r2b = ix <= g.nx;
+    } else if (A == 1) {
+      r2b = ix >= 1 && ix <= g.nx && iy <= g.ny && iz >= 1 && iz <= g.nz;
+    }
+    if (r2a) g.Bb2[c] = b2[p] - f2c[p] + f2a[p];
+    if (r2b) b = b + f2c[p] - f2b[p];
+    g.Ba[c] = b;
+  }
+}
+
 template <int A, class R>
 void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   constexpr int T1 = A == 0 ? 1 : 0, T2 = A == 2 ? 1 : 2;  // transverse axes, T1 < T2
@@ -828,23 +889,26 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     R* const Ba = Bp[A];
     R* const Bb1 = Bp[B1];
     R* const Bb2 = Bp[B2];
-    LARE_BOXW(run, 8, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
-      const int c = ix + sx * iy + sxy * iz;
-      // first flux: b1 over 0:n+1 all, a-component over 0:n+1 all
-      Bb1[c] = Bb1[c] - f1[c] + f1[c - SA];
-      R ba = Ba[c] + f1[c] - f1[c - SB1];
-      // second flux ranges (xremap.f90:141-157; yremap.f90:142-158)
-      bool r2a = true, r2b = true;
-      if (A == 0) {
-        r2a = ix >= 1 && ix <= nx && iy >= 1 && iy <= ny && iz <= nz;
-        r2b = ix <= nx;
-      } else if (A == 1) {
-        r2b = ix >= 1 && ix <= nx && iy <= ny && iz >= 1 && iz <= nz;
-      }
-      if (r2a) Bb2[c] = Bb2[c] - f2[c] + f2[c - SA];
-      if (r2b) ba = ba + f2[c] - f2[c - SB2];
-      Ba[c] = ba;
-    });
+    BUpdArgs<R> gu;
+    gu.f1 = f1;
+    gu.f2 = f2;
+    gu.Ba = Ba;
+    gu.Bb1 = Bb1;
+    gu.Bb2 = Bb2;
+    gu.nx = nx;
+    gu.ny = ny;
+    gu.nz = nz;
+    gu.sx = sx;
+    gu.sxy = sxy;
+    gu.SA = SA;
+    gu.SB1 = SB1;
+    gu.SB2 = SB2;
+    constexpr int kPts = sizeof(R) == 4 ? kBUpdZ32 : kBUpdZ64;
+    dim3 grd((nx + 2 + 31) / 32, (ny + 2 + 3) / 4, (nz + 2 + kPts - 1) / kPts);
+    const int k = run.prof_begin("remap_sweep_bupd", A, 8, (double)(nx + 2) * (ny + 2) * (nz + 2));
+    k_bupdate<A, kPts, R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gu);
+    run.prof_end(k);
+    ++run.launches;
   }
   if (predictor) return;  // xremap.f90:159-162 (pass flag not reset)
 
