@@ -112,15 +112,37 @@ __global__ void __launch_bounds__(256, MINB) k_box_mb(int i0, int j0, int k0, in
 // Block shape bx x by (bx * by <= 256), chosen per context (the ensemble
 // autotuner sets it per grid size); every point runs the same arithmetic
 // whatever the shape.
-template <int MINB = 0, class Fn>
+// ZP > 1: each thread takes ZP consecutive planes (more independent loads
+// per thread; helps some FP32 kernels, whose 4-byte words leave few bytes
+// in flight).  The order in which points are computed does not matter: a
+// point kernel writes only its own point.
+template <int ZP, class Fn>
+__global__ void __launch_bounds__(256) k_box_z(int i0, int j0, int k0, int ni, int nj, int nk, Fn fn) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= ni || j >= nj) return;
+#pragma unroll
+  for (int p = 0; p < ZP; ++p) {
+    const int k = (int)blockIdx.z * ZP + p;
+    if (k < nk) fn(i0 + i, j0 + j, k0 + k);
+  }
+}
+
+template <int MINB = 0, int ZP = 1, class Fn>
 inline void launch_box(cudaStream_t s, long long& count, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn,
                        int bx = 64, int by = 4) {
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   if (ni <= 0 || nj <= 0 || nk <= 0) return;
   dim3 blk(bx, by, 1);
   dim3 grd((ni + bx - 1) / bx, (nj + by - 1) / by, nk);
-  if constexpr (MINB > 0) k_box_mb<MINB><<<grd, blk, 0, s>>>(i0, j0, k0, ni, nj, fn);
-  else k_box<<<grd, blk, 0, s>>>(i0, j0, k0, ni, nj, fn);
+  if constexpr (MINB > 0) {
+    k_box_mb<MINB><<<grd, blk, 0, s>>>(i0, j0, k0, ni, nj, fn);
+  } else if constexpr (ZP > 1) {
+    grd.z = (nk + ZP - 1) / ZP;
+    k_box_z<ZP><<<grd, blk, 0, s>>>(i0, j0, k0, ni, nj, nk, fn);
+  } else {
+    k_box<<<grd, blk, 0, s>>>(i0, j0, k0, ni, nj, fn);
+  }
   ++count;
 }
 

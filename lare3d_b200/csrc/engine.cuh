@@ -159,12 +159,12 @@ struct Run {
 
 // ---------------------------------------------------------------------
 // Launch shorthands
-template <int MINB64 = 0, class R, class Fn>
+template <int MINB64 = 0, int ZP32 = 1, class R, class Fn>
 inline void rbox(Run<R>& run, const char* func, int line, int words, int i0, int i1, int j0, int j1, int k0, int k1,
                  Fn fn) {
   double pts = (double)(i1 - i0 + 1) * (double)(j1 - j0 + 1) * (double)(k1 - k0 + 1);
   int k = run.prof_begin(func, line, words, pts);
-  launch_box<sizeof(R) == 8 ? MINB64 : 0>(run.s, run.launches, i0, i1, j0, j1, k0, k1, fn, run.blk_x, run.blk_y);
+  launch_box<sizeof(R) == 8 ? MINB64 : 0, sizeof(R) == 4 ? ZP32 : 1>(run.s, run.launches, i0, i1, j0, j1, k0, k1, fn, run.blk_x, run.blk_y);
   run.prof_end(k);
 }
 // LARE_BOX: one kernel over an inclusive Fortran index box.  LARE_BOXW also
@@ -179,6 +179,10 @@ inline void rbox(Run<R>& run, const char* func, int line, int words, int i0, int
   rbox((run), __func__, __LINE__, (words), (i0), (i1), (j0), (j1), (k0), (k1), __VA_ARGS__)
 #define LARE_BOXWB(run, minb, words, i0, i1, j0, j1, k0, k1, ...) \
   rbox<minb>((run), __func__, __LINE__, (words), (i0), (i1), (j0), (j1), (k0), (k1), __VA_ARGS__)
+// LARE_BOXWH: both hints, the FP64 occupancy hint and the FP32 planes per
+// thread (k_box_z's ZP), each measured per kernel at 256^3.
+#define LARE_BOXWH(run, minb64, zp32, words, i0, i1, j0, j1, k0, k1, ...) \
+  rbox<minb64, zp32>((run), __func__, __LINE__, (words), (i0), (i1), (j0), (j1), (k0), (k1), __VA_ARGS__)
 
 template <class R>
 inline void ghost(Run<R>& run, const GSpec& g, A3<R> a, A3<R>* b = nullptr, A3<R>* c = nullptr) {
@@ -586,7 +590,7 @@ void eulerian_remap(Run<R>& run, int step) {
   auto dxb = run.a.dxb, dyb = run.a.dyb, dzb = run.a.dzb;
   int pass[3] = {1, 1, 1};
   // B -> flux (remap.f90:43-69), including the -2 layers.
-  LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     if (iy >= -1 && iz >= -1) bx[c] = bx[c] * dyb(iy) * dzb(iz);
     if (ix >= -1 && iz >= -1) by[c] = by[c] * dxb(ix) * dzb(iz);
@@ -606,7 +610,7 @@ void eulerian_remap(Run<R>& run, int step) {
   R* const qy = run.a.by.p;
   R* const qz = run.a.bz.p;
   const auto rbx = run.a.rdb[0], rby = run.a.rdb[1], rbz = run.a.rdb[2];
-  LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     if (iy >= -1 && iz >= -1) qx[c] = div_rcp(div_rcp(qx[c], dyb(iy), rby(iy)), dzb(iz), rbz(iz));
     if (ix >= -1 && iz >= -1) qy[c] = div_rcp(div_rcp(qy[c], dxb(ix), rbx(ix)), dzb(iz), rbz(iz));

@@ -199,7 +199,7 @@ void resistive_update(Run<R>& run) {
   auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb, dxc = A.dxc, dyc = A.dyc, dzc = A.dzc;
   const double* sc = run.sc;
   // RS2: bstep (:1588-1631) into the second buffers
-  LARE_BOXWB(run, 4, 9, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 4, 4, 9, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DTSUB];
     const int c = ix + sx * iy + sxy * iz;
     if (iy >= 1 && iz >= 1) {
@@ -278,7 +278,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
   R* const p_visc = A.p_visc.p;
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
   // LP1
-  LARE_BOXW(run, 11, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 0, 4, 11, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     R bx1 = (bx[c] + bx[c - 1]) * R(0.5);
     R by1 = (by[c] + by[c - sx]) * R(0.5);
@@ -305,7 +305,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
   if (run.p.use_viscous_damping) viscous_damping(run);
   // LP2: cs_v (:561-581)
   R* const cs_v = A.cs_v.p;
-  LARE_BOXW(run, 4, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 0, 4, 4, -1, nx + 1, -1, ny + 1, -1, nz + 1, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     const int o1 = 1, o2 = sx, o3 = 1 + sx, o4 = sxy, o5 = 1 + sxy, o6 = sx + sxy, o7 = 1 + sx + sxy;
     R s = cs[c] * cv[c] + cs[c + o1] * cv[c + o1] + cs[c + o2] * cv[c + o2] + cs[c + o3] * cv[c + o3] +
@@ -323,7 +323,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
   auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb, dxc = A.dxc, dyc = A.dyc, dzc = A.dzc;
   const R visc1 = (R)run.p.visc1;
   const double* sc = run.sc;
-  LARE_BOXWB(run, 4, 8, -1, nx + 1, -1, ny + 2, 0, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 4, 2, 8, -1, nx + 1, -1, ny + 2, 0, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const R dt = (R)sc[SC_DT], v2n = (R)sc[SC_VISC2N];
     const int c = ix + sx * iy + sxy * iz;
     auto edge = [&](const R* vcomp, int i1, int i2, R dx) {
@@ -513,7 +513,7 @@ void predictor_remap(Run<R>& run, int step) {
   R* const py = A.by0.p;
   R* const pz = A.bz0.p;
   auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb;
-  LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     if (iy >= -1 && iz >= -1) px[c] = bx[c] * dyb(iy) * dzb(iz);
     if (ix >= -1 && iz >= -1) py[c] = by[c] * dxb(ix) * dzb(iz);
@@ -544,7 +544,7 @@ void predictor_remap(Run<R>& run, int step) {
   R* const qy = A.by.p;
   R* const qz = A.bz.p;
   const auto rbx = run.a.rdb[0], rby = run.a.rdb[1], rbz = run.a.rdb[2];
-  LARE_BOXW(run, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     if (iy >= -1 && iz >= -1) qx[c] = div_rcp(div_rcp(qx[c], dyb(iy), rby(iy)), dzb(iz), rbz(iz));
     if (ix >= -1 && iz >= -1) qy[c] = div_rcp(div_rcp(qy[c], dxb(ix), rbx(ix)), dzb(iz), rbz(iz));
@@ -666,7 +666,7 @@ void predictor_corrector_step(Run<R>& run) {
   const bool cond = run.p.conduction != 0;
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
   const double* sc = run.sc;
-  LARE_BOXW(run, 8, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 0, 4, 8, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     R e;
     if (cond) {
@@ -703,7 +703,7 @@ void predictor_corrector_step(Run<R>& run) {
   const R* fzv = A.fz_visc.p;
   auto dxc = A.dxc, dyc = A.dyc, dzc = A.dzc, grav = A.grav;
   auto rdcx = A.rdc[0], rdcy = A.rdc[1], rdcz = A.rdc[2];
-  LARE_BOXWB(run, 5, 17, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 5, 4, 17, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     const R dt2 = (R)sc[SC_DT2];
     const int c = ix + sx * iy + sxy * iz;
     const int X = 1, Y = sx, Z = sxy;

@@ -921,7 +921,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   const int nt1 = nn[T1], nt2 = nn[T2];
 
   // ---- K4: mass flux with dm_[xyz]_bcs over the whole cell box
-  LARE_BOXW(run, 5, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 0, 2, 5, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     const int pp[3] = {ix, iy, iz};
     const int ia = pp[A], i1 = pp[T1], i2 = pp[T2];
@@ -953,7 +953,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   });
 
   // ---- K5: new rho (second buffer) and the energy flux (0:n)
-  LARE_BOXWB(run, 6, 10, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 6, 4, 10, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     const bool in0 = ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz;
     const bool in1 = ix >= 1 && iy >= 1 && iz >= 1 && in0;
@@ -974,7 +974,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   });
 
   // ---- K6: energy update (1:n)
-  LARE_BOXW(run, 7, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWH(run, 0, 2, 7, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     energy[c] = (energy[c] * cv1[c] * rho[c] + eflux[c - SA] - eflux[c]) / (cv2[c] * rho_new[c]);
   });
