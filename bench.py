@@ -384,9 +384,13 @@ def main():
             if (t["routine"], t["words"], t["launches"], t["grid"]) == (top["site"].split(":")[0], top["words"],
                                                                          top["launches"], n):
                 traffic = t["bytes_per_launch"]
+    # the whole step as well: algorithmic bytes of every profiled launch over their summed time
+    step_bytes = sum(p["bytes"] for p in prof)
+    step_gbs = step_bytes / (total_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": traffic, "kernel": top["site"], "share": top["ms"] / total_ms,
-                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": per_launch_bytes}
+                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": per_launch_bytes,
+                "step_achieved": step_gbs, "step_frac": step_gbs / hbm}
 
     # ---- end to end through the C ABI with pinned host buffers
     host = {}

@@ -76,7 +76,7 @@ struct Prof {
   size_t used = 0;
   std::vector<int> ev_site;          // per event pair
   std::vector<double> ev_bytes;
-  std::map<std::pair<const char*, int>, int> index;
+  std::map<std::pair<std::string, int>, int> index;  // by name and line (the same name in several template instances is one site)
   std::vector<ProfSite> sites;
 };
 
@@ -110,7 +110,7 @@ struct Run {
   // Bracket one launch with events when profiling.
   int prof_begin(const char* func, int line, int words, double points) {
     if (!prof.on) return -1;
-    auto key = std::make_pair(func, line);
+    auto key = std::make_pair(std::string(func), line);
     auto it = prof.index.find(key);
     int site;
     if (it == prof.index.end()) {

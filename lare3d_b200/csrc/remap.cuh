@@ -800,7 +800,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     ga.write_cv2 = write_cv2;
     dim3 blk(32, 4, 1);
     dim3 grd((nx + 4 + 31) / 32, (ny + 4 + 3) / 4, (nz + 4 + kGeomZ - 1) / kGeomZ);
-    const int k = run.prof_begin("remap_sweep_geom", A, 8, (double)(nx + 4) * (ny + 4) * (nz + 4));
+    const int k = run.prof_begin("remap_sweep_geom_march", 0, 8, (double)(nx + 4) * (ny + 4) * (nz + 4));
     k_geom_march<A, R><<<grd, blk, 0, run.s>>>(ga);
     run.prof_end(k);
     ++run.launches;
@@ -865,7 +865,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     ba.na = na;
     ba.n0 = nx + 3;
     ba.n1 = (A == 1 ? nz : ny) + 3;
-    const int k = run.prof_begin("remap_sweep_bflux", A, 7, (double)(nx + 3) * (ny + 3) * (nz + 3));
+    const int k = run.prof_begin(A == 0 ? "remap_sweep_bflux_x" : "remap_sweep_bflux_march", 0, 7, (double)(nx + 3) * (ny + 3) * (nz + 3));
     if (A != 0) {
       dim3 blk(32, 4, 1);
       dim3 grd((ba.n0 + 31) / 32, (ba.n1 + 3) / 4, (na + 3 + kMarch - 1) / kMarch);
@@ -905,7 +905,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     gu.SB2 = SB2;
     constexpr int kPts = sizeof(R) == 4 ? kBUpdZ32 : kBUpdZ64;
     dim3 grd((nx + 2 + 31) / 32, (ny + 2 + 3) / 4, (nz + 2 + kPts - 1) / kPts);
-    const int k = run.prof_begin("remap_sweep_bupd", A, 8, (double)(nx + 2) * (ny + 2) * (nz + 2));
+    const int k = run.prof_begin("remap_sweep_bupd", 0, 8, (double)(nx + 2) * (ny + 2) * (nz + 2));
     k_bupdate<A, kPts, R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gu);
     run.prof_end(k);
     ++run.launches;
@@ -1009,7 +1009,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     va7.sxy = sxy;
     dim3 blk(32, 4, 1);
     dim3 grd((hi[0] - lo[0] + 32) / 32, (hi[1] - lo[1] + 4) / 4, (hi[2] - lo[2] + kVertZ) / kVertZ);
-    const int k = run.prof_begin("remap_sweep_vert", A, 9,
+    const int k = run.prof_begin("remap_sweep_vert", 0, 9,
                                  (double)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1));
     k_vert_march<A, R><<<grd, blk, 0, run.s>>>(va7);
     run.prof_end(k);
@@ -1047,7 +1047,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     gm.sxy = sxy;
     gm.SA = SA;
     gm.S3 = A == 1 ? sxy : sx;
-    const int k = run.prof_begin("remap_sweep_mom", A, 14, (double)(nx + 1) * (ny + 1) * (nz + 1));
+    const int k = run.prof_begin(A == 0 ? "remap_sweep_mom_x" : "remap_sweep_mom_march", 0, 14, (double)(nx + 1) * (ny + 1) * (nz + 1));
     if (A == 0) {
       dim3 grd((nx + 1 + 30) / 31, (ny + 1 + 3) / 4, nz + 1);
       k_mom_x<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gm);
