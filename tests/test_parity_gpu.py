@@ -96,6 +96,57 @@ def test_ragged_grid_bitwise(built):
         assert_bitwise(g, r, STATE, f"step {s}")
 
 
+def _ragged_resistive_deck(nx, ny, nz, seed):
+    from lare3d_b200.abi import State
+    from lare3d_b200.grid import grid
+    d = decks.orszag_tang(8, j_max=10.0, eta0=1.0e-3)
+    m = grid(nx, ny, nz, (0, 1.1), (0, 0.9), (0, 1.6))
+    st = State.zeros(nx, ny, nz)
+    rng = np.random.default_rng(seed)
+    for k in STATE:
+        st[k][...] = rng.uniform(0.5, 1.5, st[k].shape) if k in ("rho", "energy") else rng.uniform(-0.3, 0.3, st[k].shape)
+    return decks.Deck("ragged-resistive", d.params, nx, ny, nz, m, st, nsteps=3)
+
+
+def test_partial_chunks_bitwise(built):
+    """Edges that are not multiples of any kernel's chunk (32 and 64 planes
+    marched per thread, 29 and 31 outputs per warp, 4 planes per thread),
+    with the resistive path on and j_max inside the current range, so both
+    eta branches occur: every routine bit for bit."""
+    d = _ragged_resistive_deck(45, 38, 67, 11)
+    r, g = pair(d)
+    for s in range(1, 4):
+        r.lagrangian_step(s)
+        g.lagrangian_step(s)
+        assert_bitwise(g, r, STATE + INTERMEDIATE, f"lagrangian_step {s}")
+        r.eulerian_remap(s)
+        g.eulerian_remap(s)
+        assert_bitwise(g, r, STATE, f"eulerian_remap {s}")
+        r.eta_calc()
+        g.eta_calc()
+        assert_bitwise(g, r, ["eta"], f"eta_calc {s}")
+    eta = g.get_field("eta")
+    assert (eta > 1.5e-3).any() and (eta < 1.5e-3).any()
+
+
+def test_partial_chunks_fp32(built):
+    """The FP32 form on the same grid (its own kernel choices and planes per
+    thread) against the FP64 oracle at the 1e-5 bar."""
+    d = _ragged_resistive_deck(45, 38, 67, 12)
+    from lare3d_b200 import gpu
+    from oracle import oracle
+    r = oracle.simulation(d)
+    g = gpu.simulation(d, precision=32)
+    r.start(d.state)
+    g.start(d.state)
+    for s in range(1, 4):
+        r.step(s)
+        g.step(s)
+    for f in STATE:
+        e = rel_l2(g.get_field(f), r.get_field(f))
+        assert e <= 1e-5, f"{f}: rel L2 {e:.2e}"
+
+
 @pytest.mark.slow
 def test_blast_64_100_steps(built):
     """Blast at 64^3, 100 steps at CFL 0.8: relative L2 per field <= 1e-10
