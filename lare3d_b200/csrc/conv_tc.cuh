@@ -15,8 +15,10 @@
 // buffer with a different start address.  The weights stay resident as
 // [tap][channel group][cout][8].  One elected thread issues
 // T x 27 x (CIN/16) MMAs of 128 x N x 16 (N = output channels) into T
-// accumulator tiles in tensor memory, commits them to an mbarrier, and the
-// four warps read their 32 lanes back (tcgen05.ld), add the bias, apply the
+// accumulator tiles in tensor memory, commits them to an mbarrier, and
+// eight warps (two per 32-lane quadrant of tensor memory, each for half of
+// the output channels) read the accumulators back (tcgen05.ld), add the
+// bias (held in registers), apply the
 // ReLU or the mask and store bf16 or FP32.  Padding (pad = 2, the
 // backward-data convolution) comes from the zero fill of the staging.
 //
@@ -30,7 +32,8 @@
 namespace {
 
 constexpr int kTcT = 4;           // accumulator tiles (128 rows each) per work item
-constexpr int kTcThreads = 128;
+constexpr int kTcThreads = 128;   // k_conv_tc_c1
+constexpr int kTcEpiThreads = 256; // k_conv_tc: two warps per tensor-memory lane quadrant in the epilogue
 constexpr int kErrWait = 1;
 
 __device__ int g_sur_status = 0;  // sticky error word of the tensor-core kernels
@@ -109,6 +112,17 @@ __device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float (&v)[16]) {
 }
 
 template <>
+__device__ __forceinline__ void tmem_ld<8>(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+template <>
 __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float (&v)[32]) {
   float a[16], b[16];
   tmem_ld<16>(taddr, a);
@@ -149,7 +163,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
 // CIN input channels, NTC = MMA N (output channels computed), COUT = output
 // channels stored.
 template <int CIN, int NTC, int COUT>
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(kTcEpiThreads, 1)
     k_conv_tc(const __grid_constant__ CUtensorMap xmap, const __nv_bfloat16* __restrict__ w,
               const float* __restrict__ bias, void* __restrict__ y, const __nv_bfloat16* __restrict__ mask,
               TcGeom g, int relu, int out_f32) {
@@ -166,9 +180,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int SS = g.SS, D = g.D;
+  constexpr int HALF = NTC / 2;                 // output channels per epilogue warp
+  const int quad = warp & 3;                    // tensor-memory lane quadrant of this warp
+  const int HC0 = (warp >> 2) * HALF;           // its first output channel
+  float bv[HALF];
+#pragma unroll
+  for (int c = 0; c < HALF; ++c) bv[c] = (bias && HC0 + c < COUT) ? bias[HC0 + c] : 0.f;
 
   // weights: global [27][COUT][CIN] -> shared [27][KG][NTC][8] (rows >= COUT zero)
-  for (int q = tid; q < 27 * KG * NTC; q += kTcThreads) {
+  for (int q = tid; q < 27 * KG * NTC; q += kTcEpiThreads) {
     const int co = q % NTC, kg = (q / NTC) % KG, tap = q / (NTC * KG);
     const __nv_bfloat16* src = w + ((long long)tap * COUT + (co < COUT ? co : 0)) * CIN + kg * 8;
     cp_async16(smem_u32(sw + (size_t)q * 16), src, co < COUT ? 16u : 0u);
@@ -204,6 +224,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         timed_out = true;
         break;
       }
+      __nanosleep(32);  // leave the issue slots to the thread that issues the MMAs
     }
     ph ^= 1u;
     return __syncthreads_or(timed_out) != 0;
@@ -258,40 +279,44 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // item's accumulators drain
     const long long nxt = it + gridDim.x;
     if (tid == 0 && nxt < items) stage(nxt);
-    // epilogue: warp w owns accumulator rows 32w..32w+31 of every tile
+    // epilogue: warps w and w+4 own accumulator rows 32(w%4)..32(w%4)+31 of
+    // every tile, each for half of the output channels
 #pragma unroll 1
     for (int t = 0; t < kTcT; ++t) {
-      float v[NTC];
-      tmem_ld<NTC>(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(t * NTC), v);
-      const int r = r0 + t * 128 + 32 * warp + lane;
+      if (HC0 >= COUT) break;
+      float v[HALF];
+      tmem_ld<HALF>(tbase + ((uint32_t)(32 * quad) << 16) + (uint32_t)(t * NTC + HC0), v);
+      const int r = r0 + t * 128 + 32 * quad + lane;
       const int oy = r / D, ox = r - (r / D) * D;
       if (oy < g.E && oy < y0 + g.NY && ox < g.E) {
         const long long o = (((long long)b * g.E + oz) * g.E + oy) * g.E + ox;
         if (out_f32) {
-          float* yo = reinterpret_cast<float*>(y) + o * COUT;
+          float* yo = reinterpret_cast<float*>(y) + o * COUT + HC0;
 #pragma unroll
-          for (int c = 0; c < COUT; ++c) {
-            float a = v[c] + (bias ? bias[c] : 0.f);
+          for (int c = 0; c < HALF; ++c) {
+            if (HC0 + c >= COUT) break;
+            float a = v[c] + bv[c];
             if (relu) a = fmaxf(a, 0.f);
             yo[c] = a;
           }
         } else {
-          __nv_bfloat16* yo = reinterpret_cast<__nv_bfloat16*>(y) + o * COUT;
+          __nv_bfloat16* yo = reinterpret_cast<__nv_bfloat16*>(y) + o * COUT + HC0;
 #pragma unroll
-          for (int c = 0; c < COUT; c += 8) {
+          for (int c = 0; c < HALF; c += 8) {
+            if (HC0 + c >= COUT) break;
             float a[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              a[j] = v[c + j] + (bias ? bias[c + j] : 0.f);
-              if (relu) a[j] = fmaxf(a[j], 0.f);
+            for (int jj = 0; jj < 8; ++jj) {
+              a[jj] = v[c + jj] + bv[c + jj];
+              if (relu) a[jj] = fmaxf(a[jj], 0.f);
             }
             if (mask) {
-              const uint4 mk = *reinterpret_cast<const uint4*>(mask + o * COUT + c);
+              const uint4 mk = *reinterpret_cast<const uint4*>(mask + o * COUT + HC0 + c);
               const uint32_t mw[4] = {mk.x, mk.y, mk.z, mk.w};
 #pragma unroll
-              for (int j = 0; j < 8; ++j) {
-                const unsigned short h = (unsigned short)((mw[j >> 1] >> (16 * (j & 1))) & 0xffffu);
-                if (!(__bfloat162float(__ushort_as_bfloat16(h)) > 0.f)) a[j] = 0.f;
+              for (int jj = 0; jj < 8; ++jj) {
+                const unsigned short h = (unsigned short)((mw[jj >> 1] >> (16 * (jj & 1))) & 0xffffu);
+                if (!(__bfloat162float(__ushort_as_bfloat16(h)) > 0.f)) a[jj] = 0.f;
               }
             }
             uint4 o4;

@@ -234,7 +234,7 @@ int launch_conv_tc(const void* x, int din, int pad, const void* w, const float* 
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long long items = (long long)nb * g.E * g.ntg;
   const unsigned blocks = (unsigned)(items < sms ? items : sms);
-  k_conv_tc<CIN, NTC, COUT><<<blocks, kTcThreads, smem, s>>>(xmap, (const bf16*)w, bias, y, (const bf16*)mask, g,
+  k_conv_tc<CIN, NTC, COUT><<<blocks, kTcEpiThreads, smem, s>>>(xmap, (const bf16*)w, bias, y, (const bf16*)mask, g,
                                                              relu, out_f32);
   return cudaGetLastError() == cudaSuccess ? LARE_OK : LARE_ECUDA;
 }
