@@ -29,6 +29,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from lare3d_b200 import replicas  # noqa: E402  (process-group plumbing; no torch import at module load)
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -36,7 +38,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--n", "--edge", dest="n", type=int, default=256)  # --edge: the spelling torchrun passes through
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
@@ -107,26 +109,15 @@ class Clocks:
 
 
 def dist_setup(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    return replicas.env()
 
 
 def max_over_ranks(v, ws):
-    if ws == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(v, ws, "cuda")
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    replicas.barrier(ws)
 
 
 def cpu_baseline(deck, steps=1):
@@ -333,10 +324,7 @@ def main():
     import numpy as np
     import torch
     torch.cuda.set_device(local)
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    replicas.init(ws, "nccl")
 
     from lare3d_b200 import decks, gpu
     from lare3d_b200.abi import State
@@ -361,7 +349,7 @@ def main():
     ck = clocks.stop()
     el_max = max_over_ranks(el, ws)
     n3 = n ** 3
-    value = ws * n3 * args.steps / el_max
+    value = replicas.whole_job_rate(ws, n3 * args.steps, el_max)
 
     # ---- roofline of the dominant kernel (one profiled step)
     sim.profile(True)
@@ -415,7 +403,7 @@ def main():
     e1.record(stream)
     e1.synchronize()
     e2e_el = max_over_ranks(e0.elapsed_time(e1) / 1000.0, ws)
-    e2e = {"value": ws * n3 * args.e2e_steps / e2e_el, "unit": "cell-updates/s",
+    e2e = {"value": replicas.whole_job_rate(ws, n3 * args.e2e_steps, e2e_el), "unit": "cell-updates/s",
            "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bi, "steps": args.e2e_steps}
 
     # ---- the other forms (FP32, RKL2 conduction), rank 0 only
@@ -475,10 +463,8 @@ def main():
         }
         print(json.dumps(line), flush=True)
     sim.close()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        dist.destroy_process_group()
+    barrier(ws)
+    replicas.finish(ws)
 
 
 if __name__ == "__main__":
