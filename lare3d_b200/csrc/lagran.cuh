@@ -81,6 +81,16 @@ struct EtaArgs {
 
 template <class R>
 __global__ void __launch_bounds__(128) k_eta_march(EtaArgs<R> g) {
+  // distinct arrays (no output is an input): restrict lets the compiler
+  // hoist the next plane's loads above this plane's stores
+  const R* __restrict__ bx_r = g.bx;
+  const R* __restrict__ by_r = g.by;
+  const R* __restrict__ bz_r = g.bz;
+  R* __restrict__ eta_r = g.eta;
+  R* __restrict__ fx_r = g.fx;
+  R* __restrict__ fy_r = g.fy;
+  R* __restrict__ fz_r = g.fz;
+  R* __restrict__ curlb_r = g.curlb;
   const int ix = -1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = -1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
@@ -90,13 +100,13 @@ __global__ void __launch_bounds__(128) k_eta_march(EtaArgs<R> g) {
   const R dxc = g.dxc(ix), dyc = g.dyc(iy);
   int c = ix + sx * iy + sxy * z0;
   // plane z0 values of bx (c, c+Y) and by (c, c+X), and the jz1 quotients
-  R bx0 = g.bx[c], bxy = g.bx[c + sx], by0 = g.by[c], byx = g.by[c + 1];
+  R bx0 = bx_r[c], bxy = bx_r[c + sx], by0 = by_r[c], byx = by_r[c + 1];
   R qa = (byx - by0) / dxc, qb = (bxy - bx0) / dyc;
   const bool inxy = ix >= 0 && ix <= g.nx && iy >= 0 && iy <= g.ny;
   for (int iz = z0; iz <= z1; ++iz, c += sxy) {
     const R dzc = g.dzc(iz);
-    const R bz0 = g.bz[c], bzx = g.bz[c + 1], bzy = g.bz[c + sx], bzxy = g.bz[c + 1 + sx];
-    const R bxz = g.bx[c + sxy], bxyz = g.bx[c + sx + sxy], byz = g.by[c + sxy], byxz = g.by[c + 1 + sxy];
+    const R bz0 = bz_r[c], bzx = bz_r[c + 1], bzy = bz_r[c + sx], bzxy = bz_r[c + 1 + sx];
+    const R bxz = bx_r[c + sxy], bxyz = bx_r[c + sx + sxy], byz = by_r[c + sxy], byxz = by_r[c + 1 + sxy];
     const R jx1 = (bzy - bz0) / dyc - (byz - by0) / dzc;
     const R jx2 = (bzxy - bzx) / dyc - (byxz - byx) / dzc;
     const R jy1 = (bxz - bx0) / dzc - (bzx - bz0) / dxc;
@@ -109,12 +119,12 @@ __global__ void __launch_bounds__(128) k_eta_march(EtaArgs<R> g) {
     const R jz = (jz1 + jz2) * R(0.5);
     const R j2 = jx * jx + jy * jy + jz * jz;
     const R e = sqrt(j2) > g.jmax ? g.eb + g.e0 : g.eb;
-    g.eta[c] = e;
+    eta_r[c] = e;
     if (g.rkstep && inxy && iz >= 0 && iz <= g.nz) {
-      g.fx[c] = -jx * e * dxc * R(0.5);
-      g.fy[c] = -jy * e * dyc * R(0.5);
-      g.fz[c] = -jz * e * dzc * R(0.5);
-      g.curlb[c] = e * j2;
+      fx_r[c] = -jx * e * dxc * R(0.5);
+      fy_r[c] = -jy * e * dyc * R(0.5);
+      fz_r[c] = -jz * e * dzc * R(0.5);
+      curlb_r[c] = e * j2;
     }
     bx0 = bxz;
     bxy = bxyz;
@@ -579,6 +589,13 @@ struct ShockArgs {
 
 template <class R>
 __global__ void __launch_bounds__(128) k_shock_march(ShockArgs<R> g) {
+  // distinct arrays (no output is an input): restrict lets the compiler
+  // hoist the next plane's loads above this plane's stores
+  const R* __restrict__ alpha1_r = g.alpha1;
+  const R* __restrict__ alpha2_r = g.alpha2;
+  const R* __restrict__ alpha3_r = g.alpha3;
+  const R* __restrict__ cv_r = g.cv;
+  R* __restrict__ vhp_r = g.vhp;
   const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y);
   if (ix > g.nx + 1 || iy > g.ny + 1) return;
@@ -600,7 +617,7 @@ __global__ void __launch_bounds__(128) k_shock_march(ShockArgs<R> g) {
   };
   // plane z0-1 edges: a1 = (c-X-Y-Z, c-Y-Z), a2 = (c-Y-Z, c-Z), a3 = (c-Z, c-X-Z), a4 = (c-X-Z, c-X-Y-Z)
   R a1 = dd(lo, 3, lo, 2), a2 = dd(lo, 2, lo, 0), a3 = dd(lo, 0, lo, 1), a4 = dd(lo, 1, lo, 3);
-  R al1 = g.alpha1[c], al1y = g.alpha1[c + Y], al2 = g.alpha2[c], al2x = g.alpha2[c - X];
+  R al1 = alpha1_r[c], al1y = alpha1_r[c + Y], al2 = alpha2_r[c], al2x = alpha2_r[c - X];
   const R ddx = g.dxb(ix), ddy = g.dyb(iy);
   for (int iz = z0; iz <= z1; ++iz, c += sxy) {
     R up[6][4];
@@ -616,17 +633,17 @@ __global__ void __launch_bounds__(128) k_shock_march(ShockArgs<R> g) {
     const R a10 = dd(lo, 1, up, 1);  // (c-X-Z, c-X)
     const R a11 = dd(lo, 3, up, 3);  // (c-X-Y-Z, c-X-Y)
     const R a12 = dd(lo, 2, up, 2);  // (c-Y-Z, c-Y)
-    const R al1z = g.alpha1[c + sxy], al1yz = g.alpha1[c + Y + sxy];
-    const R al2z = g.alpha2[c + sxy], al2xz = g.alpha2[c - X + sxy];
+    const R al1z = alpha1_r[c + sxy], al1yz = alpha1_r[c + Y + sxy];
+    const R al2z = alpha2_r[c + sxy], al2xz = alpha2_r[c - X + sxy];
     const R ddz = g.dzb(iz);
     R vh = -R(0.25) * ddy * ddz * al1 * a1 - R(0.25) * ddx * ddz * al2 * a2 -
            R(0.25) * ddy * ddz * al1y * a3 - R(0.25) * ddx * ddz * al2x * a4 -
            R(0.25) * ddy * ddz * al1z * a5 - R(0.25) * ddx * ddz * al2z * a6 -
            R(0.25) * ddy * ddz * al1yz * a7 - R(0.25) * ddx * ddz * al2xz * a8 -
-           R(0.25) * ddx * ddy * g.alpha3[c] * a9 - R(0.25) * ddx * ddy * g.alpha3[c - X] * a10 -
-           R(0.25) * ddx * ddy * g.alpha3[c - X - Y] * a11 - R(0.25) * ddx * ddy * g.alpha3[c - Y] * a12;
-    R v = vh / g.cv[c];
-    g.vhp[c] = v > R(0) ? v : R(0);
+           R(0.25) * ddx * ddy * alpha3_r[c] * a9 - R(0.25) * ddx * ddy * alpha3_r[c - X] * a10 -
+           R(0.25) * ddx * ddy * alpha3_r[c - X - Y] * a11 - R(0.25) * ddx * ddy * alpha3_r[c - Y] * a12;
+    R v = vh / cv_r[c];
+    vhp_r[c] = v > R(0) ? v : R(0);
     if (ix <= g.nx && iy <= g.ny && iz <= g.nz) {
 #pragma unroll
       for (int k = 0; k < 3; ++k) g.nv[k][c] = R(2) * up[k + 3][0] - up[k][0];

@@ -306,6 +306,16 @@ struct GeomArgs {
 
 template <int A, class R>
 __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
+  // distinct arrays (no output is an input): restrict lets the compiler
+  // hoist the next plane's loads above this plane's stores
+  const R* __restrict__ vx1_r = g.vx1;
+  const R* __restrict__ vy1_r = g.vy1;
+  const R* __restrict__ vz1_r = g.vz1;
+  const R* __restrict__ cv_r = g.cv;
+  R* __restrict__ cv1_r = g.cv1;
+  R* __restrict__ cv2_r = g.cv2;
+  R* __restrict__ db1_r = g.db1;
+  R* __restrict__ dc1_r = g.dc1;
   constexpr int T1 = A == 0 ? 1 : 0, T2 = A == 2 ? 1 : 2;
   const int ix = -1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int iy = -1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
@@ -316,9 +326,9 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
   const int nn[3] = {g.nx, g.ny, g.nz};
   const R q4 = R(0.25);
   const R dt = (R)g.sc[g.dt_slot];
-  const R* vx1 = g.vx1;
-  const R* vy1 = g.vy1;
-  const R* vz1 = g.vz1;
+  const R* __restrict__ vx1 = vx1_r;
+  const R* __restrict__ vy1 = vy1_r;
+  const R* __restrict__ vz1 = vz1_r;
   constexpr int NX = A == 0 ? 3 : 2;  // x faces: c - 1, c (, c + 1)
   constexpr int NY = A == 1 ? 3 : 2;  // y faces: c - sx, c (, c + sx)
   const bool ahead = (A == 0 ? ix : iy) < nn[A] + 2;  // a face beyond c along A exists (A = 0, 1)
@@ -377,21 +387,21 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
     const R term_t2 = quot(g.pass_t2 * dvv[T2], T2);
     const R term_a = quot(dvv[A], A);
     R dv = (term_t1 + term_t2 + term_a) * dt;
-    const R cvc = g.cv[c];
-    g.cv1[c] = cvc * (R(1) + dv);
+    const R cvc = cv_r[c];
+    cv1_r[c] = cvc * (R(1) + dv);
     if (g.write_cv2) {
       dv = (term_t1 + term_t2) * dt;
-      g.cv2[c] = cvc * (R(1) + dv);
+      cv2_r[c] = cvc * (R(1) + dv);
     }
     const R d0 = g.dbm[A](pp[A]) + dvv[A] * dt;
-    g.db1[c] = d0;
+    db1_r[c] = d0;
     R d1 = d0;
     if (pp[A] < nn[A] + 2) {
       const R f = A == 0 ? vxfc[NX - 1] : (A == 1 ? vyfc[NY - 1] : vz_next);
       const R fa = A == 0 ? vxb : (A == 1 ? vyb : vzb);
       d1 = g.dbm[A](pp[A] + 1) + (f - fa) * dt;
     }
-    g.dc1[c] = R(0.5) * (d0 + d1);
+    dc1_r[c] = R(0.5) * (d0 + d1);
     vz_prev = vz_cur;
     vz_cur = A == 2 ? vz_next : (iz < z1 ? vzf(c + sxy) : R(0));
   }
