@@ -34,7 +34,12 @@
 extern "C" {
 #endif
 
-/* Boundary codes, shared_data.F90:65-66. */
+/*
+ * Boundary codes, shared_data.F90:65-66.  A direction is periodic only when
+ * both its sides are (else LARE_EINVAL at init).  BC_OPEN sides get the
+ * characteristic boundaries of openboundary.f90 once per step; their second
+ * ghost layer (as uploaded) is the far field and is never overwritten.
+ */
 #define LARE_BC_PERIODIC 1
 #define LARE_BC_USER 2
 #define LARE_BC_OPEN 3

@@ -98,6 +98,7 @@ struct Run {
   bool visc2_norm_set = false;      // lagran.F90:539 first_call (SAVE)
   bool set_dt_first = true;         // lagran.F90:1078 first (SAVE)
   bool gamma_boris_one = true;      // gamma_boris holds 1 everywhere
+  bool any_open = false;            // some side has BC_OPEN (boundary.f90:35-38)
   int cur_step = 0;
   int peak_substeps = 0, last_substeps = 0, steps_taken = 0, n_s_stages = 0;
   int blk_x = 32, blk_y = 4;            // block shape of the point kernels (measured best at 256^3)
@@ -183,6 +184,33 @@ inline void rbox(Run<R>& run, const char* func, int line, int words, int i0, int
 // thread (k_box_z's ZP), each measured per kernel at 256^3.
 #define LARE_BOXWH(run, minb64, zp32, words, i0, i1, j0, j1, k0, k1, ...) \
   rbox<minb64, zp32>((run), __func__, __LINE__, (words), (i0), (i1), (j0), (j1), (k0), (k1), __VA_ARGS__)
+
+// Some kernels write an array's new values into a second buffer that is
+// then swapped in, covering only the points the reference updates (which it
+// does in place, so every other point keeps its old value).  Periodic and
+// BC_USER ghost fills rewrite every ghost right after; an open side is never
+// refilled, so with an open side every point of the array's bounds [lo, hi]
+// outside the updated box [a, b] is carried from the old buffer.
+template <class R>
+inline void carry_outside(Run<R>& run, R* dst, const R* src, const int lo[3], const int hi[3], const int a[3],
+                          const int b[3]) {
+  if (!run.any_open) return;
+  const int sx = run.sx, sxy = run.sxy;
+  const int a0 = a[0], a1 = a[1], a2 = a[2], b0 = b[0], b1 = b[1], b2 = b[2];
+  LARE_BOX(run, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int i, int j, int k) {
+    if (i >= a0 && i <= b0 && j >= a1 && j <= b1 && k >= a2 && k <= b2) return;
+    const int c = i + sx * j + sxy * k;
+    dst[c] = src[c];
+  });
+}
+
+// the three velocity components after an update of the nodes 0:n
+template <class R>
+inline void carry_velocity(Run<R>& run, R* const nv[3], R* const ov[3]) {
+  const int lo[3] = {-2, -2, -2}, hi[3] = {run.n[0] + 2, run.n[1] + 2, run.n[2] + 2};
+  const int a[3] = {0, 0, 0}, b[3] = {run.n[0], run.n[1], run.n[2]};
+  for (int q = 0; q < 3; ++q) carry_outside(run, nv[q], ov[q], lo, hi, a, b);
+}
 
 template <class R>
 inline void ghost(Run<R>& run, const GSpec& g, A3<R> a, A3<R>* b = nullptr, A3<R>* c = nullptr) {
@@ -665,6 +693,50 @@ void energy_account(Run<R>& run) {
     if (iz == 0 || iz == nz) w1 = w1 * 0.5;
     v[0] = w1 * 0.5;
   }, SC_EN_KE, false);
+}
+
+}  // namespace lare
+
+#include "openbc.cuh"
+
+namespace lare {
+
+template <int F, class R>
+inline void open_face(Run<R>& run, const OpenArgs<R>& g) {
+  if (run.p.bc[F / 2][F & 1] != LARE_BC_OPEN) return;
+  const int nu = F / 2 == 0 ? run.n[1] : run.n[0], nw = F / 2 == 2 ? run.n[1] : run.n[2];
+  dim3 blk(32, 4, 1);
+  dim3 grd((nu + 2 + 31) / 32, (nw + 2 + 3) / 4, 1);
+  const int k = run.prof_begin("open_bcs", F, 0, (double)(nu + 2) * (nw + 2));
+  k_open_face<F, R><<<grd, blk, 0, run.s>>>(g);
+  run.prof_end(k);
+  ++run.launches;
+}
+
+// openboundary.f90:30-324 open_bcs: the open faces in the reference's order.
+template <class R>
+void open_bcs(Run<R>& run) {
+  OpenArgs<R> g;
+  g.vx = run.a.vx.p;
+  g.vy = run.a.vy.p;
+  g.vz = run.a.vz.p;
+  g.bx = run.a.bx.p;
+  g.by = run.a.by.p;
+  g.bz = run.a.bz.p;
+  g.rho = run.a.rho.p;
+  g.energy = run.a.energy.p;
+  g.g = (R)run.p.gamma;
+  g.nx = run.n[0];
+  g.ny = run.n[1];
+  g.nz = run.n[2];
+  g.sx = run.sx;
+  g.sxy = run.sxy;
+  open_face<0>(run, g);
+  open_face<1>(run, g);
+  open_face<2>(run, g);
+  open_face<3>(run, g);
+  open_face<4>(run, g);
+  open_face<5>(run, g);
 }
 
 }  // namespace lare

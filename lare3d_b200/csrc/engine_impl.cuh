@@ -170,6 +170,8 @@ class EngineT : public EngineBase {
       p.bc[d][1] = bcs[2 * d + 1];
       p.per[d] = bcs[2 * d] == LARE_BC_PERIODIC && bcs[2 * d + 1] == LARE_BC_PERIODIC;
     }
+    run.any_open = false;
+    for (int q = 0; q < 6; ++q) run.any_open = run.any_open || bcs[q] == LARE_BC_OPEN;
     run.n[0] = nx; run.n[1] = ny; run.n[2] = nz;
     run.sx = ((nx + 5) + 3) / 4 * 4;
     int sy = ny + 5, sz = nz + 5;

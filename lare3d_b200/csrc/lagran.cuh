@@ -231,6 +231,18 @@ void resistive_update(Run<R>& run) {
   std::swap(A.bx.p, A.bx1.p);
   std::swap(A.by.p, A.by1.p);
   std::swap(A.bz.p, A.bz1.p);
+  {
+    // bstep updates bx over 0:n x 1:n x 1:n, by over 1:n x 0:n x 1:n, bz
+    // over 1:n x 1:n x 0:n (lagran.F90:1588-1631)
+    R* const nb[3] = {A.bx.p, A.by.p, A.bz.p};
+    R* const ob[3] = {A.bx1.p, A.by1.p, A.bz1.p};
+    for (int q = 0; q < 3; ++q) {
+      int lo[3] = {-1, -1, -1}, hi[3] = {nx + 2, ny + 2, nz + 2}, a[3] = {1, 1, 1}, b[3] = {nx, ny, nz};
+      lo[q] = -2;
+      a[q] = 0;
+      carry_outside(run, nb[q], ob[q], lo, hi, a, b);
+    }
+  }
   bfield_bcs(run);
   // RS3: ohmic heating (1:n), MAX(energy, 0) (-1:n+2) and the
   // total_ohmic_heating sum over vertices 0:n (:1270-1328)
@@ -532,8 +544,15 @@ void predictor_remap(Run<R>& run, int step) {
   std::swap(A.bx.p, A.bx0.p);
   std::swap(A.by.p, A.by0.p);
   std::swap(A.bz.p, A.bz0.p);
-  // vx1 = vx (lagran.F90:1051-1053): the sweeps read v itself
+  // vx1 = vx (lagran.F90:1051-1053): the sweeps read v itself.  vx1's own
+  // nodes 0:n are rewritten by the predictor force and its ghosts by
+  // remap_v_bcs, except on an open side: there the copy's ghost values are
+  // carried into the vx1 buffer.
   R* const keep[3] = {A.vx1.p, A.vy1.p, A.vz1.p};
+  {
+    R* const ov[3] = {A.vx.p, A.vy.p, A.vz.p};
+    carry_velocity(run, keep, ov);
+  }
   A.vx1.p = A.vx.p;
   A.vy1.p = A.vy.p;
   A.vz1.p = A.vz.p;
@@ -796,7 +815,13 @@ void predictor_corrector_step(Run<R>& run) {
   std::swap(A.vx.p, A.qx.p);
   std::swap(A.vy.p, A.qy.p);
   std::swap(A.vz.p, A.qz.p);
+  {
+    R* const nv[3] = {A.vx.p, A.vy.p, A.vz.p};
+    R* const ov[3] = {A.qx.p, A.qy.p, A.qz.p};
+    carry_velocity(run, nv, ov);
+  }
   velocity_bcs(run);
+  open_bcs(run);  // lagran.F90:410-412 (no launch unless a side is open)
   // PC4 (1:n): final cv1, energy, visc_dep, rho; total_visc_heating
   R* const cv1w = A.cv1.p;
   R* const rhow = A.rho.p;

@@ -16,7 +16,7 @@ struct lare_ctx {
 };
 
 namespace {
-bool bc_supported(int c) { return c == LARE_BC_PERIODIC || c == LARE_BC_USER; }
+bool bc_supported(int c) { return c == LARE_BC_PERIODIC || c == LARE_BC_USER || c == LARE_BC_OPEN; }
 
 int guard(lare_ctx* c) { return (c && c->e) ? LARE_OK : LARE_EINVAL; }
 
@@ -40,7 +40,7 @@ int lare_gpu_init(const lare_params* p, int nx, int ny, int nz, const double* dx
   if (precision != 64 && precision != 32) return LARE_EINVAL;
   const int bcs[6] = {p->xbc_min, p->xbc_max, p->ybc_min, p->ybc_max, p->zbc_min, p->zbc_max};
   for (int q = 0; q < 6; ++q)
-    if (!bc_supported(bcs[q])) return LARE_EINVAL;  // BC_OPEN (openboundary.f90) is not on this path
+    if (!bc_supported(bcs[q])) return LARE_EINVAL;
   // A periodic boundary needs both sides periodic: the reference leaves the
   // ghosts of a half-periodic direction unset (mpi_routines.F90:195-210).
   for (int d = 0; d < 3; ++d)

@@ -1071,6 +1071,11 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   std::swap(Ar.vx.p, Ar.qx.p);
   std::swap(Ar.vy.p, Ar.qy.p);
   std::swap(Ar.vz.p, Ar.qz.p);
+  {
+    R* const nv[3] = {Ar.vx.p, Ar.vy.p, Ar.vz.p};
+    R* const ov[3] = {Ar.qx.p, Ar.qy.p, Ar.qz.p};
+    carry_velocity(run, nv, ov);
+  }
 
   // The new density becomes rho; the old buffer is scratch again.
   std::swap(Ar.rho.p, Ar.rho_alt.p);

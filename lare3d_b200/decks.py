@@ -23,7 +23,7 @@ from typing import Optional
 
 import numpy as np
 
-from .abi import BC_PERIODIC, BC_USER, LareParams, State, default_params
+from .abi import BC_OPEN, BC_PERIODIC, BC_USER, LareParams, State, default_params
 from .grid import grid
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -93,6 +93,34 @@ def blast(n: int = 64, **over) -> Deck:
     st["by"][...] = b0
     st["bz"][...] = 0.0
     return Deck("blast", p, n, n, n, m, st, nsteps=100)
+
+
+def open_blast(n: int = 64, b=(1.0 / math.sqrt(2.0), 1.0 / math.sqrt(2.0), 0.0), p_in: float = 0.3,
+               **over) -> Deck:
+    """A pressure pulse off-centre towards x min in a box with open
+    (characteristic) boundaries on the x and y sides and periodic z
+    (openboundary.f90).  The ghosts of the open sides carry the ambient
+    state, which serves as the far field.  A field along x only makes the
+    x faces take the Alfven-mode solver (no transverse far field).  The
+    reference's characteristic boundary is linearised about the far field:
+    a strong wave leaving the box (inner pressure many times the ambient)
+    drives its ghost density to TINY, so the default overpressure is 3:1."""
+    g = 5.0 / 3.0
+    p = default_params(gamma=g, visc1=0.1, visc2=0.5, dt_multiplier=0.8,
+                       xbc_min=BC_OPEN, xbc_max=BC_OPEN, ybc_min=BC_OPEN, ybc_max=BC_OPEN)
+    for k, v in over.items():
+        setattr(p, k, v)
+    m = grid(n, n, n, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0))
+    st = State.zeros(n, n, n)
+    xc, yc, zc, *_ = _coords(m, n, n, n)
+    r = np.sqrt((xc - 0.25) ** 2 + (yc - 0.5) ** 2 + (zc - 0.5) ** 2)
+    pres = np.where(r < 0.15, p_in, 0.1)
+    st["rho"][...] = 1.0
+    st["energy"][...] = np.asfortranarray(pres / ((g - 1.0) * 1.0))
+    st["bx"][...] = b[0]
+    st["by"][...] = b[1]
+    st["bz"][...] = b[2]
+    return Deck("open_blast", p, n, n, n, m, st, nsteps=100)
 
 
 def _curl_edges(Ax, Ay, Az, m, n):

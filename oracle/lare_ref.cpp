@@ -272,6 +272,213 @@ struct lare_ref {
       if (user(d, true)) for (int q = N; q <= N + 2; ++q) zero_plane(a, d, q);
     }
   }
+  // ------------------------------------------------------------------
+  // Open (characteristic) boundaries, openboundary.f90.  A side with
+  // BC_OPEN gets no ghost fill from boundary.f90 (the direction is not
+  // periodic and the mirror rules are BC_USER only), so its second ghost
+  // layer keeps the uploaded far-field state; once per step (after
+  // velocity_bcs in predictor_corrector_step, lagran.F90:409-412) the first
+  // ghost layer of B, rho and energy is set from the Riemann invariants
+  // carried out of the domain and in from the far field.
+  struct OpenIn {
+    double vn, vx1, vy1, vz1, bx1, by1, bz1, r1, e1, pbc, pfar, uxf, uyf, uzf, bxf, byf, bzf, rf;
+  };
+  struct OpenOut {
+    double bx0, by0, bz0, r0, e0;
+  };
+  // openboundary.f90:326-378, open_bcs_fast (transverse field present)
+  static OpenOut open_fast(const OpenIn& a, double g) {
+    OpenOut o;
+    const double c0far = std::sqrt(g * a.pfar / a.rf);
+    const double ctfar = std::sqrt((a.byf * a.byf + a.bzf * a.bzf) / a.rf);
+    const double cffar = std::sqrt(c0far * c0far + ctfar * ctfar);
+    const double c0 = std::sqrt(g * (g - 1.0) * a.e1);
+    const double ct = std::sqrt((a.by1 * a.by1 + a.bz1 * a.bz1) / a.r1);
+    const double cf = std::sqrt(c0 * c0 + ct * ct);
+    const double vtest[3] = {a.vn + cf, a.vn - cf, a.vn};
+    double pstar[3], pmag[3], vstar[3], rstar[3], bys[3], bzs[3];
+    for (int i = 0; i < 3; ++i) {
+      if (vtest[i] >= 0.0) {
+        pstar[i] = a.pbc + 0.5 * (a.by1 * a.by1 + a.bz1 * a.bz1);
+        pmag[i] = 0.5 * (a.by1 * a.by1 + a.bz1 * a.bz1);
+        vstar[i] = a.vx1;
+        rstar[i] = a.r1;
+        bys[i] = a.by1;
+        bzs[i] = a.bz1;
+      } else {
+        pstar[i] = a.pfar + 0.5 * (a.byf * a.byf + a.bzf * a.bzf);
+        pmag[i] = 0.5 * (a.byf * a.byf + a.bzf * a.bzf);
+        vstar[i] = a.uxf;
+        rstar[i] = a.rf;
+        bys[i] = a.byf;
+        bzs[i] = a.bzf;
+      }
+    }
+    o.bx0 = 0.5 * (a.bx1 + a.bxf);
+    o.by0 = 0.5 * (bys[0] + bys[1]);
+    o.bz0 = 0.5 * (bzs[0] + bzs[1]);
+    double pg = 0.5 * (pstar[0] + pstar[1] + a.rf * cffar * (vstar[0] - vstar[1])) - 0.5 * (pmag[0] + pmag[1]);
+    pg = std::fmax(pg, 0.0);
+    const double rhog = rstar[2] + (pg - (pstar[2] - pmag[2])) / (c0far * c0far);
+    o.r0 = std::fmax(rhog, none_zero);
+    o.e0 = pg / (g - 1.0) / o.r0;
+    return o;
+  }
+  // openboundary.f90:382-455, open_bcs_alfven (no transverse far field)
+  static OpenOut open_alfven(const OpenIn& a, double g) {
+    OpenOut o;
+    const double lyfar = -(a.bxf * a.byf), lzfar = -(a.bxf * a.bzf);
+    const double c0far = std::sqrt(g * a.pfar / a.rf);
+    const double cxfar = std::sqrt(a.bxf * a.bxf / a.rf);
+    const double c0 = std::sqrt(g * (g - 1.0) * a.e1);
+    const double cx = std::sqrt(a.bx1 * a.bx1 / a.r1);
+    const double vtest[5] = {a.vn + c0, a.vn - c0, a.vn + cx, a.vn - cx, a.vn};
+    double pstar[5], pmag[5], ly[5], lz[5], ux[5], uy[5], uz[5], rstar[5];
+    for (int i = 0; i < 5; ++i) {
+      if (vtest[i] >= 0.0) {
+        pstar[i] = a.pbc + 0.5 * (a.by1 * a.by1 + a.bz1 * a.bz1 - a.bx1 * a.bx1);
+        pmag[i] = 0.5 * (a.by1 * a.by1 + a.bz1 * a.bz1 - a.bx1 * a.bx1);
+        ly[i] = -(a.by1 * a.bx1);
+        lz[i] = -(a.bz1 * a.bx1);
+        ux[i] = a.vx1;
+        uy[i] = a.vy1;
+        uz[i] = a.vz1;
+        rstar[i] = a.r1;
+      } else {
+        pstar[i] = a.pfar + 0.5 * (a.byf * a.byf + a.bzf * a.bzf - a.bxf * a.bxf);
+        pmag[i] = 0.5 * (a.byf * a.byf + a.bzf * a.bzf - a.bxf * a.bxf);
+        ly[i] = lyfar;
+        lz[i] = lzfar;
+        ux[i] = a.uxf;
+        uy[i] = a.uyf;
+        uz[i] = a.uzf;
+        rstar[i] = a.rf;
+      }
+    }
+    o.bx0 = 0.5 * (a.bx1 + a.bxf);
+    if (std::fabs(o.bx0) <= none_zero) o.bx0 = none_zero;
+    double lg = 0.5 * (ly[2] + ly[3] + a.rf * cxfar * (uy[2] - uy[3]));
+    o.by0 = -(lg / o.bx0);
+    lg = 0.5 * (lz[2] + lz[3] + a.rf * cxfar * (uz[2] - uz[3]));
+    o.bz0 = -(lg / o.bx0);
+    double pg = 0.5 * (pstar[0] + pstar[1] + a.rf * c0far * (ux[0] - ux[1])) -
+                0.5 * (o.by0 * o.by0 + o.bz0 * o.bz0 - o.bx0 * o.bx0);
+    pg = std::fmax(pg, none_zero);
+    const double rhog = rstar[4] + (pg - (pstar[4] - pmag[4])) / (c0far * c0far);
+    o.r0 = std::fmax(rhog, none_zero);
+    o.e0 = pg / (g - 1.0) / o.r0;
+    return o;
+  }
+  static OpenOut open_solve(const OpenIn& a, double g) {
+    // solver choice on the far-field transverse field (openboundary.f90:63-71)
+    const double bperp = std::sqrt(a.byf * a.byf + a.bzf * a.bzf);
+    return bperp <= none_zero ? open_alfven(a, g) : open_fast(a, g);
+  }
+  bool any_open() const {
+    const int c[6] = {p.xbc_min, p.xbc_max, p.ybc_min, p.ybc_max, p.zbc_min, p.zbc_max};
+    for (int q = 0; q < 6; ++q)
+      if (c[q] == LARE_BC_OPEN) return true;
+    return false;
+  }
+  // openboundary.f90:30-324, faces in the reference's order; a later face
+  // reads edge values an earlier one wrote.  In each face the normal
+  // velocity and field are sign-flipped on the min side, and the far field
+  // is the second ghost layer.
+  void open_bcs() {
+    const double g = p.gamma;
+    auto pres = [&](int i, int j, int k) { return (g - 1.0) * energy(i, j, k) * rho(i, j, k); };
+    if (p.xbc_min == LARE_BC_OPEN) {  // :35-80
+      for (int iz = 0; iz <= nz + 1; ++iz)
+        for (int iy = 0; iy <= ny + 1; ++iy) {
+          OpenIn a{-vx(0, iy, iz), -vx(0, iy, iz), vy(0, iy, iz), vz(0, iy, iz), -bx(0, iy, iz), by(1, iy, iz),
+                   bz(1, iy, iz), rho(1, iy, iz), energy(1, iy, iz), pres(1, iy, iz), pres(-1, iy, iz),
+                   -vx(-2, iy, iz), vy(-2, iy, iz), vz(-2, iy, iz), -bx(-2, iy, iz), by(-1, iy, iz),
+                   bz(-1, iy, iz), rho(-1, iy, iz)};
+          OpenOut o = open_solve(a, g);
+          bx(-1, iy, iz) = -o.bx0;
+          by(0, iy, iz) = o.by0;
+          bz(0, iy, iz) = o.bz0;
+          rho(0, iy, iz) = o.r0;
+          energy(0, iy, iz) = o.e0;
+        }
+    }
+    if (p.xbc_max == LARE_BC_OPEN) {  // :83-128
+      for (int iz = 0; iz <= nz + 1; ++iz)
+        for (int iy = 0; iy <= ny + 1; ++iy) {
+          OpenIn a{vx(nx, iy, iz), vx(nx, iy, iz), vy(nx, iy, iz), vz(nx, iy, iz), bx(nx, iy, iz), by(nx, iy, iz),
+                   bz(nx, iy, iz), rho(nx, iy, iz), energy(nx, iy, iz), pres(nx, iy, iz), pres(nx + 2, iy, iz),
+                   vx(nx + 2, iy, iz), vy(nx + 2, iy, iz), vz(nx + 2, iy, iz), bx(nx + 2, iy, iz),
+                   by(nx + 2, iy, iz), bz(nx + 2, iy, iz), rho(nx + 2, iy, iz)};
+          OpenOut o = open_solve(a, g);
+          bx(nx + 1, iy, iz) = o.bx0;
+          by(nx + 1, iy, iz) = o.by0;
+          bz(nx + 1, iy, iz) = o.bz0;
+          rho(nx + 1, iy, iz) = o.r0;
+          energy(nx + 1, iy, iz) = o.e0;
+        }
+    }
+    if (p.ybc_min == LARE_BC_OPEN) {  // :131-176
+      for (int iz = 0; iz <= nz + 1; ++iz)
+        for (int ix = 0; ix <= nx + 1; ++ix) {
+          OpenIn a{-vy(ix, 0, iz), -vy(ix, 0, iz), vx(ix, 0, iz), vz(ix, 0, iz), -by(ix, 0, iz), bx(ix, 1, iz),
+                   bz(ix, 1, iz), rho(ix, 1, iz), energy(ix, 1, iz), pres(ix, 1, iz), pres(ix, -1, iz),
+                   -vy(ix, -2, iz), vx(ix, -2, iz), vz(ix, -2, iz), -by(ix, -2, iz), bx(ix, -1, iz),
+                   bz(ix, -1, iz), rho(ix, -1, iz)};
+          OpenOut o = open_solve(a, g);
+          bx(ix, 0, iz) = o.by0;
+          by(ix, -1, iz) = -o.bx0;
+          bz(ix, 0, iz) = o.bz0;
+          rho(ix, 0, iz) = o.r0;
+          energy(ix, 0, iz) = o.e0;
+        }
+    }
+    if (p.ybc_max == LARE_BC_OPEN) {  // :179-224
+      for (int iz = 0; iz <= nz + 1; ++iz)
+        for (int ix = 0; ix <= nx + 1; ++ix) {
+          OpenIn a{vy(ix, ny, iz), vy(ix, ny, iz), vx(ix, ny, iz), vz(ix, ny, iz), by(ix, ny, iz), bx(ix, ny, iz),
+                   bz(ix, ny, iz), rho(ix, ny, iz), energy(ix, ny, iz), pres(ix, ny, iz), pres(ix, ny + 2, iz),
+                   vy(ix, ny + 2, iz), vx(ix, ny + 2, iz), vz(ix, ny + 2, iz), by(ix, ny + 2, iz),
+                   bx(ix, ny + 2, iz), bz(ix, ny + 2, iz), rho(ix, ny + 2, iz)};
+          OpenOut o = open_solve(a, g);
+          bx(ix, ny + 1, iz) = o.by0;
+          by(ix, ny + 1, iz) = o.bx0;
+          bz(ix, ny + 1, iz) = o.bz0;
+          rho(ix, ny + 1, iz) = o.r0;
+          energy(ix, ny + 1, iz) = o.e0;
+        }
+    }
+    if (p.zbc_min == LARE_BC_OPEN) {  // :227-273
+      for (int iy = 0; iy <= ny + 1; ++iy)
+        for (int ix = 0; ix <= nx + 1; ++ix) {
+          OpenIn a{-vz(ix, iy, 0), -vz(ix, iy, 0), vy(ix, iy, 0), vx(ix, iy, 0), -bz(ix, iy, 0), by(ix, iy, 1),
+                   bx(ix, iy, 1), rho(ix, iy, 1), energy(ix, iy, 1), pres(ix, iy, 1), pres(ix, iy, -1),
+                   -vz(ix, iy, -2), vy(ix, iy, -2), vx(ix, iy, -2), -bz(ix, iy, -2), by(ix, iy, -1),
+                   bx(ix, iy, -1), rho(ix, iy, -1)};
+          OpenOut o = open_solve(a, g);
+          bx(ix, iy, 0) = o.bz0;
+          by(ix, iy, 0) = o.by0;
+          bz(ix, iy, -1) = -o.bx0;
+          rho(ix, iy, 0) = o.r0;
+          energy(ix, iy, 0) = o.e0;
+        }
+    }
+    if (p.zbc_max == LARE_BC_OPEN) {  // :276-320
+      for (int iy = 0; iy <= ny + 1; ++iy)
+        for (int ix = 0; ix <= nx + 1; ++ix) {
+          OpenIn a{vz(ix, iy, nz), vz(ix, iy, nz), vy(ix, iy, nz), vx(ix, iy, nz), bz(ix, iy, nz), by(ix, iy, nz),
+                   bx(ix, iy, nz), rho(ix, iy, nz), energy(ix, iy, nz), pres(ix, iy, nz), pres(ix, iy, nz + 2),
+                   vz(ix, iy, nz + 2), vy(ix, iy, nz + 2), vx(ix, iy, nz + 2), bz(ix, iy, nz + 2),
+                   by(ix, iy, nz + 2), bx(ix, iy, nz + 2), rho(ix, iy, nz + 2)};
+          OpenOut o = open_solve(a, g);
+          bx(ix, iy, nz + 1) = o.bz0;
+          by(ix, iy, nz + 1) = o.by0;
+          bz(ix, iy, nz + 1) = o.bx0;
+          rho(ix, iy, nz + 1) = o.r0;
+          energy(ix, iy, nz + 1) = o.e0;
+        }
+    }
+  }
+
   void velocity_bcs() {  // boundary.f90:255
     node_mpi(vx); node_mpi(vy); node_mpi(vz);
     node_user(vx); node_user(vy); node_user(vz);
@@ -486,6 +693,7 @@ struct lare_ref {
       vz(ix, iy, iz) = 2.0 * vz1(ix, iy, iz) - vz(ix, iy, iz);
     });
     velocity_bcs();
+    if (any_open()) open_bcs();  // :409-412
 
     // :415-462, serial because of the total_visc_heating sum.
     for (int iz = 1; iz <= nz; ++iz) {
@@ -1405,7 +1613,7 @@ int fail(lare_ref* r, int code, const char* msg) {
   if (r) r->err = msg;
   return code;
 }
-bool bc_ok(int c) { return c == LARE_BC_PERIODIC || c == LARE_BC_USER; }
+bool bc_ok(int c) { return c == LARE_BC_PERIODIC || c == LARE_BC_USER || c == LARE_BC_OPEN; }
 
 void copy_in(F3& a, const double* h) { std::memcpy(a.d.data(), h, a.d.size() * sizeof(double)); }
 void copy_out(F3& a, double* h) { std::memcpy(h, a.d.data(), a.d.size() * sizeof(double)); }

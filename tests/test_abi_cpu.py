@@ -88,9 +88,12 @@ def test_host_side_argument_checks(built):
     m = [np.ascontiguousarray(d.metrics[k]) for k in ("dxb", "dxc", "dyb", "dyc", "dzb", "dzc")]
     ptr = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in m]
     lib.lare_gpu_init.restype = C.c_int
-    # n < 4, bad precision and unsupported BC_OPEN are rejected on the host.
+    # n < 4, bad precision, an unknown BC code and a half-periodic direction
+    # (open on one side, periodic on the other) are rejected on the host.
     assert lib.lare_gpu_init(C.byref(d.params), 3, 8, 8, *ptr, 64, C.byref(out)) == -1
     assert lib.lare_gpu_init(C.byref(d.params), 8, 8, 8, *ptr, 16, C.byref(out)) == -1
+    p = default_params(xbc_min=7, xbc_max=7)
+    assert lib.lare_gpu_init(C.byref(p), 8, 8, 8, *ptr, 64, C.byref(out)) == -1
     p = default_params(xbc_min=3)
     assert lib.lare_gpu_init(C.byref(p), 8, 8, 8, *ptr, 64, C.byref(out)) == -1
     assert not out.value

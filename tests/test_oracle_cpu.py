@@ -202,3 +202,52 @@ def test_kappa_perp_extension_moves_heat_across_the_field(built):
     dev = e0[core] - e0[core].mean()
     assert np.corrcoef(dev.ravel(), d.ravel())[0, 1] < -0.5
     assert d.ravel()[np.argmax(dev)] < 0 < d.ravel()[np.argmin(dev)]
+
+
+# ---------------------------------------------------------------------------
+# Open (characteristic) boundaries, openboundary.f90
+
+
+@pytest.mark.parametrize("b", [(2 ** -0.5, 2 ** -0.5, 0.0), (1.0, 0.0, 0.0)])
+def test_open_boundaries_bounds_checked(built, b):
+    """Both solvers (fast mode; Alfven mode where the far field has no
+    transverse B) stay inside the reference's array bounds."""
+    d = decks.open_blast(12, b=b)
+    s = oracle_sim(d, checked=True)
+    s.start(d.state)
+    for st in range(1, 7):
+        s.step(st)
+    assert all(np.isfinite(v).all() for v in s.download().arrays.values())
+
+
+def test_open_boundaries_keep_a_uniform_state(built):
+    d = decks.open_blast(10)
+    d.state["energy"][...] = 0.1 / (d.params.gamma - 1.0)
+    s = oracle_sim(d)
+    s.start(d.state)
+    a = s.download()
+    for st in range(1, 7):
+        s.step(st)
+    c = s.download()
+    for f in ("rho", "energy", "vx", "vy", "vz", "bx", "by", "bz"):
+        assert np.abs(c[f] - a[f]).max() < 1e-12, f
+
+
+def test_open_boundaries_let_waves_out(built):
+    """A pressure pulse in a box open on four sides loses mass and keeps
+    little kinetic energy, while the same pulse in a periodic box keeps its
+    mass exactly and rings."""
+    n = 16
+    out = {}
+    for name, over in (("open", {}), ("periodic", dict(xbc_min=BC_PERIODIC, xbc_max=BC_PERIODIC,
+                                                       ybc_min=BC_PERIODIC, ybc_max=BC_PERIODIC))):
+        d = decks.open_blast(n, **over)
+        s = oracle_sim(d)
+        s.start(d.state)
+        m0 = mass(s.download(), d.metrics, n)
+        for st in range(1, 81):
+            s.step(st)
+        out[name] = ((mass(s.download(), d.metrics, n) - m0) / m0, s.energy()[1])
+    assert out["open"][0] < -1e-3
+    assert abs(out["periodic"][0]) < 1e-13
+    assert out["open"][1] < 0.2 * out["periodic"][1]
