@@ -54,6 +54,12 @@ extern "C" {
 #define LARE_ENOTFOUND (-6)  /* unknown field name */
 #define LARE_ENONFINITE (-7) /* non-finite value in uploaded state */
 #define LARE_ETOOLARGE (-8)  /* grid beyond a fixed-capacity entry point's limit */
+#define LARE_EEOS (-9)       /* neutral_fraction's temperature bracket is empty (neutral.f90:171-174) */
+
+/* Equations of state, shared_data.F90:73 (0 is taken as EOS_IDEAL). */
+#define LARE_EOS_IDEAL 1
+#define LARE_EOS_ION 2
+#define LARE_EOS_PI 3
 
 /*
  * Control scalars read by the hot path.  Field names follow
@@ -79,6 +85,18 @@ typedef struct lare_params {
   int boris;               /* control.f90:183 */
   int restart;             /* IC_RESTART (lare3d.f90:56-60) */
   int xbc_min, xbc_max, ybc_min, ybc_max, zbc_min, zbc_max; /* control.f90:169-174 */
+  /*
+   * Partially ionised plasma (neutral.f90).  With eos_number EOS_ION or
+   * EOS_PI the neutral fraction xi_n becomes a per-cell array that
+   * neutral_fraction solves for; with cowling_resistivity the cross-field
+   * resistivity eta_perp (perpendicular_resistivity) enters set_dt and the
+   * resistive fluxes.  The constants are the normalised values the
+   * reference holds after setup_neutral (neutral.f90:31-63) and
+   * normalise_transport (normalise.f90:39-51); xi_n above is then unused.
+   */
+  int eos_number;          /* LARE_EOS_* (control.f90:191) */
+  int cowling_resistivity; /* control.f90:162 */
+  double f_bar, t_bar, r_bar, tr, eta_bar;
 } lare_params;
 
 /* Scalars of shared_data that the step updates. */
@@ -141,8 +159,26 @@ int lare_gpu_eta_calc(lare_ctx* ctx);
 int lare_gpu_boundary_conditions(lare_ctx* ctx);
 
 /*
- * One timestep of the driver loop (lare3d.f90:83-87): lagrangian_step,
- * eulerian_remap(step), eta_calc.  time/dt (may be NULL) receive the
+ * neutral.f90:158 neutral_fraction: xi_n over the whole cell array from rho
+ * and energy by bisection on the temperature (a no-op under EOS_IDEAL).
+ * LARE_EEOS where a cell's temperature bracket is empty (the reference
+ * stops there).  lare_gpu_step and lare_gpu_run call it first in each step
+ * (lare3d.f90:83), and the resistive sub-cycles and the RKL2 stages call it
+ * where the reference does (lagran.F90:147, conduct.f90:404).
+ */
+int lare_gpu_neutral_fraction(lare_ctx* ctx);
+
+/*
+ * neutral.f90:68 perpendicular_resistivity: eta_perp at the vertices 0:n
+ * (LARE_EINVAL unless cowling_resistivity).  The resistive sub-cycles call
+ * it after neutral_fraction (lagran.F90:148); a driver calls both once
+ * after the initial boundary_conditions and eta_calc (lare3d.f90:70-74).
+ */
+int lare_gpu_perpendicular_resistivity(lare_ctx* ctx);
+
+/*
+ * One timestep of the driver loop (lare3d.f90:83-87): neutral_fraction
+ * (unless EOS_IDEAL), lagrangian_step, eulerian_remap(step), eta_calc.  time/dt (may be NULL) receive the
  * updated clock.
  */
 int lare_gpu_step(lare_ctx* ctx, int step, double* time, double* dt);

@@ -17,6 +17,10 @@ BC_PERIODIC = 1
 BC_USER = 2
 BC_OPEN = 3
 
+EOS_IDEAL = 1
+EOS_ION = 2
+EOS_PI = 3
+
 LARE_OK = 0
 ERRORS = {
     -1: "LARE_EINVAL",
@@ -27,6 +31,7 @@ ERRORS = {
     -6: "LARE_ENOTFOUND",
     -7: "LARE_ENONFINITE",
     -8: "LARE_ETOOLARGE",
+    -9: "LARE_EEOS",
 }
 
 
@@ -60,6 +65,13 @@ class LareParams(C.Structure):
         ("ybc_max", C.c_int),
         ("zbc_min", C.c_int),
         ("zbc_max", C.c_int),
+        ("eos_number", C.c_int),
+        ("cowling_resistivity", C.c_int),
+        ("f_bar", C.c_double),
+        ("t_bar", C.c_double),
+        ("r_bar", C.c_double),
+        ("tr", C.c_double),
+        ("eta_bar", C.c_double),
     ]
 
 
@@ -105,6 +117,8 @@ def default_params(**kw) -> LareParams:
     p.restart = 0
     for s in ("xbc_min", "xbc_max", "ybc_min", "ybc_max", "zbc_min", "zbc_max"):
         setattr(p, s, BC_PERIODIC)
+    p.eos_number = EOS_IDEAL
+    p.cowling_resistivity = 0
     for k, v in kw.items():
         if not hasattr(p, k):
             raise KeyError(k)
@@ -220,6 +234,9 @@ class Binding:
             f("conduction_stages", [C.c_void_p, C.c_double, C.POINTER(C.c_int)])
             f("field_device", [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int),
                                C.POINTER(C.c_int), C.POINTER(C.c_int)])
+        if hasattr(lib, prefix + "neutral_fraction"):
+            f("neutral_fraction", [C.c_void_p])
+            f("perpendicular_resistivity", [C.c_void_p])
         if hasattr(lib, prefix + "run"):
             f("run", [C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_int), dp, dp])
         if hasattr(lib, prefix + "launch_count"):
@@ -317,6 +334,12 @@ class Simulation:
     def boundary_conditions(self):
         self.b.call(self.ctx, "boundary_conditions")
 
+    def neutral_fraction(self):
+        self.b.call(self.ctx, "neutral_fraction")
+
+    def perpendicular_resistivity(self):
+        self.b.call(self.ctx, "perpendicular_resistivity")
+
     def step(self, step):
         t = C.c_double()
         d = C.c_double()
@@ -395,10 +418,14 @@ class Simulation:
     def __exit__(self, *exc):
         self.close()
 
-    # ---- the reference's initialisation tail (lare3d.f90:65-68)
+    # ---- the reference's initialisation tail (lare3d.f90:65-74)
     def start(self, st: State, eta=None, grav=None, visc3=None, time=0.0, dt=0.0):
         self.upload(st)
         self.upload_aux(eta=eta, grav=grav, visc3=visc3)
         self.set_time(time, dt)
         self.boundary_conditions()
         self.eta_calc()
+        if self.params.eos_number not in (0, EOS_IDEAL):
+            self.neutral_fraction()
+        if self.params.cowling_resistivity:
+            self.perpendicular_resistivity()

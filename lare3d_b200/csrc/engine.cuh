@@ -33,6 +33,8 @@ struct Par {
   double gamma, visc1, visc2, eta_background, eta0, j_max, kappa_0, flux_limiter;
   double ionise_pot, xi_n, va_max, dt_multiplier, dt_from_restart, kappa_perp_ratio;
   int resistive_mhd, conduction, heat_flux_limiter, use_viscous_damping, boris, restart;
+  int eos_number, cowling_resistivity;                 // neutral.f90 (eos_number 0 read as EOS_IDEAL)
+  double f_bar, t_bar, r_bar, tr, eta_bar;
   int bc[3][2];   // [dim][0=min,1=max]
   bool per[3];    // periodic communicator in this dimension (mpi_routines.F90:195-210)
 };
@@ -52,6 +54,8 @@ struct Arrays {
   // conduct.f90 temporaries
   A3<R> larsen, Y1, Y2, Y3, Lc_Y0;  // RKL2 (Y0 is read from energy itself)
   A3<R> kf[9];                        // stage-invariant face coefficients, 3 per face direction
+  // neutral.f90 (allocated only for a partially ionised run)
+  A3<R> xi, eta_perp;
   // 1-D metrics (pointers at Fortran index 0)
   A1<R> dxb, dxc, dyb, dyc, dzb, dzc, grav;
   // reciprocals for conduction: 1/dxb, 1/dxc, 1/(dxc(i) + dxc(i-1)), per axis
@@ -99,6 +103,8 @@ struct Run {
   bool set_dt_first = true;         // lagran.F90:1078 first (SAVE)
   bool gamma_boris_one = true;      // gamma_boris holds 1 everywhere
   bool any_open = false;            // some side has BC_OPEN (boundary.f90:35-38)
+  bool pip = false;                 // eos_number /= EOS_IDEAL: xi_n is the per-cell array a.xi
+  bool cowling = false;             // cowling_resistivity: eta_perp in set_dt and rkstep
   int cur_step = 0;
   int peak_substeps = 0, last_substeps = 0, steps_taken = 0, n_s_stages = 0;
   int blk_x = 32, blk_y = 4;            // block shape of the point kernels (measured best at 256^3)
@@ -392,8 +398,11 @@ void calc_s_stages(Run<R>& run, int dt_slot) {
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot, k0 = (R)run.p.kappa_0;
   const R fl = (R)run.p.flux_limiter;
   const bool limiter = run.p.heat_flux_limiter != 0;
+  const bool pip = run.pip;
+  auto xia = run.a.xi;  // per-cell xi_n when partially ionised
   LARE_BOXW(run, 2, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
-    temperature(ix, iy, iz) = (g - R(1)) / (R(2) - xi) * (energy(ix, iy, iz) - (R(1) - xi) * ip);
+    const R x = pip ? xia(ix, iy, iz) : xi;
+    temperature(ix, iy, iz) = (g - R(1)) / (R(2) - x) * (energy(ix, iy, iz) - (R(1) - x) * ip);
   });
   LARE_BOXW(run, 3, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz) {
     if (!limiter) { larsen(ix, iy, iz) = R(1); return; }
@@ -412,7 +421,8 @@ void calc_s_stages(Run<R>& run, int dt_slot) {
   launch_scalar(run.s, run.launches, [=] __device__() { us[U_DTPARAB] = (unsigned long long)__double_as_longlong(1.e10); });
   box_min<1>(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
     R kappa1 = k0 * larsen(ix, iy, iz);
-    R temp = (g - R(1)) / (R(2) - xi) * (energy(ix, iy, iz) - (R(1) - xi) * ip);
+    const R x = pip ? xia(ix, iy, iz) : xi;
+    R temp = (g - R(1)) / (R(2) - x) * (energy(ix, iy, iz) - (R(1) - x) * ip);
     R tp = pow25(temp);
     R r = rho(ix, iy, iz);
     R dt1 = r * (dxb(ix) * dxb(ix)) / (R(2) * kappa1 * tp);
@@ -456,8 +466,11 @@ void temperature_from(Run<R>& run, A3<R> e) {
   const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
   auto temperature = run.a.temperature;
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
+  const bool pip = run.pip;
+  auto xia = run.a.xi;
   LARE_BOXW(run, 2, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
-    temperature(ix, iy, iz) = (g - R(1)) / (R(2) - xi) * (e(ix, iy, iz) - (R(1) - xi) * ip);
+    const R x = pip ? xia(ix, iy, iz) : xi;
+    temperature(ix, iy, iz) = (g - R(1)) / (R(2) - x) * (e(ix, iy, iz) - (R(1) - x) * ip);
   });
 }
 
@@ -472,6 +485,7 @@ void copy_whole(Run<R>& run, A3<R> dst, A3<R> src) {
 
 }  // namespace lare
 
+#include "neutral.cuh"
 #include "conduct.cuh"
 
 namespace lare {
@@ -514,7 +528,12 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
   auto energy = A.energy;
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
   const R tc = (g - R(1)) / (R(2) - xi), te0 = (R(1) - xi) * ip;
-  auto temp = [&](A3<R> y) { return TempOf<R>{y, tc, te0}; };
+  // With a per-cell xi_n (partially ionised) the temperature changes with
+  // xi_n between stages, so each stage forms it into the temperature array
+  // exactly as conduct.f90:346-376 does, and the stage reads it back
+  // through 1 * (T - 0) = T.
+  const bool pip = run.pip;
+  auto temp = [&](A3<R> y) { return pip ? TempOf<R>{A.temperature, R(1), R(0)} : TempOf<R>{y, tc, te0}; };
   if (s < 2) {
     // The stage loop is empty and energy(1:n) = Y(3)(1:n) = energy: the
     // reference leaves the energy unchanged (conduct.f90:409).
@@ -526,7 +545,15 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
   A3<R> Y1 = energy, Y2 = bufs[0], Y3 = bufs[1];
   int next_free = 2;
   copy_whole(run, Y2, energy);
+  if (run.any_open) {
+    // The reference's Y(3) keeps the energy's ghosts throughout (only
+    // 1:n is written), and energy_bcs leaves an open side's ghosts alone:
+    // every stage buffer starts as the energy so that those ghosts match.
+    copy_whole(run, bufs[1], energy);
+    copy_whole(run, bufs[2], energy);
+  }
   face_coefficients(run);
+  if (pip) temperature_from(run, energy);
   rkl2_stage<R, true>(run, __LINE__, temp(energy), energy, energy, energy, Y2, dt_slot, (R)mu_tilde[1], R(0), R(0),
                       R(0), R(0));
   ghost(run, run.g_cell_user, Y2);
@@ -538,11 +565,16 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
   for (int j = 2; j <= s; ++j) {
     const R gt = (R)gamma_tilde[j], mtj = (R)mu_tilde[j], mj = (R)mu[j], nj = (R)nu[j];
     const R omn_r = R(1) - mj - nj;
+    if (pip) {
+      temperature_from(run, Y2);
+      temperature_bcs(run);
+    }
     rkl2_stage<R, false>(run, __LINE__, temp(Y2), Y2, Y1, energy, Y3, dt_slot, mtj, mj, nj, omn_r, gt);
     if (j < s) {
       GhostBatch<R> bb;
       bb.add(run.g_cell, Y3.p);  // energy_bcs on the copy of Y3
       ghost_flush(run, bb);
+      if (pip) neutral_fraction(run, Y3);  // conduct.f90:404
       A3<R> freed = Y1;
       Y1 = Y2;
       Y2 = Y3;
@@ -558,12 +590,14 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
   {
     auto temperature = A.temperature;
     A3<R> y2 = Y2, y3 = Y3;
-    LARE_BOXW(run, 2, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
-      temperature(ix, iy, iz) = tc * (y2(ix, iy, iz) - te0);
-    });
-    GhostBatch<R> bb;
-    bb.add(run.g_cell_user, temperature.p);
-    ghost_flush(run, bb);
+    if (!pip) {  // (a partially ionised run formed it for the last stage)
+      LARE_BOXW(run, 2, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+        temperature(ix, iy, iz) = tc * (y2(ix, iy, iz) - te0);
+      });
+      GhostBatch<R> bb;
+      bb.add(run.g_cell_user, temperature.p);
+      ghost_flush(run, bb);
+    }
     LARE_BOXW(run, 2, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) { energy(ix, iy, iz) = y3(ix, iy, iz); });
   }
   energy_bcs(run);

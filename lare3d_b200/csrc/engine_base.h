@@ -17,6 +17,9 @@ class EngineBase {
   virtual int eulerian_remap(int step) = 0;
   virtual int eta_calc() = 0;
   virtual int boundary_conditions() = 0;
+  virtual int neutral_fraction() = 0;           // no-op under EOS_IDEAL
+  virtual int perpendicular_resistivity() = 0;
+  virtual bool partially_ionised() const = 0;
   virtual int conduct_heat(double dt, int force_stages, int* n_stages) = 0;
   virtual int conduction_stages(double dt, int* n_stages) = 0;
   virtual int energy(double out[5]) = 0;

@@ -164,6 +164,11 @@ class EngineT : public EngineBase {
     p.resistive_mhd = prm->resistive_mhd; p.conduction = prm->conduction;
     p.heat_flux_limiter = prm->heat_flux_limiter; p.use_viscous_damping = prm->use_viscous_damping;
     p.boris = prm->boris; p.restart = prm->restart;
+    p.eos_number = prm->eos_number == 0 ? LARE_EOS_IDEAL : prm->eos_number;
+    p.cowling_resistivity = prm->cowling_resistivity;
+    p.f_bar = prm->f_bar; p.t_bar = prm->t_bar; p.r_bar = prm->r_bar; p.tr = prm->tr; p.eta_bar = prm->eta_bar;
+    run.pip = p.eos_number != LARE_EOS_IDEAL;
+    run.cowling = p.cowling_resistivity != 0;
     int bcs[6] = {prm->xbc_min, prm->xbc_max, prm->ybc_min, prm->ybc_max, prm->zbc_min, prm->zbc_max};
     for (int d = 0; d < 3; ++d) {
       p.bc[d][0] = bcs[2 * d];
@@ -200,6 +205,8 @@ class EngineT : public EngineBase {
     } else {
       // conduct_heat may still be called on its own; allocate lazily there.
     }
+    if (run.pip || run.cowling) all.push_back(&run.a.xi);
+    if (run.cowling) all.push_back(&run.a.eta_perp);
     for (A3<R>* x : all) {
       R* base = dalloc<R>(run.elems, err);
       if (!base) return LARE_ENOMEM;
@@ -209,6 +216,7 @@ class EngineT : public EngineBase {
       fill(*x, R(0));
     }
     fill(run.a.gamma_boris, R(1));
+    if (run.a.xi.p) fill(run.a.xi, (R)p.xi_n);  // the constant until neutral_fraction runs
     run.sc = dalloc<double>(SC_NSLOTS, err);
     run.us = dalloc<unsigned long long>(U_NSLOTS, err);
     size_t nb = (size_t)((nx + 5 + 63) / 64 + 1) * ((ny + 5 + 3) / 4 + 1) * (nz + 6);
@@ -306,6 +314,8 @@ class EngineT : public EngineBase {
     add("fy_visc", &run.a.fy_visc, 0, X, 0, Y, 0, Z);
     add("fz_visc", &run.a.fz_visc, 0, X, 0, Y, 0, Z);
     if (p.conduction) add("larsen_factor", &run.a.larsen, 0, X, 0, Y, 0, Z);
+    if (run.a.xi.p) add("xi_n", &run.a.xi, -1, X + 2, -1, Y + 2, -1, Z + 2);
+    if (run.a.eta_perp.p) add("eta_perp", &run.a.eta_perp, -1, X + 2, -1, Y + 2, -1, Z + 2);
     cudaError_t e = cudaStreamSynchronize(run.s);
     if (e != cudaSuccess) { err = cudaGetErrorString(e); return LARE_ECUDA; }
     return LARE_OK;
@@ -443,8 +453,30 @@ class EngineT : public EngineBase {
   int lagrangian_step(int step) override {
     int rc = lare::lagrangian_step(run, step);
     if (rc) return fail(rc, rc == LARE_EDT ? "dt underflow or non-finite dt" : "lagrangian_step failed");
+    if (run.pip) {
+      if ((rc = eos_error())) return rc;
+    }
     return cuda_check("lagrangian_step");
   }
+  // LARE_EEOS raised by a neutral_fraction launch (syncs)
+  int eos_error() {
+    if (pull_scalars(run) != cudaSuccess) return fail(LARE_ECUDA, "sync failed");
+    if ((int)run.host_sc[SC_ERROR] == LARE_EEOS)
+      return fail(LARE_EEOS, "neutral_fraction: temperature bounds problem (empty bracket)");
+    return LARE_OK;
+  }
+  int neutral_fraction() override {
+    if (!run.pip) return LARE_OK;
+    lare::neutral_fraction(run, run.a.energy);
+    int rc = eos_error();
+    return rc ? rc : cuda_check("neutral_fraction");
+  }
+  int perpendicular_resistivity() override {
+    if (!run.cowling) return fail(LARE_EINVAL, "perpendicular_resistivity: cowling_resistivity is off");
+    lare::perpendicular_resistivity(run);
+    return cuda_check("perpendicular_resistivity");
+  }
+  bool partially_ionised() const override { return run.pip; }
   int eulerian_remap(int step) override {
     lare::eulerian_remap(run, step);
     return cuda_check("eulerian_remap");
@@ -524,6 +556,7 @@ class EngineT : public EngineBase {
     run.capturing = true;
     int rc = LARE_OK;
     for (int k = 0; k < nsteps && rc == LARE_OK; ++k) {
+      if (run.pip) lare::neutral_fraction(run, run.a.energy);  // lare3d.f90:83
       rc = lare::lagrangian_step(run, first + k);
       if (rc == LARE_OK) lare::eulerian_remap(run, first + k);
       if (rc == LARE_OK) lare::eta_calc(run);
@@ -545,7 +578,7 @@ class EngineT : public EngineBase {
   int device_error() override {
     if (pull_scalars(run) != cudaSuccess) return fail(LARE_ECUDA, "device_error: sync failed");
     const int code = (int)run.host_sc[SC_ERROR];
-    if (code) fail(code, "raised on the device in a recorded step (bad dt or sub-cycle count)");
+    if (code) fail(code, "raised on the device in a recorded step (bad dt, sub-cycle count or EOS bracket)");
     return code;
   }
   int conduction_stages(double dt, int* n_stages) override {

@@ -73,13 +73,18 @@ struct EtaArgs {
   R* fy;
   R* fz;
   R* curlb;
+  const R* eta_perp;  // Cowling branch only
   A1<R> dxc, dyc, dzc;
   R jmax, eb, e0;
   int nx, ny, nz, sx, sxy;
   bool rkstep;
 };
 
-template <class R>
+// COW: rkstep's partially ionised branch (lagran.F90:1506-1575), which
+// splits the current into its parts along and across the vertex field and
+// adds eta_perp to the cross-field part.  The vertex field averages use the
+// same bx, by and bz values the current does.
+template <class R, bool COW>
 __global__ void __launch_bounds__(128) k_eta_march(EtaArgs<R> g) {
   // distinct arrays (no output is an input): restrict lets the compiler
   // hoist the next plane's loads above this plane's stores
@@ -121,10 +126,31 @@ __global__ void __launch_bounds__(128) k_eta_march(EtaArgs<R> g) {
     const R e = sqrt(j2) > g.jmax ? g.eb + g.e0 : g.eb;
     eta_r[c] = e;
     if (g.rkstep && inxy && iz >= 0 && iz <= g.nz) {
-      fx_r[c] = -jx * e * dxc * R(0.5);
-      fy_r[c] = -jy * e * dyc * R(0.5);
-      fz_r[c] = -jz * e * dzc * R(0.5);
-      curlb_r[c] = e * j2;
+      if constexpr (COW) {
+        const R bxv = (bx0 + bxy + bxz + bxyz) * R(0.25);
+        const R byv = (by0 + byx + byz + byxz) * R(0.25);
+        const R bzv = (bz0 + bzx + bzy + bzxy) * R(0.25);
+        const R magn_b = bxv * bxv + byv * byv + bzv * bzv;
+        R jpx = R(0), jpy = R(0), jpz = R(0);
+        if (magn_b > Num<R>::tiny()) {
+          jpx = (jx * bxv + jy * byv + jz * bzv) * bxv / magn_b;
+          jpy = (jx * bxv + jy * byv + jz * bzv) * byv / magn_b;
+          jpz = (jx * bxv + jy * byv + jz * bzv) * bzv / magn_b;
+        }
+        const R jqx = jx - jpx, jqy = jy - jpy, jqz = jz - jpz;
+        const R mpar = sqrt(jpx * jpx + jpy * jpy + jpz * jpz);
+        const R mperp = sqrt(jqx * jqx + jqy * jqy + jqz * jqz);
+        const R ep = g.eta_perp[c];
+        curlb_r[c] = e * (mpar * mpar) + (ep + e) * (mperp * mperp);
+        fx_r[c] = -((jpx + jqx) * e + jqx * ep) * dxc * R(0.5);
+        fy_r[c] = -((jpy + jqy) * e + jqy * ep) * dyc * R(0.5);
+        fz_r[c] = -((jpz + jqz) * e + jqz * ep) * dzc * R(0.5);
+      } else {
+        fx_r[c] = -jx * e * dxc * R(0.5);
+        fy_r[c] = -jy * e * dyc * R(0.5);
+        fz_r[c] = -jz * e * dzc * R(0.5);
+        curlb_r[c] = e * j2;
+      }
     }
     bx0 = bxz;
     bxy = bxyz;
@@ -165,6 +191,7 @@ void eta_and_rkstep(Run<R>& run, bool with_rkstep) {
   ga.fy = fyp;
   ga.fz = fzp;
   ga.curlb = curlb;
+  ga.eta_perp = run.a.eta_perp.p;
   ga.dxc = dxc;
   ga.dyc = dyc;
   ga.dzc = dzc;
@@ -179,7 +206,10 @@ void eta_and_rkstep(Run<R>& run, bool with_rkstep) {
   ga.rkstep = with_rkstep;
   dim3 grd((nx + 3 + 31) / 32, (ny + 3 + 3) / 4, (nz + 3 + kEtaZ - 1) / kEtaZ);
   const int k = run.prof_begin("eta_and_rkstep", 0, with_rkstep ? 8 : 4, (double)(nx + 3) * (ny + 3) * (nz + 3));
-  k_eta_march<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(ga);
+  if (with_rkstep && run.cowling)
+    k_eta_march<R, true><<<grd, dim3(32, 4, 1), 0, run.s>>>(ga);
+  else
+    k_eta_march<R, false><<<grd, dim3(32, 4, 1), 0, run.s>>>(ga);
   run.prof_end(k);
   ++run.launches;
 }
@@ -299,6 +329,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
   R* const cv_v = A.cv_v.p;
   R* const p_visc = A.p_visc.p;
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
+  const R* xin = run.pip ? A.xi.p : nullptr;  // per-cell xi_n (neutral.f90) or the constant
   // LP1
   LARE_BOXWH(run, 0, 4, 11, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
@@ -306,7 +337,8 @@ void prologue_and_shock_viscosity(Run<R>& run) {
     R by1 = (by[c] + by[c - sx]) * R(0.5);
     R bz1 = (bz[c] + bz[c - sxy]) * R(0.5);
     R r = rho[c];
-    R pr = (g - R(1)) * r * (energy[c] - (R(1) - xi) * ip);
+    const R x = xin ? xin[c] : xi;
+    R pr = (g - R(1)) * r * (energy[c] - (R(1) - x) * ip);
     pressure[c] = pr;
     R rmin = fmax(r, Num<R>::tiny());
     R b2 = bx1 * bx1 + by1 * by1 + bz1 * bz1;
@@ -446,9 +478,10 @@ void set_dt(Run<R>& run) {
   const R* vy = A.vy.p;
   const R* vz = A.vz.p;
   const R* eta = A.eta.p;
+  const R* eta_perp = A.eta_perp.p;
   R* const gamma_boris = A.gamma_boris.p;
   auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb;
-  const bool boris = run.p.boris != 0, resistive = run.p.resistive_mhd != 0;
+  const bool boris = run.p.boris != 0, resistive = run.p.resistive_mhd != 0, cowling = run.cowling;
   const R g = (R)run.p.gamma;
   const R va_max2 = (R)run.p.va_max * (R)run.p.va_max;
   if (!run.gamma_boris_one || boris) {
@@ -480,7 +513,10 @@ void set_dt(Run<R>& run) {
                  dzb(iz) / fmax(fabs(vz[c]), Num<R>::tiny()));
     dt_local = fmin(dt_local, dt2);
     R dt3 = Num<R>::huge();
-    if (resistive) {
+    if (cowling) {  // lagran.F90:1132-1134
+      R dxlocal = R(1) / (R(1) / (dxb(ix) * dxb(ix)) + R(1) / (dyb(iy) * dyb(iy)) + R(1) / (dzb(iz) * dzb(iz)));
+      dt3 = R(0.2) * dxlocal / fmax(fmax(eta[c], eta_perp[c]), Num<R>::tiny());
+    } else if (resistive) {
       R dxlocal = R(1) / (R(1) / (dxb(ix) * dxb(ix)) + R(1) / (dyb(iy) * dyb(iy)) + R(1) / (dzb(iz) * dzb(iz)));
       dt3 = R(0.2) * dxlocal / fmax(eta[c], Num<R>::tiny());
     }
@@ -701,6 +737,7 @@ void predictor_corrector_step(Run<R>& run) {
   const R* visc_heat = A.visc_heat.p;
   const bool cond = run.p.conduction != 0;
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
+  const R* xin = run.pip ? A.xi.p : nullptr;
   const double* sc = run.sc;
   LARE_BOXWH(run, 0, 4, 8, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
@@ -719,7 +756,8 @@ void predictor_corrector_step(Run<R>& run) {
       R dv = cv1[c] / cv[c] - R(1);
       R e1 = e - pressure[c] * dv / rho[c];
       e1 = e1 + visc_heat[c] * dt2 / rho[c];
-      pressure[c] = (e1 - (R(1) - xi) * ip) * (g - R(1)) * rho[c] * cv[c] / cv1[c];
+      const R x = xin ? xin[c] : xi;
+      pressure[c] = (e1 - (R(1) - x) * ip) * (g - R(1)) * rho[c] * cv[c] / cv1[c];
     }
   });
   // PC2 (0:n): vertex forces with the predicted B; half-step velocity
@@ -848,6 +886,15 @@ void predictor_corrector_step(Run<R>& run) {
 }
 
 // ---------------------------------------------------------------------
+// lagran.F90:147-148 in each resistive sub-cycle, after eta_calc (which
+// reads neither result, so it may follow them here, fused with rkstep).
+template <class R>
+void neutral_models(Run<R>& run) {
+  if (run.pip) neutral_fraction(run, run.a.energy);
+  if (run.cowling) perpendicular_resistivity(run);
+}
+
+// ---------------------------------------------------------------------
 // lagran.F90:135-150, the resistive sub-cycles, recorded into a CUDA graph:
 // the count is known only on the device, so the loop is a conditional WHILE
 // node whose body (eta + rkstep, bstep, ohmic heating) ends with a kernel
@@ -893,6 +940,7 @@ int resistive_subcycles_captured(Run<R>& run) {
     return LARE_ECUDA;
   cudaStream_t outer = run.s;
   run.s = run.s_body;
+  neutral_models(run);
   eta_and_rkstep(run, true);
   resistive_update(run);
   launch_scalar(run.s, run.launches, [=] __device__() {
@@ -935,6 +983,7 @@ int lagrangian_step(Run<R>& run, int step) {
     if (substeps > run.peak_substeps) run.peak_substeps = substeps;
     run.last_substeps = substeps;
     for (int i = 1; i <= substeps; ++i) {
+      neutral_models(run);
       eta_and_rkstep(run, true);
       resistive_update(run);
     }

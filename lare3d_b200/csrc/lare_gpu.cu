@@ -46,6 +46,10 @@ int lare_gpu_init(const lare_params* p, int nx, int ny, int nz, const double* dx
   for (int d = 0; d < 3; ++d)
     if ((bcs[2 * d] == LARE_BC_PERIODIC) != (bcs[2 * d + 1] == LARE_BC_PERIODIC)) return LARE_EINVAL;
   if (!(p->gamma > 1.0) || !(p->dt_multiplier > 0.0)) return LARE_EINVAL;
+  if (p->eos_number < 0 || p->eos_number > LARE_EOS_PI) return LARE_EINVAL;
+  if ((p->eos_number > LARE_EOS_IDEAL || p->cowling_resistivity) &&
+      !(p->f_bar > 0.0 && p->t_bar > 0.0 && p->r_bar > 0.0 && p->tr > 0.0 && p->eta_bar >= 0.0))
+    return LARE_EINVAL;  // the ionisation model's constants must be set
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return LARE_ECUDA;
   const double* m6[6] = {dxb, dxc, dyb, dyc, dzb, dzc};
@@ -99,9 +103,21 @@ int lare_gpu_boundary_conditions(lare_ctx* c) {
   return c->e->boundary_conditions();
 }
 
+int lare_gpu_neutral_fraction(lare_ctx* c) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->neutral_fraction();
+}
+
+int lare_gpu_perpendicular_resistivity(lare_ctx* c) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->perpendicular_resistivity();
+}
+
 int lare_gpu_step(lare_ctx* c, int step, double* time, double* dt) {
   if (guard(c)) return LARE_EINVAL;
-  int rc = c->e->lagrangian_step(step);
+  int rc = c->e->neutral_fraction();  // lare3d.f90:83 (a no-op under EOS_IDEAL)
+  if (rc) return rc;
+  rc = c->e->lagrangian_step(step);
   if (rc) return rc;
   if ((rc = c->e->eulerian_remap(step))) return rc;
   if ((rc = c->e->eta_calc())) return rc;
@@ -123,6 +139,7 @@ int lare_gpu_run(lare_ctx* c, int first_step, int nsteps, double t_end, int* ste
   // lare3d.f90:80-89
   while (!((done >= nsteps && nsteps >= 0) || s.time >= t_end)) {
     ++step;
+    if ((rc = c->e->neutral_fraction())) return rc;
     if ((rc = c->e->lagrangian_step(step))) return rc;
     if ((rc = c->e->eulerian_remap(step))) return rc;
     if ((rc = c->e->eta_calc())) return rc;

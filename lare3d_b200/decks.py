@@ -23,7 +23,7 @@ from typing import Optional
 
 import numpy as np
 
-from .abi import BC_OPEN, BC_PERIODIC, BC_USER, LareParams, State, default_params
+from .abi import BC_OPEN, BC_PERIODIC, BC_USER, EOS_ION, LareParams, State, default_params
 from .grid import grid
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -121,6 +121,85 @@ def open_blast(n: int = 64, b=(1.0 / math.sqrt(2.0), 1.0 / math.sqrt(2.0), 0.0),
     st["by"][...] = b[1]
     st["bz"][...] = b[2]
     return Deck("open_blast", p, n, n, n, m, st, nsteps=100)
+
+
+# Physical constants of shared_data.F90:36-57 (SI).
+_MU0 = 4.0e-7 * math.pi
+_KB = 1.3806488e-23
+_MH = 1.672621777e-27
+_ME = 9.10938291e-31
+_HP = 6.62606957e-34
+_CHI = 2.17870364e-18   # ionisation potential of hydrogen
+
+
+def neutral_constants(eos_number: int, B_norm: float = 0.1, L_norm: float = 1.0e6, rho_norm: float = 1.67e-4,
+                      mf: float = 1.2, sigma_in: float = 5.0e-19) -> dict:
+    """The ionisation model's constants as the reference holds them after
+    setup_neutral (neutral.f90:31-63) and normalise_transport
+    (normalise.f90:25-51), for the normalisation of control.f90:46-60."""
+    mbar = _MH * mf
+    f_bar = (2.0 * math.pi * (_ME / _HP) * (_KB / _HP)) ** 1.5
+    t_bar = _CHI / _KB
+    r_bar = 4.0 / mbar
+    eta_bar = 2.0 * mbar / (math.sqrt(16.0 * _KB / (math.pi * mbar)) * sigma_in)
+    pressure0 = B_norm ** 2 / _MU0
+    energy0 = pressure0 / rho_norm
+    v0 = math.sqrt(energy0)
+    temp_norm = (mbar / _KB) * energy0
+    t_bar = t_bar / temp_norm
+    r_bar = r_bar * rho_norm / temp_norm ** 1.5
+    eta_bar_0 = (_MU0 * L_norm * v0) * rho_norm ** 2 * math.sqrt(temp_norm) / B_norm ** 2
+    eta_bar = eta_bar / eta_bar_0
+    ionise_pot = _CHI / (energy0 * mbar) if eos_number == EOS_ION else 0.0
+    return dict(f_bar=f_bar, t_bar=t_bar, r_bar=r_bar, tr=6420.0 / temp_norm, eta_bar=eta_bar, ionise_pot=ionise_pot)
+
+
+def get_neutral(t_v, rho_v, c: dict):
+    """neutral.f90:140-153 in numpy (initial conditions only)."""
+    bof = 1.0 / (0.5 * c["f_bar"] * c["tr"] * np.sqrt(t_v)) * np.exp(
+        (0.25 * (t_v / c["tr"] - 1.0) + 1.0) * c["t_bar"] / t_v)
+    r = 0.5 * (-1.0 + np.sqrt(1.0 + c["r_bar"] * rho_v * bof))
+    return r / (1.0 + r)
+
+
+def partially_ionised(n: int = 32, eos_number: int = EOS_ION, cowling: bool = True, T0: float = 1.8,
+                      dT: float = 0.4, v0: float = 0.3, eta_bar: Optional[float] = None, **over) -> Deck:
+    """A partially ionised Orszag-Tang-type vortex on the periodic [0, 2pi]^3
+    (neutral.f90, eos_number EOS_ION or EOS_PI, optionally with Cowling
+    resistivity): uniform density 1, a temperature of T0 +- dT around a
+    normalised 1.8 (about 12,500 K under the default normalisation, where
+    hydrogen is some 5 % ionised at this density), and the energy set from
+    it as initial_conditions.f90:69-87 does.  The physical eta_bar of the
+    default normalisation makes eta_perp some 1e-8; pass a larger eta_bar
+    to give the Cowling terms weight."""
+    g = 5.0 / 3.0
+    c = neutral_constants(eos_number)
+    if eta_bar is not None:
+        c["eta_bar"] = eta_bar
+    p = default_params(gamma=g, visc1=0.1, visc2=0.5, dt_multiplier=0.8, resistive_mhd=1,
+                       eta_background=1.0e-3, eta0=0.0, j_max=1.0e10, eos_number=eos_number,
+                       cowling_resistivity=1 if cowling else 0, **c)
+    for k, v in over.items():
+        setattr(p, k, v)
+    L = 2.0 * math.pi
+    m = grid(n, n, n, (0.0, L), (0.0, L), (0.0, L))
+    st = State.zeros(n, n, n)
+    xc, yc, zc, xb, yb, zb = _coords(m, n, n, n)
+    ones_c = np.ones((n + 4, n + 4, n + 4))
+    T = (T0 + dT * np.sin(xc) * np.sin(yc) * np.cos(zc)) * ones_c
+    rho = ones_c.copy()
+    xi = get_neutral(T, rho, c)
+    st["rho"][...] = rho
+    st["energy"][...] = np.asfortranarray((T * (2.0 - xi) + (1.0 - xi) * p.ionise_pot * (g - 1.0)) / (g - 1.0))
+    ones_n = np.ones((n + 5, n + 5, n + 5))
+    st["vx"][...] = np.asfortranarray(-v0 * np.sin(zb) * ones_n)
+    st["vy"][...] = np.asfortranarray(v0 * np.sin(xb) * ones_n)
+    st["vz"][...] = np.asfortranarray(v0 * np.sin(yb) * ones_n)
+    s4 = 1.0 / math.sqrt(4.0 * math.pi)
+    st["bx"][...] = (-np.sin(m["zc"]) * s4)[None, None, :]
+    st["by"][...] = (np.sin(2.0 * m["xc"]) * s4)[:, None, None]
+    st["bz"][...] = (np.sin(m["yc"]) * s4)[None, :, None]
+    return Deck("partially_ionised", p, n, n, n, m, st, nsteps=20, info={"eos_number": eos_number})
 
 
 def _curl_edges(Ax, Ay, Az, m, n):

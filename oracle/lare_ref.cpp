@@ -96,6 +96,29 @@ const double none_zero = DBL_MIN;         // TINY(1.0_num), shared_data.F90:62
 const double largest_number = DBL_MAX;    // HUGE(1.0_num), shared_data.F90:63
 const double sixth = 1.0 / 6.0;           // shared_data.F90:64
 const double pow_c = 5.0 / 2.0;           // conduct.f90:27
+
+// The exponential of the ionisation model: Cody and Waite's reduction
+// x = k ln2 + r (ln 2 as a 33-bit head plus its tail), a Taylor polynomial
+// through r^13 by Horner's rule and a scaling by 2^k.  The reference calls
+// the Fortran EXP (the C library's exp); this one is within about 1 ulp of
+// the exact value and is used so that the checked library, which evaluates
+// the same operations, gives identical bits through the bisection.
+double cw_exp(double x) {
+  if (!(x == x)) return x;
+  if (x > 709.782712893384) return HUGE_VAL;
+  if (x < -745.1332191019412) return 0.0;
+  const double ln2_hi = 0x1.62e42fee00000p-1, ln2_lo = 0x1.a39ef35793c76p-33;
+  const double k = std::rint(x * 0x1.71547652b82fep+0);
+  const double r = (x - k * ln2_hi) - k * ln2_lo;
+  static const double c[] = {0x1.1eed8eff8d898p-29, 0x1.ae64567f544e4p-26, 0x1.27e4fb7789f5cp-22,
+                             0x1.71de3a556c734p-19, 0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-13,
+                             0x1.6c16c16c16c17p-10, 0x1.1111111111111p-7,  0x1.5555555555555p-5,
+                             0x1.5555555555555p-3,  0.5,                   1.0,
+                             1.0};
+  double q = 0x1.6124613a86d09p-33;  // 1/13!, then 1/12! ... 1/2!, 1, 1
+  for (double ci : c) q = q * r + ci;
+  return std::ldexp(q, (int)k);
+}
 const double min_b = 1.0e-10;             // conduct.f90:28
 
 }  // namespace
@@ -128,6 +151,10 @@ struct lare_ref {
   F3 r_db1, r_dc1, r_rho_v, r_rho_v1, r_rho1, r_dm, r_cv2, r_flux[3];
   // conduct.f90 temporaries.
   F3 larsen_factor, c_flux, Y[4], Lc_Y0;
+  // neutral.f90:37-44 (xi_n always exists in the reference; eta_perp with
+  // cowling_resistivity)
+  F3 xi_n, eta_perp;
+  bool eos_error = false;  // neutral.f90:171-174 'Temperature bounds problem'
 
   // shared_data scalars.
   double time = 0.0, dt = 0.0, dt2 = 0.0, dtr = 0.0;
@@ -178,6 +205,11 @@ struct lare_ref {
     for (int j = 0; j < 4; ++j) cell(Y[j]);
     Lc_Y0.alloc(1, N, 1, M, 1, L);
     gamma_boris.fill(1.0);
+    // xi_n = 0 (neutral.f90:38), or 1 for a neutral gas under EOS_IDEAL
+    // (lare3d.f90:72): the constant p.xi_n until neutral_fraction runs
+    cell(xi_n);
+    xi_n.fill(p.xi_n);
+    if (p.cowling_resistivity) cell(eta_perp);
 
     V[0] = &vx; V[1] = &vy; V[2] = &vz;
     V1[0] = &vx1; V1[1] = &vy1; V1[2] = &vz1;
@@ -194,7 +226,9 @@ struct lare_ref {
               {"bz1", &bz1}, {"alpha1", &alpha1}, {"alpha2", &alpha2},
               {"alpha3", &alpha3}, {"visc_heat", &visc_heat}, {"pressure", &pressure},
               {"rho_v", &rho_v}, {"cv_v", &cv_v}, {"fx_visc", &fx_visc},
-              {"fy_visc", &fy_visc}, {"fz_visc", &fz_visc}, {"larsen_factor", &larsen_factor}};
+              {"fy_visc", &fy_visc}, {"fz_visc", &fz_visc}, {"larsen_factor", &larsen_factor},
+              {"xi_n", &xi_n}};
+    if (p.cowling_resistivity) fields["eta_perp"] = &eta_perp;
   }
 
   // ------------------------------------------------------------------
@@ -564,13 +598,13 @@ struct lare_ref {
   void lagrangian_step(int step) {
     cur_step = step;
     const double g = p.gamma;
-    const double xi = p.xi_n, ip = p.ionise_pot;
+    const double ip = p.ionise_pot;
     box(-1, nx + 2, -1, ny + 2, -1, nz + 2, [&](int ix, int iy, int iz) {
       int ixm = ix - 1, iym = iy - 1, izm = iz - 1;
       bx1(ix, iy, iz) = (bx(ix, iy, iz) + bx(ixm, iy, iz)) * 0.5;
       by1(ix, iy, iz) = (by(ix, iy, iz) + by(ix, iym, iz)) * 0.5;
       bz1(ix, iy, iz) = (bz(ix, iy, iz) + bz(ix, iy, izm)) * 0.5;
-      pressure(ix, iy, iz) = (g - 1.0) * rho(ix, iy, iz) * (energy(ix, iy, iz) - (1.0 - xi) * ip);
+      pressure(ix, iy, iz) = (g - 1.0) * rho(ix, iy, iz) * (energy(ix, iy, iz) - (1.0 - xi_n(ix, iy, iz)) * ip);
     });
     box(-1, nx + 1, -1, ny + 1, -1, nz + 1, [&](int ix, int iy, int iz) {
       int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
@@ -599,6 +633,8 @@ struct lare_ref {
       dt = dt / (double)substeps;
       for (int sc = 1; sc <= substeps; ++sc) {
         eta_calc();
+        if (eos_number() != LARE_EOS_IDEAL) neutral_fraction(energy);  // :147
+        if (p.cowling_resistivity) perpendicular_resistivity();        // :148
         resistive_effects();
       }
       box(-1, nx + 2, -1, ny + 2, -1, nz + 2, [&](int ix, int iy, int iz) {
@@ -631,7 +667,7 @@ struct lare_ref {
 
   // lagran.F90:208-478
   void predictor_corrector_step() {
-    const double g = p.gamma, xi = p.xi_n, ip = p.ionise_pot;
+    const double g = p.gamma, ip = p.ionise_pot;
     bx0.d = bx.d; by0.d = by.d; bz0.d = bz.d;
 
     b_field_and_cv1_update();
@@ -641,7 +677,7 @@ struct lare_ref {
       double dv = cv1(ix, iy, iz) / cv(ix, iy, iz) - 1.0;
       double e1 = energy(ix, iy, iz) - pressure(ix, iy, iz) * dv / rho(ix, iy, iz);
       e1 = e1 + visc_heat(ix, iy, iz) * dt2 / rho(ix, iy, iz);
-      pressure(ix, iy, iz) = (e1 - (1.0 - xi) * ip) * (g - 1.0) * rho(ix, iy, iz) * cv(ix, iy, iz)
+      pressure(ix, iy, iz) = (e1 - (1.0 - xi_n(ix, iy, iz)) * ip) * (g - 1.0) * rho(ix, iy, iz) * cv(ix, iy, iz)
                            / cv1(ix, iy, iz);
     });
 
@@ -943,7 +979,10 @@ struct lare_ref {
           double dxlocal = 1.0 / (1.0 / (dxb(ix) * dxb(ix)) + 1.0 / (dyb(iy) * dyb(iy))
                                   + 1.0 / (dzb(iz) * dzb(iz)));
           double dt3 = largest_number;
-          if (p.resistive_mhd) dt3 = 0.2 * dxlocal / std::fmax(eta(ix, iy, iz), none_zero);
+          if (p.cowling_resistivity)  // :1132-1134
+            dt3 = 0.2 * dxlocal / std::fmax(std::fmax(eta(ix, iy, iz), eta_perp(ix, iy, iz)), none_zero);
+          else if (p.resistive_mhd)
+            dt3 = 0.2 * dxlocal / std::fmax(eta(ix, iy, iz), none_zero);
           dtr_local = std::fmin(dtr_local, dt3);
         }
     dt = p.dt_multiplier * dt_local;
@@ -1022,11 +1061,99 @@ struct lare_ref {
       double jz2 = (by(ixp, iy, izp) - by(ix, iy, izp)) / dxc(ix) - (bx(ix, iyp, izp) - bx(ix, iy, izp)) / dyc(iy);
       double jx = (jx1 + jx2) * 0.5, jy = (jy1 + jy2) * 0.5, jz = (jz1 + jz2) * 0.5;
       double e = eta(ix, iy, iz);
-      flux_x(ix, iy, iz) = -jx * e * dxc(ix) * 0.5;
-      flux_y(ix, iy, iz) = -jy * e * dyc(iy) * 0.5;
-      flux_z(ix, iy, iz) = -jz * e * dzc(iz) * 0.5;
-      curlb(ix, iy, iz) = e * (jx * jx + jy * jy + jz * jz);
+      if (!p.cowling_resistivity) {
+        flux_x(ix, iy, iz) = -jx * e * dxc(ix) * 0.5;
+        flux_y(ix, iy, iz) = -jy * e * dyc(iy) * 0.5;
+        flux_z(ix, iy, iz) = -jz * e * dzc(iz) * 0.5;
+        curlb(ix, iy, iz) = e * (jx * jx + jy * jy + jz * jz);
+        return;
+      }
+      // :1527-1572, the partially ionised branch
+      double bxv = (bx(ix, iy, iz) + bx(ix, iyp, iz) + bx(ix, iy, izp) + bx(ix, iyp, izp)) * 0.25;
+      double byv = (by(ix, iy, iz) + by(ixp, iy, iz) + by(ix, iy, izp) + by(ixp, iy, izp)) * 0.25;
+      double bzv = (bz(ix, iy, iz) + bz(ixp, iy, iz) + bz(ix, iyp, iz) + bz(ixp, iyp, iz)) * 0.25;
+      double magn_b = bxv * bxv + byv * byv + bzv * bzv;
+      double j_par_x = 0.0, j_par_y = 0.0, j_par_z = 0.0;
+      if (magn_b > none_zero) {
+        j_par_x = (jx * bxv + jy * byv + jz * bzv) * bxv / magn_b;
+        j_par_y = (jx * bxv + jy * byv + jz * bzv) * byv / magn_b;
+        j_par_z = (jx * bxv + jy * byv + jz * bzv) * bzv / magn_b;
+      }
+      double j_perp_x = jx - j_par_x, j_perp_y = jy - j_par_y, j_perp_z = jz - j_par_z;
+      double magn_j_par = std::sqrt(j_par_x * j_par_x + j_par_y * j_par_y + j_par_z * j_par_z);
+      double magn_j_perp = std::sqrt(j_perp_x * j_perp_x + j_perp_y * j_perp_y + j_perp_z * j_perp_z);
+      double ep = eta_perp(ix, iy, iz);
+      curlb(ix, iy, iz) = e * (magn_j_par * magn_j_par) + (ep + e) * (magn_j_perp * magn_j_perp);
+      flux_x(ix, iy, iz) = -((j_par_x + j_perp_x) * e + j_perp_x * ep) * dxc(ix) * 0.5;
+      flux_y(ix, iy, iz) = -((j_par_y + j_perp_y) * e + j_perp_y * ep) * dyc(iy) * 0.5;
+      flux_z(ix, iy, iz) = -((j_par_z + j_perp_z) * e + j_perp_z * ep) * dzc(iz) * 0.5;
     });
+  }
+
+  int eos_number() const { return p.eos_number == 0 ? LARE_EOS_IDEAL : p.eos_number; }
+
+  // neutral.f90:140-153
+  double get_neutral(double t_v, double rho_v) const {
+    double t_rad = p.tr, dilution = 0.5;
+    double bof = 1.0 / (dilution * p.f_bar * t_rad * std::sqrt(t_v))
+               * cw_exp((0.25 * (t_v / t_rad - 1.0) + 1.0) * p.t_bar / t_v);
+    double r = 0.5 * (-1.0 + std::sqrt(1.0 + p.r_bar * rho_v * bof));
+    return r / (1.0 + r);
+  }
+
+  // neutral.f90:158-195, on the energy-like array e
+  void neutral_fraction(F3& e) {
+    const double g = p.gamma, ip = p.ionise_pot;
+    box(-1, nx + 2, -1, ny + 2, -1, nz + 2, [&](int ix, int iy, int iz) {
+      double rho0 = rho(ix, iy, iz), e0 = e(ix, iy, iz);
+      double ta1 = (g - 1.0) * std::fmax((e0 - ip) / 2.0, none_zero), ta2 = (g - 1.0) * e0;
+      if (ta1 > ta2) {
+        eos_error = true;  // the reference prints and STOPs
+        return;
+      }
+      double dx = ta2 - ta1, t = ta1, x = ta1;
+      for (int loop = 1; loop <= 100; ++loop) {
+        dx = dx / 2.0;
+        x = t + dx;
+        double xi_a = get_neutral(x, rho0);
+        double fa = x - (g - 1.0) * (e0 - (1.0 - xi_a) * ip) / (2.0 - xi_a);
+        if (fa <= 0.0) t = x;
+        if (std::fabs(dx) < 1.e-8 || std::fabs(fa) < 1.e-8) break;
+      }
+      xi_n(ix, iy, iz) = get_neutral(x, rho0);
+    });
+  }
+
+  // neutral.f90:68-124 (bxv and byv take their z terms from bz, as written)
+  void perpendicular_resistivity() {
+    const double g = p.gamma, ip = p.ionise_pot;
+    box(0, nx, 0, ny, 0, nz, [&](int ix, int iy, int iz) {
+      int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
+      double rho_v = rho(ix, iy, iz) * cv(ix, iy, iz) + rho(ixp, iy, iz) * cv(ixp, iy, iz)
+                   + rho(ix, iyp, iz) * cv(ix, iyp, iz) + rho(ixp, iyp, iz) * cv(ixp, iyp, iz)
+                   + rho(ix, iy, izp) * cv(ix, iy, izp) + rho(ixp, iy, izp) * cv(ixp, iy, izp)
+                   + rho(ix, iyp, izp) * cv(ix, iyp, izp) + rho(ixp, iyp, izp) * cv(ixp, iyp, izp);
+      rho_v = rho_v / (cv(ix, iy, iz) + cv(ixp, iy, iz) + cv(ix, iyp, iz) + cv(ixp, iyp, iz)
+                       + cv(ix, iy, izp) + cv(ixp, iy, izp) + cv(ix, iyp, izp) + cv(ixp, iyp, izp));
+      double bxv = bx(ix, iy, iz) + bx(ix, iyp, iz) + bz(ix, iy, izp) + bz(ix, iyp, izp);
+      double byv = by(ix, iy, iz) + by(ixp, iy, iz) + bz(ix, iy, izp) + bz(ixp, iy, izp);
+      double bzv = bz(ix, iy, iz) + bz(ixp, iy, iz) + bz(ix, iyp, iz) + bz(ixp, iyp, iz);
+      bxv = 0.25 * bxv;
+      byv = 0.25 * byv;
+      bzv = 0.25 * bzv;
+      double bfieldsq = bxv * bxv + byv * byv + bzv * bzv;
+      double t_v = 0.0;
+      for (int iz2 = iz; iz2 <= iz + 1; ++iz2)
+        for (int iy2 = iy; iy2 <= iy + 1; ++iy2)
+          for (int ix2 = ix; ix2 <= ix + 1; ++ix2)
+            t_v = t_v + (energy(ix2, iy2, iz2) - (1.0 - xi_n(ix2, iy2, iz2)) * ip) / (2.0 - xi_n(ix2, iy2, iz2));
+      t_v = t_v * (g - 1.0) / 8.0;
+      double xi_v = get_neutral(t_v, rho_v);
+      double f = std::fmax(1.0 - xi_v, none_zero);
+      if (f > 0) eta_perp(ix, iy, iz) = p.eta_bar * xi_v / f * bfieldsq / (rho_v * rho_v) / std::sqrt(t_v);
+      else eta_perp(ix, iy, iz) = 0.0;
+    });
+    for (double& v : eta_perp.d) v = std::fmin(v, 100.0);  // :122
   }
 
   // lagran.F90:1582-1635
@@ -1381,8 +1508,9 @@ struct lare_ref {
   }
 
   void temperature_from(F3& e) {
-    const double g = p.gamma, xi = p.xi_n, ip = p.ionise_pot;
+    const double g = p.gamma, ip = p.ionise_pot;
     box(-1, nx + 2, -1, ny + 2, -1, nz + 2, [&](int ix, int iy, int iz) {
+      const double xi = xi_n(ix, iy, iz);
       temperature(ix, iy, iz) = (g - 1.0) / (2.0 - xi) * (e(ix, iy, iz) - (1.0 - xi) * ip);
     });
   }
@@ -1411,7 +1539,7 @@ struct lare_ref {
       for (int iy = 1; iy <= ny; ++iy)
         for (int ix = 1; ix <= nx; ++ix) {
           double kappa1 = k0 * larsen_factor(ix, iy, iz);
-          double temp = (g - 1.0) / (2.0 - xi) * (energy(ix, iy, iz) - (1.0 - xi) * ip);
+          double temp = (g - 1.0) / (2.0 - xi_n(ix, iy, iz)) * (energy(ix, iy, iz) - (1.0 - xi_n(ix, iy, iz)) * ip);
           double tp = std::pow(temp, pow_c);
           double r = rho(ix, iy, iz);
           double dt1 = r * (dxb(ix) * dxb(ix)) / (2.0 * kappa1 * tp);
@@ -1560,6 +1688,7 @@ struct lare_ref {
         Y[1].d = Y[2].d;
         energy.d = Y[3].d;
         energy_bcs();
+        if (eos_number() != LARE_EOS_IDEAL) neutral_fraction(energy);  // conduct.f90:404
         Y[2].d = energy.d;
         box(1, nx, 1, ny, 1, nz, [&](int ix, int iy, int iz) { Y[3](ix, iy, iz) = 0.0; });
       }
@@ -1630,6 +1759,7 @@ int lare_ref_init(const lare_params* params, int nx, int ny, int nz, const doubl
   if (!bc_ok(p.xbc_min) || !bc_ok(p.xbc_max) || !bc_ok(p.ybc_min) || !bc_ok(p.ybc_max) ||
       !bc_ok(p.zbc_min) || !bc_ok(p.zbc_max))
     return LARE_EINVAL;
+  if (p.eos_number < 0 || p.eos_number > LARE_EOS_PI) return LARE_EINVAL;
   lare_ref* r = new lare_ref();
   r->p = p;
   r->nx = nx; r->ny = ny; r->nz = nz;
@@ -1687,7 +1817,22 @@ int lare_ref_set_time(lare_ref* r, double time, double dt) {
 int lare_ref_lagrangian_step(lare_ref* r, int step) {
   if (!r) return LARE_EINVAL;
   r->lagrangian_step(step);
+  if (r->eos_error) return fail(r, LARE_EEOS, "Temperature bounds problem");
   if (!(r->dt > 0.0) || !std::isfinite(r->dt)) return fail(r, LARE_EDT, "dt underflow or non-finite");
+  return LARE_OK;
+}
+int lare_ref_neutral_fraction(lare_ref* r) {
+  if (!r) return LARE_EINVAL;
+  if (r->eos_number() == LARE_EOS_IDEAL) return LARE_OK;
+  r->neutral_fraction(r->energy);
+  if (r->eos_error) return fail(r, LARE_EEOS, "Temperature bounds problem");
+  return LARE_OK;
+}
+double lare_ref_exp(double x) { return cw_exp(x); }
+int lare_ref_perpendicular_resistivity(lare_ref* r) {
+  if (!r) return LARE_EINVAL;
+  if (!r->p.cowling_resistivity) return fail(r, LARE_EINVAL, "cowling_resistivity is off");
+  r->perpendicular_resistivity();
   return LARE_OK;
 }
 int lare_ref_eulerian_remap(lare_ref* r, int step) {
@@ -1706,7 +1851,9 @@ int lare_ref_boundary_conditions(lare_ref* r) {
   return LARE_OK;
 }
 int lare_ref_step(lare_ref* r, int step, double* time, double* dt) {
-  int rc = lare_ref_lagrangian_step(r, step);
+  int rc = lare_ref_neutral_fraction(r);  // lare3d.f90:83
+  if (rc) return rc;
+  rc = lare_ref_lagrangian_step(r, step);
   if (rc) return rc;
   r->eulerian_remap(step);
   r->eta_calc();

@@ -36,6 +36,10 @@ int lare_ref_lagrangian_step(lare_ref* r, int step);
 int lare_ref_eulerian_remap(lare_ref* r, int step);
 int lare_ref_eta_calc(lare_ref* r);
 int lare_ref_boundary_conditions(lare_ref* r);
+int lare_ref_neutral_fraction(lare_ref* r);
+int lare_ref_perpendicular_resistivity(lare_ref* r);
+/* the exponential the ionisation model uses (Cody-Waite + Taylor) */
+double lare_ref_exp(double x);
 int lare_ref_step(lare_ref* r, int step, double* time, double* dt);
 int lare_ref_conduct_heat(lare_ref* r, double dt, int* n_stages);
 int lare_ref_energy(lare_ref* r, double out[5]);

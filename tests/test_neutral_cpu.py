@@ -1,0 +1,139 @@
+"""The partially ionised plasma on the oracle (neutral.f90): its exponential,
+the neutral fraction's bisection, the Cowling resistivity against a numpy
+restatement, and properties of whole steps (mass conservation, the error a
+cell with no temperature bracket raises, the Cowling terms' extra heating)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import STATE
+from lare3d_b200 import decks
+from lare3d_b200.abi import EOS_ION, EOS_PI, LareError
+
+
+def _sim(d):
+    from oracle import oracle
+    s = oracle.simulation(d)
+    s.start(d.state)
+    return s
+
+
+def test_exponential_within_one_ulp_of_numpy():
+    from oracle import oracle
+    f = oracle.library().lare_ref_exp
+    f.argtypes = [C.c_double]
+    f.restype = C.c_double
+    rng = np.random.default_rng(5)
+    x = np.concatenate([rng.uniform(-745.0, 709.7, 20000), rng.uniform(-3.0, 3.0, 20000),
+                        rng.uniform(-1e-6, 1e-6, 2000), np.array([0.0, -0.0, 1.0, -1.0, 709.78, -745.13])])
+    got = np.array([f(float(v)) for v in x])
+    want = np.exp(x)
+    normal = want > np.finfo(np.float64).tiny
+    ulp = np.abs(got[normal] - want[normal]) / np.spacing(want[normal])
+    assert ulp.max() <= 1.0
+    assert np.all(np.abs(got[~normal] - want[~normal]) <= np.spacing(np.float64(0.0)))  # subnormal results
+    assert f(710.0) == np.inf and f(-746.0) == 0.0 and np.isnan(f(float("nan")))
+
+
+@pytest.mark.parametrize("eos", [EOS_ION, EOS_PI])
+def test_neutral_fraction_solves_the_equation_of_state(eos):
+    """xi_n = get_neutral(T, rho) with T = (gamma-1)(e - (1-xi_n) chi)/(2 - xi_n),
+    to the bisection's tolerance, over the whole cell array."""
+    d = decks.partially_ionised(10, eos_number=eos)
+    s = _sim(d)
+    xi = s.get_field("xi_n")
+    e = s.get_field("energy")
+    rho = s.get_field("rho")
+    p = d.params
+    T = (p.gamma - 1.0) / (2.0 - xi) * (e - (1.0 - xi) * p.ionise_pot)
+    c = decks.neutral_constants(eos)
+    assert np.all((xi > 0.5) & (xi < 1.0))
+    assert np.abs(xi - decks.get_neutral(T, rho, c)).max() < 1e-7
+
+
+def _eta_perp_numpy(s, p, n):
+    """neutral.f90:68-124 in numpy at the vertices 0:n."""
+    rho, cv, e, xi = (s.get_field(k) for k in ("rho", "cv", "energy", "xi_n"))
+    bx, by, bz = (s.get_field(k) for k in ("bx", "by", "bz"))
+    # cell arrays start at -1, bx at (-2, -1, -1), by at (-1, -2, -1), bz at (-1, -1, -2)
+    c = lambda a, i, j, k: a[1 + i:2 + n + i, 1 + j:2 + n + j, 1 + k:2 + n + k]
+    fx = lambda i, j, k: bx[2 + i:3 + n + i, 1 + j:2 + n + j, 1 + k:2 + n + k]
+    fy = lambda i, j, k: by[1 + i:2 + n + i, 2 + j:3 + n + j, 1 + k:2 + n + k]
+    fz = lambda i, j, k: bz[1 + i:2 + n + i, 1 + j:2 + n + j, 2 + k:3 + n + k]
+    o8 = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 0), (0, 0, 1), (1, 0, 1), (0, 1, 1), (1, 1, 1)]
+    rv = sum(c(rho, *o) * c(cv, *o) for o in o8) / sum(c(cv, *o) for o in o8)
+    bxv = 0.25 * (fx(0, 0, 0) + fx(0, 1, 0) + fz(0, 0, 1) + fz(0, 1, 1))
+    byv = 0.25 * (fy(0, 0, 0) + fy(1, 0, 0) + fz(0, 0, 1) + fz(1, 0, 1))
+    bzv = 0.25 * (fz(0, 0, 0) + fz(1, 0, 0) + fz(0, 1, 0) + fz(1, 1, 0))
+    tv = sum((c(e, *o) - (1.0 - c(xi, *o)) * p.ionise_pot) / (2.0 - c(xi, *o)) for o in o8) * (p.gamma - 1.0) / 8.0
+    cst = dict(f_bar=p.f_bar, t_bar=p.t_bar, r_bar=p.r_bar, tr=p.tr)
+    xv = decks.get_neutral(tv, rv, cst)
+    f = np.maximum(1.0 - xv, np.finfo(np.float64).tiny)
+    return np.minimum(p.eta_bar * xv / f * (bxv ** 2 + byv ** 2 + bzv ** 2) / rv ** 2 / np.sqrt(tv), 100.0)
+
+
+def test_perpendicular_resistivity_matches_numpy():
+    n = 10
+    d = decks.partially_ionised(n, eta_bar=1e-2)
+    s = _sim(d)
+    ep = s.get_field("eta_perp")[1:n + 2, 1:n + 2, 1:n + 2]
+    want = _eta_perp_numpy(s, d.params, n)
+    assert want.max() > 1e-3
+    assert np.allclose(ep, want, rtol=1e-12, atol=0.0)
+
+
+@pytest.mark.parametrize("eos", [EOS_ION, EOS_PI])
+def test_steps_conserve_mass_and_stay_finite(eos):
+    n = 10
+    d = decks.partially_ionised(n, eos_number=eos, eta_bar=1e-2)
+    s = _sim(d)
+    inner = (slice(2, n + 2),) * 3
+    m0 = np.sum(s.get_field("rho")[inner] * s.get_field("cv")[inner])
+    for k in range(1, 5):
+        s.step(k)
+    st = s.download()
+    for f in STATE:
+        assert np.isfinite(st[f]).all(), f
+    m1 = np.sum(s.get_field("rho")[inner] * s.get_field("cv")[inner])
+    assert abs(m1 - m0) <= 1e-12 * m0
+    xi = s.get_field("xi_n")
+    assert np.all((xi > 0.5) & (xi < 1.0))
+
+
+def test_cowling_terms_add_heating():
+    """eta_perp >= 0 adds (eta_perp + eta) |j_perp|^2 - eta |j_perp|^2 to
+    the ohmic heating (lagran.F90:1564-1565)."""
+    out = []
+    for cow in (False, True):
+        d = decks.partially_ionised(10, cowling=cow, eta_bar=1e-2)
+        s = _sim(d)
+        for k in range(1, 3):
+            s.step(k)
+        out.append(s.scalars().total_ohmic_heating)
+    assert out[1] > out[0] > 0.0
+
+
+@pytest.mark.parametrize("eos", [EOS_ION, EOS_PI])
+def test_empty_temperature_bracket_is_an_error(eos):
+    """A cell with negative energy has no temperature bracket: the reference
+    stops (neutral.f90:171-174); the call returns LARE_EEOS."""
+    d = decks.partially_ionised(8, eos_number=eos)
+    d.state["energy"][5, 5, 5] = -1.0
+    from oracle import oracle
+    s = oracle.simulation(d)
+    with pytest.raises(LareError) as ei:
+        s.start(d.state)
+    assert ei.value.code == -9
+
+
+def test_ideal_eos_code_zero_is_ideal():
+    """eos_number 0 (a zero-initialised struct) reads as EOS_IDEAL."""
+    a = decks.blast(8)
+    b = decks.blast(8, eos_number=0)
+    ra, rb = _sim(a), _sim(b)
+    for k in range(1, 3):
+        ra.step(k)
+        rb.step(k)
+    for f in STATE:
+        assert np.array_equal(ra.get_field(f), rb.get_field(f)), f
