@@ -97,6 +97,14 @@ typedef struct lare_params {
   int eos_number;          /* LARE_EOS_* (control.f90:191) */
   int cowling_resistivity; /* control.f90:162 */
   double f_bar, t_bar, r_bar, tr, eta_bar;
+  /*
+   * Optically thin radiative losses (radiative.f90:98-208, lagran.F90:174-
+   * 178): Townsend's exact integration of the reference's default piecewise
+   * power-law loss function.  temp_norm and time_norm are normalise.f90's
+   * (:32-34); rho_norm and mf are control.f90's (:46, :60).
+   */
+  int radiation;
+  double temp_norm, time_norm, rho_norm, mf;
 } lare_params;
 
 /* Scalars of shared_data that the step updates. */

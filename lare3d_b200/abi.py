@@ -72,6 +72,11 @@ class LareParams(C.Structure):
         ("r_bar", C.c_double),
         ("tr", C.c_double),
         ("eta_bar", C.c_double),
+        ("radiation", C.c_int),
+        ("temp_norm", C.c_double),
+        ("time_norm", C.c_double),
+        ("rho_norm", C.c_double),
+        ("mf", C.c_double),
     ]
 
 
@@ -119,6 +124,8 @@ def default_params(**kw) -> LareParams:
         setattr(p, s, BC_PERIODIC)
     p.eos_number = EOS_IDEAL
     p.cowling_resistivity = 0
+    p.radiation = 0
+    p.mf = 1.2
     for k, v in kw.items():
         if not hasattr(p, k):
             raise KeyError(k)

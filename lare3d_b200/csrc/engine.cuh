@@ -35,6 +35,8 @@ struct Par {
   int resistive_mhd, conduction, heat_flux_limiter, use_viscous_damping, boris, restart;
   int eos_number, cowling_resistivity;                 // neutral.f90 (eos_number 0 read as EOS_IDEAL)
   double f_bar, t_bar, r_bar, tr, eta_bar;
+  int radiation;                                       // radiative.f90
+  double temp_norm, time_norm, rho_norm, mf;
   int bc[3][2];   // [dim][0=min,1=max]
   bool per[3];    // periodic communicator in this dimension (mpi_routines.F90:195-210)
 };
@@ -56,6 +58,8 @@ struct Arrays {
   A3<R> kf[9];                        // stage-invariant face coefficients, 3 per face direction
   // neutral.f90 (allocated only for a partially ionised run)
   A3<R> xi, eta_perp;
+  // the energy after rad_losses (radiative.f90), allocated with radiation on
+  A3<R> erad;
   // 1-D metrics (pointers at Fortran index 0)
   A1<R> dxb, dxc, dyb, dyc, dzb, dzc, grav;
   // reciprocals for conduction: 1/dxb, 1/dxc, 1/(dxc(i) + dxc(i-1)), per axis
@@ -486,6 +490,7 @@ void copy_whole(Run<R>& run, A3<R> dst, A3<R> src) {
 }  // namespace lare
 
 #include "neutral.cuh"
+#include "radiative.cuh"
 #include "conduct.cuh"
 
 namespace lare {

@@ -167,6 +167,8 @@ class EngineT : public EngineBase {
     p.eos_number = prm->eos_number == 0 ? LARE_EOS_IDEAL : prm->eos_number;
     p.cowling_resistivity = prm->cowling_resistivity;
     p.f_bar = prm->f_bar; p.t_bar = prm->t_bar; p.r_bar = prm->r_bar; p.tr = prm->tr; p.eta_bar = prm->eta_bar;
+    p.radiation = prm->radiation;
+    p.temp_norm = prm->temp_norm; p.time_norm = prm->time_norm; p.rho_norm = prm->rho_norm; p.mf = prm->mf;
     run.pip = p.eos_number != LARE_EOS_IDEAL;
     run.cowling = p.cowling_resistivity != 0;
     int bcs[6] = {prm->xbc_min, prm->xbc_max, prm->ybc_min, prm->ybc_max, prm->zbc_min, prm->zbc_max};
@@ -207,6 +209,7 @@ class EngineT : public EngineBase {
     }
     if (run.pip || run.cowling) all.push_back(&run.a.xi);
     if (run.cowling) all.push_back(&run.a.eta_perp);
+    if (p.radiation) all.push_back(&run.a.erad);
     for (A3<R>* x : all) {
       R* base = dalloc<R>(run.elems, err);
       if (!base) return LARE_ENOMEM;

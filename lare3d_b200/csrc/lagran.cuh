@@ -736,6 +736,7 @@ void predictor_corrector_step(Run<R>& run) {
   const R* rho = A.rho.p;
   const R* visc_heat = A.visc_heat.p;
   const bool cond = run.p.conduction != 0;
+  const R* erad = run.p.radiation ? A.erad.p : nullptr;  // the energy after rad_losses
   const R g = (R)run.p.gamma, xi = (R)run.p.xi_n, ip = (R)run.p.ionise_pot;
   const R* xin = run.pip ? A.xi.p : nullptr;
   const double* sc = run.sc;
@@ -745,6 +746,11 @@ void predictor_corrector_step(Run<R>& run) {
     if (cond) {
       R e0 = energy0[c];
       R d = energy[c] - e0;
+      if (erad) d = d + (erad[c] - e0);
+      e = e0 + d;
+    } else if (erad) {
+      R e0 = energy[c];
+      R d = R(0) + (erad[c] - e0);
       e = e0 + d;
     } else {
       e = energy[c] + R(0);
@@ -999,6 +1005,9 @@ int lagrangian_step(Run<R>& run, int step) {
     run.n_s_stages = ns;
     heat_conduct_sts2(run, SC_DT);
   }
+  // lagran.F90:174-178: rad_losses on the energy before conduction (energy0
+  // when conduction ran, else the energy itself); PC1 adds the two deltas
+  if (run.p.radiation) rad_losses(run, run.a.erad, run.p.conduction ? run.a.energy0 : run.a.energy, SC_DT);
   predictor_corrector_step(run);
   end_of_step_bcs(run);
   ++run.steps_taken;

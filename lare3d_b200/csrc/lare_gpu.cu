@@ -50,6 +50,8 @@ int lare_gpu_init(const lare_params* p, int nx, int ny, int nz, const double* dx
   if ((p->eos_number > LARE_EOS_IDEAL || p->cowling_resistivity) &&
       !(p->f_bar > 0.0 && p->t_bar > 0.0 && p->r_bar > 0.0 && p->tr > 0.0 && p->eta_bar >= 0.0))
     return LARE_EINVAL;  // the ionisation model's constants must be set
+  if (p->radiation && !(p->temp_norm > 0.0 && p->time_norm > 0.0 && p->rho_norm > 0.0 && p->mf > 0.0))
+    return LARE_EINVAL;  // radiative losses need the normalisation
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return LARE_ECUDA;
   const double* m6[6] = {dxb, dxc, dyb, dyc, dzb, dzc};

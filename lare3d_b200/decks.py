@@ -202,6 +202,33 @@ def partially_ionised(n: int = 32, eos_number: int = EOS_ION, cowling: bool = Tr
     return Deck("partially_ionised", p, n, n, n, m, st, nsteps=20, info={"eos_number": eos_number})
 
 
+def normalisation(B_norm: float = 0.1, L_norm: float = 1.0e6, rho_norm: float = 1.67e-4, mf: float = 1.2) -> dict:
+    """temp_norm and time_norm as normalise_transport forms them
+    (normalise.f90:25-34), with rho_norm and mf, for lare_params."""
+    mbar = _MH * mf
+    energy0 = (B_norm ** 2 / _MU0) / rho_norm
+    return dict(temp_norm=(mbar / _KB) * energy0, time_norm=L_norm / math.sqrt(energy0), rho_norm=rho_norm, mf=mf)
+
+
+def radiative_blast(n: int = 16, rho_norm: float = 1.0e-11, **over) -> Deck:
+    """The blast deck with optically thin radiative losses on
+    (radiative.f90) under a coronal normalisation (B_norm 1e-3 T,
+    L_norm 1e6 m): the ambient pressure rises along x so that the ambient
+    temperature sweeps the loss table's bands from 3.5e4 K to 3.5e6 K, and
+    the hot core (above the table's 1e7 K) is left alone, as the reference
+    leaves it."""
+    d = blast(n, radiation=1, **normalisation(B_norm=1.0e-3, L_norm=1.0e6, rho_norm=rho_norm))
+    for k, v in over.items():
+        setattr(d.params, k, v)
+    g = d.params.gamma
+    xc, yc, zc, *_ = _coords(d.metrics, n, n, n)
+    r = np.sqrt((xc - 0.5) ** 2 + (yc - 0.5) ** 2 + (zc - 0.5) ** 2)
+    pres = np.where(r < 0.1, 10.0, 0.1 * xc ** 2 + 0.001) * np.ones((n + 4, n + 4, n + 4))
+    d.state["energy"][...] = np.asfortranarray(pres / (g - 1.0))
+    d.name = "radiative_blast"
+    return d
+
+
 def _curl_edges(Ax, Ay, Az, m, n):
     """Discrete curl of periodic edge fields onto the face arrays.
 

@@ -654,6 +654,11 @@ struct lare_ref {
       for (size_t q = 0; q < energy.size(); ++q) delta_energy.d[q] = energy.d[q] - energy0.d[q];
       energy.d = energy0.d;
     }
+    if (p.radiation) {
+      rad_losses();
+      for (size_t q = 0; q < energy.size(); ++q) delta_energy.d[q] = delta_energy.d[q] + (energy.d[q] - energy0.d[q]);
+      energy.d = energy0.d;
+    }
     for (size_t q = 0; q < energy.size(); ++q) energy.d[q] = energy0.d[q] + delta_energy.d[q];
     for (size_t q = 0; q < energy.size(); ++q) energy.d[q] = fmax0(energy.d[q]);
 
@@ -1091,6 +1096,85 @@ struct lare_ref {
   }
 
   int eos_number() const { return p.eos_number == 0 ? LARE_EOS_IDEAL : p.eos_number; }
+
+  // radiative.f90:38-62 setup_loss_function and :180-208
+  // set_exact_integration_arrays (n = 7 boundaries, kmax = 6 bands)
+  struct Rad {
+    double t_boundary[8], pow[7], psi[7], yk[8], qk[8], ratios[8];
+    int alpha[7];
+    double cool, ratio;
+  };
+  Rad rad;
+  bool rad_first_call = true;
+  void setup_radiation() {
+    const int n = 7, kmax = 6;
+    const double tb[] = {0.02, 0.0398, 0.0794, 0.251, 0.562, 1.995, 10.0};
+    for (int i = 1; i <= n; ++i) rad.t_boundary[i] = tb[i - 1] * 1e6;
+    const double frac = -2.0 / 3.0;
+    const int al[] = {0, 2, 0, -2, 0, 0};
+    const double ex[] = {0.0, 0.0, 0.0, 0.0, 0.0, frac};
+    const double ps[] = {-21.85, -31.0, -21.2, -10.4, -21.94, -17.73};
+    for (int k = 1; k <= kmax; ++k) {
+      rad.alpha[k] = al[k - 1];
+      rad.pow[k] = (double)al[k - 1] + ex[k - 1];
+      rad.psi[k] = 1.e-13 * std::pow(10.0, ps[k - 1]);
+    }
+    for (int k = 1; k <= kmax; ++k) rad.qk[k] = rad.psi[k] * std::pow(rad.t_boundary[k], rad.pow[k]);
+    rad.qk[n] = rad.qk[n - 1] * std::pow(rad.t_boundary[n] / rad.t_boundary[n - 1], rad.pow[n - 1]);
+    rad.ratio = rad.qk[n] / rad.t_boundary[n];
+    const double kb_si = 1.3806488e-23, mh_si = 1.672621777e-27;
+    rad.cool = 0.5 * rad.ratio * (p.gamma - 1.0) * p.rho_norm / (kb_si * p.mf * mh_si);
+    for (int k = 1; k <= n; ++k) rad.ratios[k] = rad.ratio * (rad.t_boundary[k] / rad.qk[k]);
+    rad.yk[n] = 0.0;
+    for (int k = kmax; k >= 1; --k) {
+      if (rad.alpha[k] != 1) {
+        double fac = 1.0 / (1.0 - rad.pow[k]);
+        rad.yk[k] = rad.yk[k + 1]
+                  - fac * rad.ratios[k] * (1.0 - std::pow(rad.t_boundary[k] / rad.t_boundary[k + 1], rad.pow[k] - 1.0));
+      } else {
+        rad.yk[k] = rad.yk[k + 1] - rad.ratios[k] * std::log(rad.t_boundary[k] / rad.t_boundary[k + 1]);
+      }
+    }
+  }
+
+  // radiative.f90:98-176 rad_losses / exact_intergation_method
+  void rad_losses() {
+    if (rad_first_call) { rad_first_call = false; setup_radiation(); }
+    const int kmax = 6;
+    const double g = p.gamma;
+    box(1, nx, 1, ny, 1, nz, [&](int ix, int iy, int iz) {
+      double temp_si = 0.5 * p.temp_norm * energy(ix, iy, iz) * (g - 1.0);
+      int k = -1;
+      for (int i = 1; i <= kmax; ++i)
+        if (temp_si > rad.t_boundary[i] && temp_si <= rad.t_boundary[i + 1]) { k = i; break; }
+      if (k < 0) return;
+      double yt;
+      if (rad.alpha[k] != 1) {
+        double fac = 1.0 / (1.0 - rad.pow[k]);
+        yt = rad.yk[k] + fac * rad.ratios[k] * (1.0 - std::pow(rad.t_boundary[k] / temp_si, rad.pow[k] - 1.0));
+      } else {
+        yt = rad.yk[k] + rad.ratios[k] * std::log(rad.t_boundary[k] / temp_si);
+      }
+      double inverse_t_cool = rad.cool * rho(ix, iy, iz);
+      yt = yt + dt * inverse_t_cool * p.time_norm;
+      k = -1;
+      for (int i = 1; i <= kmax; ++i)
+        if ((yt > rad.yk[i] && yt <= rad.yk[i + 1]) || (yt < rad.yk[i] && yt >= rad.yk[i + 1])) { k = i; break; }
+      if (k < 0) {
+        temp_si = rad.t_boundary[1];
+        energy(ix, iy, iz) = temp_si * 2.0 / (g - 1.0) / p.temp_norm;
+        return;
+      }
+      if (rad.alpha[k] != 1) {
+        double fac = 1.0 / (1.0 - rad.pow[k]);
+        temp_si = rad.t_boundary[k] * std::pow(1.0 - (1.0 - rad.pow[k]) / rad.ratios[k] * (yt - rad.yk[k]), fac);
+      } else {
+        temp_si = rad.t_boundary[k] * std::exp((yt - rad.yk[k]) / rad.ratios[k]);
+      }
+      energy(ix, iy, iz) = temp_si * 2.0 / (g - 1.0) / p.temp_norm;
+    });
+    energy_bcs();
+  }
 
   // neutral.f90:140-153
   double get_neutral(double t_v, double rho_v) const {

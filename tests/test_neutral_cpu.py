@@ -137,3 +137,51 @@ def test_ideal_eos_code_zero_is_ideal():
         rb.step(k)
     for f in STATE:
         assert np.array_equal(ra.get_field(f), rb.get_field(f)), f
+
+
+# ---------------------------------------------------------------------
+# Optically thin radiation (radiative.f90), in the same file because it is
+# the other per-cell energy source of lagran.F90:168-181.
+
+def test_radiative_losses_constant_band_closed_form():
+    """A static uniform plasma in a band where Q(T) is constant (pow = 0,
+    0.562-1.995 MK) cools linearly: Townsend's exact step reduces to
+    T' = T - dt time_norm (gamma-1)/2 rho rho_norm psi / (kb mf mh)."""
+    from lare3d_b200.abi import State
+    n = 8
+    d = decks.radiative_blast(n, rho_norm=1.0e-9)
+    p = d.params
+    g = p.gamma
+    T = 1.0e6
+    e = T * 2.0 / (g - 1.0) / p.temp_norm
+    st = State.zeros(n, n, n)
+    st["rho"][...] = 1.0
+    st["energy"][...] = e
+    d.state = st
+    s = _sim(d)
+    _, dt = s.step(1)
+    psi = 1e-13 * 10.0 ** -21.94
+    kb, mh = 1.3806488e-23, 1.672621777e-27
+    T1 = T - dt * p.time_norm * 0.5 * (g - 1.0) * 1.0 * p.rho_norm * psi / (kb * p.mf * mh)
+    got = s.get_field("energy")[2:n + 2, 2:n + 2, 2:n + 2]
+    want = T1 * 2.0 / (g - 1.0) / p.temp_norm
+    assert T1 < 0.99 * T                     # a visible loss
+    assert np.allclose(got, want, rtol=1e-9, atol=0.0)
+
+
+def test_radiative_losses_cool_only_inside_the_table():
+    """Cells below 2e4 K or above 1e7 K are left unchanged (the reference's
+    CYCLE); cells inside lose energy, none gains."""
+    n = 12
+    d = decks.radiative_blast(n)
+    d0 = decks.radiative_blast(n, radiation=0)
+    s, s0 = _sim(d), _sim(d0)
+    s.step(1)
+    s0.step(1)
+    e, e0 = s.get_field("energy"), s0.get_field("energy")
+    p = d.params
+    T = 0.5 * p.temp_norm * d.state["energy"] * (p.gamma - 1.0)
+    inner = (slice(2, n + 2),) * 3
+    inside = ((T > 2e4) & (T <= 1e7))[inner]
+    assert np.all(e[inner] <= e0[inner] + 1e-15)
+    assert np.all(e[inner][inside] < e0[inner][inside])

@@ -111,3 +111,30 @@ def test_open_boundaries_with_conduction(built):
         for f in STATE:
             assert rel_l2(g.get_field(f), r.get_field(f)) <= 1e-12, (s, f)
     assert r.scalars().n_s_stages >= 3
+
+
+@pytest.mark.parametrize("cond", [0, 1])
+def test_radiative_losses(built, cond):
+    """Optically thin radiation (radiative.f90) alone and next to
+    conduction (lagran.F90:168-181 adds both energy changes to energy0).
+    The band powers come from pow(), so the bar is 1e-12 as for conduction."""
+    d = decks.radiative_blast(16, conduction=cond, kappa_0=2.0e-2)
+    r, g = pair(d)
+    for s in range(1, 4):
+        r.step(s)
+        g.step(s)
+        for f in STATE:
+            assert rel_l2(g.get_field(f), r.get_field(f)) <= 1e-12, (s, f)
+    if cond:
+        assert r.scalars().n_s_stages == g.scalars().n_s_stages >= 3
+
+
+def test_radiative_losses_fp32(built):
+    d = decks.radiative_blast(16)
+    r, g = pair(d, precision=32)
+    for s in range(1, 6):
+        r.step(s)
+        g.step(s)
+    for f in STATE:
+        e = rel_l2(g.get_field(f), r.get_field(f))
+        assert e <= 1e-5, f"{f}: rel L2 {e:.2e}"
