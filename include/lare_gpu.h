@@ -105,6 +105,12 @@ typedef struct lare_params {
    */
   int radiation;
   double temp_norm, time_norm, rho_norm, mf;
+  /*
+   * rke (control.f90): the momentum remap records the kinetic energy it
+   * loses per cell ([xyz]remap.f90, x_momx_flux :664-695 and siblings) and
+   * energy_correction returns it to the internal energy after the remap.
+   */
+  int rke;
 } lare_params;
 
 /* Scalars of shared_data that the step updates. */
@@ -160,6 +166,14 @@ int lare_gpu_lagrangian_step(lare_ctx* ctx, int step);
 /* remap.f90:33 eulerian_remap(step): Strang-permuted x/y/z remap + bfield_bcs. */
 int lare_gpu_eulerian_remap(lare_ctx* ctx, int step);
 
+/*
+ * diagnostics.F90:613 energy_correction: delta_ke (recorded by the last
+ * eulerian_remap) into the energy of cells 1:n, then energy_bcs.
+ * LARE_EINVAL unless rke.  lare_gpu_step and lare_gpu_run call it after the
+ * remap (lare3d.f90:86).
+ */
+int lare_gpu_energy_correction(lare_ctx* ctx);
+
 /* lagran.F90:1176 eta_calc. */
 int lare_gpu_eta_calc(lare_ctx* ctx);
 
@@ -186,7 +200,8 @@ int lare_gpu_perpendicular_resistivity(lare_ctx* ctx);
 
 /*
  * One timestep of the driver loop (lare3d.f90:83-87): neutral_fraction
- * (unless EOS_IDEAL), lagrangian_step, eulerian_remap(step), eta_calc.  time/dt (may be NULL) receive the
+ * (unless EOS_IDEAL), lagrangian_step, eulerian_remap(step),
+ * energy_correction (with rke), eta_calc.  time/dt (may be NULL) receive the
  * updated clock.
  */
 int lare_gpu_step(lare_ctx* ctx, int step, double* time, double* dt);

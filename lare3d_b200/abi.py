@@ -77,6 +77,7 @@ class LareParams(C.Structure):
         ("time_norm", C.c_double),
         ("rho_norm", C.c_double),
         ("mf", C.c_double),
+        ("rke", C.c_int),
     ]
 
 
@@ -125,6 +126,7 @@ def default_params(**kw) -> LareParams:
     p.eos_number = EOS_IDEAL
     p.cowling_resistivity = 0
     p.radiation = 0
+    p.rke = 0
     p.mf = 1.2
     for k, v in kw.items():
         if not hasattr(p, k):
@@ -244,6 +246,7 @@ class Binding:
         if hasattr(lib, prefix + "neutral_fraction"):
             f("neutral_fraction", [C.c_void_p])
             f("perpendicular_resistivity", [C.c_void_p])
+            f("energy_correction", [C.c_void_p])
         if hasattr(lib, prefix + "run"):
             f("run", [C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_int), dp, dp])
         if hasattr(lib, prefix + "launch_count"):
@@ -340,6 +343,9 @@ class Simulation:
 
     def boundary_conditions(self):
         self.b.call(self.ctx, "boundary_conditions")
+
+    def energy_correction(self):
+        self.b.call(self.ctx, "energy_correction")
 
     def neutral_fraction(self):
         self.b.call(self.ctx, "neutral_fraction")

@@ -36,6 +36,7 @@ struct Par {
   int eos_number, cowling_resistivity;                 // neutral.f90 (eos_number 0 read as EOS_IDEAL)
   double f_bar, t_bar, r_bar, tr, eta_bar;
   int radiation;                                       // radiative.f90
+  int rke;                                             // the remap's kinetic-energy correction
   double temp_norm, time_norm, rho_norm, mf;
   int bc[3][2];   // [dim][0=min,1=max]
   bool per[3];    // periodic communicator in this dimension (mpi_routines.F90:195-210)
@@ -60,6 +61,9 @@ struct Arrays {
   A3<R> xi, eta_perp;
   // the energy after rad_losses (radiative.f90), allocated with radiation on
   A3<R> erad;
+  // rke: the remap's kinetic-energy defect (shared_data.F90:108) and the
+  // three momentum fluxes before their product with dm
+  A3<R> delta_ke, rke_f[3];
   // 1-D metrics (pointers at Fortran index 0)
   A1<R> dxb, dxc, dyb, dyc, dzb, dzc, grav;
   // reciprocals for conduction: 1/dxb, 1/dxc, 1/(dxc(i) + dxc(i-1)), per axis
@@ -656,6 +660,10 @@ void eulerian_remap(Run<R>& run, int step) {
   R* const bz = run.a.bz.p;
   auto dxb = run.a.dxb, dyb = run.a.dyb, dzb = run.a.dzb;
   int pass[3] = {1, 1, 1};
+  if (run.p.rke) {  // remap.f90:38
+    R* const dke = run.a.delta_ke.p;
+    LARE_BOXW(run, 1, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) { dke[ix + sx * iy + sxy * iz] = R(0); });
+  }
   // B -> flux (remap.f90:43-69), including the -2 layers.
   LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
@@ -732,6 +740,27 @@ void energy_account(Run<R>& run) {
     if (iz == 0 || iz == nz) w1 = w1 * 0.5;
     v[0] = w1 * 0.5;
   }, SC_EN_KE, false);
+}
+
+}  // namespace lare
+
+namespace lare {
+
+// diagnostics.F90:613-629 energy_correction, after eulerian_remap when rke
+// is on (lare3d.f90:86): the kinetic energy the remap lost, where it lost
+// some, goes into the internal energy of cells 1:n; then energy_bcs.
+template <class R>
+void energy_correction(Run<R>& run) {
+  const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
+  auto dke = run.a.delta_ke, rho = run.a.rho, cv = run.a.cv, energy = run.a.energy;
+  LARE_BOXW(run, 5, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
+    R d = -dke(ix, iy, iz);
+    if (d < R(0)) d = R(0);
+    d = d / (rho(ix, iy, iz) * cv(ix, iy, iz));
+    dke(ix, iy, iz) = d;
+    energy(ix, iy, iz) = energy(ix, iy, iz) + d;
+  });
+  energy_bcs(run);
 }
 
 }  // namespace lare

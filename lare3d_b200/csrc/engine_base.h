@@ -20,6 +20,8 @@ class EngineBase {
   virtual int neutral_fraction() = 0;           // no-op under EOS_IDEAL
   virtual int perpendicular_resistivity() = 0;
   virtual bool partially_ionised() const = 0;
+  virtual int energy_correction() = 0;          // LARE_EINVAL unless rke
+  virtual bool rke() const = 0;
   virtual int conduct_heat(double dt, int force_stages, int* n_stages) = 0;
   virtual int conduction_stages(double dt, int* n_stages) = 0;
   virtual int energy(double out[5]) = 0;

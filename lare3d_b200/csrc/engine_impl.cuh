@@ -168,6 +168,7 @@ class EngineT : public EngineBase {
     p.cowling_resistivity = prm->cowling_resistivity;
     p.f_bar = prm->f_bar; p.t_bar = prm->t_bar; p.r_bar = prm->r_bar; p.tr = prm->tr; p.eta_bar = prm->eta_bar;
     p.radiation = prm->radiation;
+    p.rke = prm->rke;
     p.temp_norm = prm->temp_norm; p.time_norm = prm->time_norm; p.rho_norm = prm->rho_norm; p.mf = prm->mf;
     run.pip = p.eos_number != LARE_EOS_IDEAL;
     run.cowling = p.cowling_resistivity != 0;
@@ -210,6 +211,8 @@ class EngineT : public EngineBase {
     if (run.pip || run.cowling) all.push_back(&run.a.xi);
     if (run.cowling) all.push_back(&run.a.eta_perp);
     if (p.radiation) all.push_back(&run.a.erad);
+    if (p.rke)
+      for (A3<R>* x : {&run.a.delta_ke, &run.a.rke_f[0], &run.a.rke_f[1], &run.a.rke_f[2]}) all.push_back(x);
     for (A3<R>* x : all) {
       R* base = dalloc<R>(run.elems, err);
       if (!base) return LARE_ENOMEM;
@@ -319,6 +322,7 @@ class EngineT : public EngineBase {
     if (p.conduction) add("larsen_factor", &run.a.larsen, 0, X, 0, Y, 0, Z);
     if (run.a.xi.p) add("xi_n", &run.a.xi, -1, X + 2, -1, Y + 2, -1, Z + 2);
     if (run.a.eta_perp.p) add("eta_perp", &run.a.eta_perp, -1, X + 2, -1, Y + 2, -1, Z + 2);
+    if (run.a.delta_ke.p) add("delta_ke", &run.a.delta_ke, -1, X + 2, -1, Y + 2, -1, Z + 2);
     cudaError_t e = cudaStreamSynchronize(run.s);
     if (e != cudaSuccess) { err = cudaGetErrorString(e); return LARE_ECUDA; }
     return LARE_OK;
@@ -480,6 +484,12 @@ class EngineT : public EngineBase {
     return cuda_check("perpendicular_resistivity");
   }
   bool partially_ionised() const override { return run.pip; }
+  int energy_correction() override {
+    if (!run.p.rke) return fail(LARE_EINVAL, "energy_correction: rke is off");
+    lare::energy_correction(run);
+    return cuda_check("energy_correction");
+  }
+  bool rke() const override { return run.p.rke != 0; }
   int eulerian_remap(int step) override {
     lare::eulerian_remap(run, step);
     return cuda_check("eulerian_remap");
@@ -562,6 +572,7 @@ class EngineT : public EngineBase {
       if (run.pip) lare::neutral_fraction(run, run.a.energy);  // lare3d.f90:83
       rc = lare::lagrangian_step(run, first + k);
       if (rc == LARE_OK) lare::eulerian_remap(run, first + k);
+      if (rc == LARE_OK && run.p.rke) lare::energy_correction(run);  // lare3d.f90:86
       if (rc == LARE_OK) lare::eta_calc(run);
     }
     run.capturing = false;

@@ -115,6 +115,11 @@ int lare_gpu_perpendicular_resistivity(lare_ctx* c) {
   return c->e->perpendicular_resistivity();
 }
 
+int lare_gpu_energy_correction(lare_ctx* c) {
+  if (guard(c)) return LARE_EINVAL;
+  return c->e->energy_correction();
+}
+
 int lare_gpu_step(lare_ctx* c, int step, double* time, double* dt) {
   if (guard(c)) return LARE_EINVAL;
   int rc = c->e->neutral_fraction();  // lare3d.f90:83 (a no-op under EOS_IDEAL)
@@ -122,6 +127,7 @@ int lare_gpu_step(lare_ctx* c, int step, double* time, double* dt) {
   rc = c->e->lagrangian_step(step);
   if (rc) return rc;
   if ((rc = c->e->eulerian_remap(step))) return rc;
+  if (c->e->rke() && (rc = c->e->energy_correction())) return rc;  // lare3d.f90:86
   if ((rc = c->e->eta_calc())) return rc;
   if (time || dt) {
     lare_scalars s;
@@ -144,6 +150,7 @@ int lare_gpu_run(lare_ctx* c, int first_step, int nsteps, double t_end, int* ste
     if ((rc = c->e->neutral_fraction())) return rc;
     if ((rc = c->e->lagrangian_step(step))) return rc;
     if ((rc = c->e->eulerian_remap(step))) return rc;
+    if (c->e->rke() && (rc = c->e->energy_correction())) return rc;
     if ((rc = c->e->eta_calc())) return rc;
     ++done;
     if ((rc = c->e->scalars(&s))) return rc;

@@ -563,7 +563,9 @@ struct MomArgs {
 // the three momentum fluxes through a face (K8's body) from its stencil
 // values: w[comp] = v at c-e_A, c, c+e_A, c+2e_A; db1 at c, c+e_A, c+2e_A;
 // dc1 at c, c+e_A; v1 (va), rho_v (rv) at c, c+e_A; dm at c
-template <class R>
+// PRE: the flux before its product with dm (what rke's kinetic-energy
+// terms use, xremap.f90:664-695).
+template <class R, bool PRE = false>
 __device__ __forceinline__ void mom_flux_vals(R area, R va0, R va1, R rvc, R rvp, R dmc, R db0, R db1, R db2, R dc0,
                                               R dc1, const R (&w)[3][4], R dt, R (&F)[3]) {
   const R v_advect = (va0 + va1) * R(0.5);  // the face-averaged v1 of xremap.f90:257-265
@@ -590,12 +592,12 @@ __device__ __forceinline__ void mom_flux_vals(R area, R va0, R va1, R rvc, R rvp
     const R ss = R(0.5) * (copysign(R(1), dfi) + copysign(R(1), dfu));
     const R Di = sign_v * ss * fmin(fmin(fabs(Da) * dxbu, fabs(dfi)), fabs(dfu));
     const R f = fu + Di * (R(1) - dmu);
-    F[comp] = f * dmc;
+    F[comp] = PRE ? f : f * dmc;
   }
 }
 
 // the same, loading the stencil of face c
-template <class R>
+template <class R, bool PRE = false>
 __device__ __forceinline__ void mom_flux(const MomArgs<R>& g, int c, int i1, int i2, R dt, R (&F)[3]) {
   const int SA = g.SA;
   R w[3][4];
@@ -603,8 +605,25 @@ __device__ __forceinline__ void mom_flux(const MomArgs<R>& g, int c, int i1, int
   for (int comp = 0; comp < 3; ++comp)
 #pragma unroll
     for (int q = 0; q < 4; ++q) w[comp][q] = g.v[comp][c + (q - 1) * SA];
-  mom_flux_vals(g.dct1(i1) * g.dct2(i2), g.va[c], g.va[c + SA], g.rv[c], g.rv[c + SA], g.dmv[c], g.db1[c],
-                g.db1[c + SA], g.db1[c + 2 * SA], g.dc1[c], g.dc1[c + SA], w, dt, F);
+  mom_flux_vals<R, PRE>(g.dct1(i1) * g.dct2(i2), g.va[c], g.va[c + SA], g.rv[c], g.rv[c + SA], g.dmv[c], g.db1[c],
+                        g.db1[c + SA], g.db1[c + 2 * SA], g.dc1[c], g.dc1[c + SA], w, dt, F);
+}
+
+// rke's kinetic-energy defect of one component through the vertex pair
+// (c, c + e_A) (xremap.f90:664-695 and its eight siblings in [xyz]remap.f90,
+// all of one form): f the flux before the product with dm, v the velocity
+// before the update.
+template <class R>
+__device__ __forceinline__ R rke_dk(const R* v, const R* f, const R* dmv, const R* rv1, const R* cv2v, int c,
+                                    int SA) {
+  const R v0 = v[c], v1 = v[c + SA];
+  const R fm = f[c - SA], f0 = f[c], fp = f[c + SA];
+  const R dmm = dmv[c - SA], dm0 = dmv[c], dmp = dmv[c + SA];
+  const R m = rv1[c] * cv2v[c], mp = rv1[c + SA] * cv2v[c + SA];
+  const R ai = (v0 - fm) * dmm / m - (v0 - f0) * dm0 / m;
+  const R aip = (v1 - f0) * dm0 / mp - (v1 - fp) * dmp / mp;
+  R dk = (v1 - v0) * (f0 - R(0.5) * (v1 + v0)) - R(0.5) * ai * (v0 - f0) + R(0.5) * aip * (v1 - f0);
+  return dk * dm0 * R(0.5);
 }
 
 // K9's update at c from the fluxes at faces c - e_A (Fm) and c (F)
@@ -1067,6 +1086,58 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     }
     run.prof_end(k);
     ++run.launches;
+  }
+  if (run.p.rke) {
+    // rke (xremap.f90:664-695 and siblings): the old velocities are still
+    // in v (the new ones went to the q buffers).  R1 keeps the three fluxes
+    // before their product with dm (faces -1:n along A); R2 adds, per cell
+    // 1:n, the defect dk of each vertex whose update scatters into it, for
+    // the components in file order and the vertices in the reference's loop
+    // order, so the sums are the reference's bit for bit.
+    MomArgs<R> gm;
+    gm.va = va;
+    gm.rv = rv;
+    gm.dmv = dmv;
+    gm.db1 = db1;
+    gm.dc1 = dc1;
+    gm.v[0] = Ar.vx.p;
+    gm.v[1] = Ar.vy.p;
+    gm.v[2] = Ar.vz.p;
+    gm.dct1 = dct1;
+    gm.dct2 = dct2;
+    gm.SA = SA;
+    R* const rf0 = Ar.rke_f[0].p;
+    R* const rf1 = Ar.rke_f[1].p;
+    R* const rf2 = Ar.rke_f[2].p;
+    int lo[3] = {0, 0, 0}, hi[3] = {nx, ny, nz};
+    lo[A] = -1;
+    hi[A] = na;
+    LARE_BOXW(run, 13, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
+      const int p3[3] = {ix, iy, iz};
+      const int c = ix + sx * iy + sxy * iz;
+      R F[3];
+      mom_flux<R, true>(gm, c, p3[T1], p3[T2], (R)sc[dt_slot], F);
+      rf0[c] = F[0];
+      rf1[c] = F[1];
+      rf2[c] = F[2];
+    });
+    R* const dke = Ar.delta_ke.p;
+    const R* const vv0 = Ar.vx.p;
+    const R* const vv1 = Ar.vy.p;
+    const R* const vv2 = Ar.vz.p;
+    LARE_BOXW(run, 12, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
+      const int c = ix + sx * iy + sxy * iz;
+      const int b = c - SA;  // the vertex below along A; its transverse neighbours below
+      const int vtx[4] = {b - S1 - S2, b - S2, b - S1, b};
+      const R* const vq[3] = {vv0, vv1, vv2};
+      const R* const fq[3] = {rf0, rf1, rf2};
+      R d = dke[c];
+#pragma unroll
+      for (int comp = 0; comp < 3; ++comp)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) d = d + rke_dk(vq[comp], fq[comp], dmv, rv1, cv2v, vtx[q], SA);
+      dke[c] = d;
+    });
   }
   std::swap(Ar.vx.p, Ar.qx.p);
   std::swap(Ar.vy.p, Ar.qy.p);

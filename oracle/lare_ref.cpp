@@ -155,6 +155,7 @@ struct lare_ref {
   // cowling_resistivity)
   F3 xi_n, eta_perp;
   bool eos_error = false;  // neutral.f90:171-174 'Temperature bounds problem'
+  F3 delta_ke;             // rke (shared_data.F90:108, allocated mpi_routines.F90:313)
 
   // shared_data scalars.
   double time = 0.0, dt = 0.0, dt2 = 0.0, dtr = 0.0;
@@ -210,6 +211,7 @@ struct lare_ref {
     cell(xi_n);
     xi_n.fill(p.xi_n);
     if (p.cowling_resistivity) cell(eta_perp);
+    if (p.rke) cell(delta_ke);
 
     V[0] = &vx; V[1] = &vy; V[2] = &vz;
     V1[0] = &vx1; V1[1] = &vy1; V1[2] = &vz1;
@@ -229,6 +231,7 @@ struct lare_ref {
               {"fy_visc", &fy_visc}, {"fz_visc", &fz_visc}, {"larsen_factor", &larsen_factor},
               {"xi_n", &xi_n}};
     if (p.cowling_resistivity) fields["eta_perp"] = &eta_perp;
+    if (p.rke) fields["delta_ke"] = &delta_ke;
   }
 
   // ------------------------------------------------------------------
@@ -1097,6 +1100,18 @@ struct lare_ref {
 
   int eos_number() const { return p.eos_number == 0 ? LARE_EOS_IDEAL : p.eos_number; }
 
+  // diagnostics.F90:613-629
+  void energy_correction() {
+    for (size_t q = 0; q < delta_ke.d.size(); ++q) delta_ke.d[q] = -delta_ke.d[q];
+    for (size_t q = 0; q < delta_ke.d.size(); ++q)
+      if (delta_ke.d[q] < 0.0) delta_ke.d[q] = 0.0;
+    for (size_t q = 0; q < delta_ke.d.size(); ++q) delta_ke.d[q] = delta_ke.d[q] / (rho.d[q] * cv.d[q]);
+    box(1, nx, 1, ny, 1, nz, [&](int ix, int iy, int iz) {
+      energy(ix, iy, iz) = energy(ix, iy, iz) + delta_ke(ix, iy, iz);
+    });
+    energy_bcs();
+  }
+
   // radiative.f90:38-62 setup_loss_function and :180-208
   // set_exact_integration_arrays (n = 7 boundaries, kmax = 6 bands)
   struct Rad {
@@ -1270,6 +1285,7 @@ struct lare_ref {
   // ------------------------------------------------------------------
   // remap.f90:33-131
   void eulerian_remap(int step) {
+    if (p.rke) delta_ke.fill(0.0);  // remap.f90:38
     xpass = ypass = zpass = 1;
     box(-1, nx + 2, -1, ny + 2, -1, nz + 2, [&](int ix, int iy, int iz) {
       bx(ix, iy, iz) = bx(ix, iy, iz) * dyb(iy) * dzb(iz);
@@ -1566,6 +1582,38 @@ struct lare_ref {
         double dmu = std::fabs(dm(ix, iy, iz)) / area / L.dxbu / rhou;
         flux(ix, iy, iz) = L.fu + L.Di * (1.0 - dmu);
       });
+      if (p.rke) {
+        // xremap.f90:664-695 (and the eight siblings): serial, in the
+        // reference's loop order, because the scatter adds into shared cells
+        int rlo[3] = {0, 0, 0}, rhi[3] = {nx, ny, nz};
+        rhi[a] = na - 1;
+        const int u = a == 0 ? 1 : 0, w = a == 2 ? 1 : 2;  // transverse axes, u < w
+        for (int iz = rlo[2]; iz <= rhi[2]; ++iz)
+          for (int iy = rlo[1]; iy <= rhi[1]; ++iy)
+            for (int ix = rlo[0]; ix <= rhi[0]; ++ix) {
+              int pp[3] = {ix, iy, iz}, pm[3], pq[3];
+              sh(pp, a, -1, pm);
+              sh(pp, a, 1, pq);
+              double m = rv1(ix, iy, iz) * cv2(ix, iy, iz);
+              double mp = rv1(pq[0], pq[1], pq[2]) * cv2(pq[0], pq[1], pq[2]);
+              double v0 = vc(ix, iy, iz), v1 = vc(pq[0], pq[1], pq[2]);
+              double fm = flux(pm[0], pm[1], pm[2]), f0 = flux(ix, iy, iz), fp = flux(pq[0], pq[1], pq[2]);
+              double dmm = dm(pm[0], pm[1], pm[2]), dm0 = dm(ix, iy, iz), dmp = dm(pq[0], pq[1], pq[2]);
+              double ai = (v0 - fm) * dmm / m - (v0 - f0) * dm0 / m;
+              double aip = (v1 - f0) * dm0 / mp - (v1 - fp) * dmp / mp;
+              double dk = (v1 - v0) * (f0 - 0.5 * (v1 + v0)) - 0.5 * ai * (v0 - f0) + 0.5 * aip * (v1 - f0);
+              dk = dk * dm0 * 0.5;
+              int t[3] = {pq[0], pq[1], pq[2]};
+              delta_ke(t[0], t[1], t[2]) = delta_ke(t[0], t[1], t[2]) + dk;
+              t[u] += 1;
+              delta_ke(t[0], t[1], t[2]) = delta_ke(t[0], t[1], t[2]) + dk;
+              t[u] -= 1;
+              t[w] += 1;
+              delta_ke(t[0], t[1], t[2]) = delta_ke(t[0], t[1], t[2]) + dk;
+              t[u] += 1;
+              delta_ke(t[0], t[1], t[2]) = delta_ke(t[0], t[1], t[2]) + dk;
+            }
+      }
       box(lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [&](int ix, int iy, int iz) {
         flux(ix, iy, iz) = flux(ix, iy, iz) * dm(ix, iy, iz);
       });
@@ -1913,6 +1961,12 @@ int lare_ref_neutral_fraction(lare_ref* r) {
   return LARE_OK;
 }
 double lare_ref_exp(double x) { return cw_exp(x); }
+int lare_ref_energy_correction(lare_ref* r) {
+  if (!r) return LARE_EINVAL;
+  if (!r->p.rke) return fail(r, LARE_EINVAL, "rke is off");
+  r->energy_correction();
+  return LARE_OK;
+}
 int lare_ref_perpendicular_resistivity(lare_ref* r) {
   if (!r) return LARE_EINVAL;
   if (!r->p.cowling_resistivity) return fail(r, LARE_EINVAL, "cowling_resistivity is off");
@@ -1940,6 +1994,7 @@ int lare_ref_step(lare_ref* r, int step, double* time, double* dt) {
   rc = lare_ref_lagrangian_step(r, step);
   if (rc) return rc;
   r->eulerian_remap(step);
+  if (r->p.rke) r->energy_correction();  // lare3d.f90:86
   r->eta_calc();
   if (time) *time = r->time;
   if (dt) *dt = r->dt;

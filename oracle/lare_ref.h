@@ -38,6 +38,7 @@ int lare_ref_eta_calc(lare_ref* r);
 int lare_ref_boundary_conditions(lare_ref* r);
 int lare_ref_neutral_fraction(lare_ref* r);
 int lare_ref_perpendicular_resistivity(lare_ref* r);
+int lare_ref_energy_correction(lare_ref* r);
 /* the exponential the ionisation model uses (Cody-Waite + Taylor) */
 double lare_ref_exp(double x);
 int lare_ref_step(lare_ref* r, int step, double* time, double* dt);

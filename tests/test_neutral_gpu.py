@@ -138,3 +138,31 @@ def test_radiative_losses_fp32(built):
     for f in STATE:
         e = rel_l2(g.get_field(f), r.get_field(f))
         assert e <= 1e-5, f"{f}: rel L2 {e:.2e}"
+
+
+@pytest.mark.parametrize("name", ["orszag_tang", "open_blast"])
+def test_rke_bitwise(built, name):
+    """rke: every cell's kinetic-energy defect is the reference's sum, in
+    the reference's order, so delta_ke (cells 1:n, after the remap) and the
+    corrected energy agree bit for bit."""
+    d = getattr(decks, name)(16, rke=1)
+    r, g = pair(d)
+    n = 16
+    inner = (slice(2, n + 2),) * 3
+    for s in range(1, 5):
+        r.lagrangian_step(s)
+        g.lagrangian_step(s)
+        r.eulerian_remap(s)
+        g.eulerian_remap(s)
+        a, b = g.get_field("delta_ke")[inner], r.get_field("delta_ke")[inner]
+        assert np.count_nonzero(a != b) == 0, f"step {s}: delta_ke differs (max {np.abs(a - b).max():.3e})"
+        r.energy_correction()
+        g.energy_correction()
+        r.eta_calc()
+        g.eta_calc()
+        assert_bitwise(g, r, STATE, f"step {s}")
+    # and through lare_gpu_step
+    for s in range(5, 7):
+        r.step(s)
+        g.step(s)
+        assert_bitwise(g, r, STATE, f"step {s}")
