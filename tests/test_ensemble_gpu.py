@@ -77,3 +77,28 @@ def test_autotune_picks_a_measured_shape(built):
     best, times = autotune(16, blocks=BLOCKS[:3], launches=1, kind="blast")
     assert best in BLOCKS[:3] and set(times) == set(BLOCKS[:3])
     assert all(t > 0 for t in times.values())
+
+
+def test_ensemble_with_the_widened_physics(built):
+    """Recorded steps carry the partially ionised models (neutral_fraction at
+    each step start and in the device-side sub-cycle loop), radiation and
+    rke's energy_correction: FP64 members match their single runs bit for
+    bit."""
+    from lare3d_b200 import decks, gpu
+    from lare3d_b200.ensemble import Ensemble
+    ds = [decks.partially_ionised(12, eta_bar=1e-2), decks.radiative_blast(12),
+          decks.orszag_tang(12, rke=1), decks.partially_ionised(10, cowling=False, rke=1)]
+    ens = Ensemble(ds, precision=64)
+    ens.launch(1)
+    ens.sync()
+    for i, d in enumerate(ds):
+        ref = gpu.simulation(d, precision=64)
+        ref.start(d.state)
+        for s in range(1, 8):
+            ref.step(s)
+        got = ens.sims[i]
+        for f in STATE:
+            a, b = got.get_field(f), ref.get_field(f)
+            assert np.array_equal(a, b), (i, f, float(np.abs(a - b).max()))
+        ref.close()
+    ens.close()
