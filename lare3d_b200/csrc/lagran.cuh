@@ -949,6 +949,18 @@ int resistive_subcycles_captured(Run<R>& run) {
   neutral_models(run);
   eta_and_rkstep(run, true);
   resistive_update(run);
+  {
+    // bstep swapped the B buffers on the host, but the body replays with
+    // the pointers it was recorded with: copy the new B back into the
+    // buffers the body reads and restore the pointers, so every pass starts
+    // from the previous pass's field.
+    Arrays<R>& A = run.a;
+    for (A3<R>* b : {&A.bx, &A.by, &A.bz}) {
+      A3<R>& o = b == &A.bx ? A.bx1 : (b == &A.by ? A.by1 : A.bz1);
+      copy_whole(run, o, *b);
+      std::swap(b->p, o.p);
+    }
+  }
   launch_scalar(run.s, run.launches, [=] __device__() {
     const double left = sc[SC_LOOP] - 1.0;
     sc[SC_LOOP] = left;
