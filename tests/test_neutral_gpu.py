@@ -166,3 +166,27 @@ def test_rke_bitwise(built, name):
         r.step(s)
         g.step(s)
         assert_bitwise(g, r, STATE, f"step {s}")
+
+
+def test_widened_physics_together_with_open_sides(built):
+    """Partially ionised with Cowling resistivity, rke and open x/y sides in
+    one deck: FP64 bit for bit over four steps."""
+    from lare3d_b200.abi import BC_OPEN
+    d = decks.partially_ionised(16, eta_bar=1e-2, rke=1, xbc_min=BC_OPEN, xbc_max=BC_OPEN, ybc_min=BC_OPEN,
+                                ybc_max=BC_OPEN)
+    r, g = pair(d)
+    for s in range(1, 5):
+        r.step(s)
+        g.step(s)
+        assert_bitwise(g, r, STATE + ["xi_n", "eta_perp"], f"step {s}")
+
+
+def test_rke_fp32(built):
+    d = decks.orszag_tang(16, rke=1)
+    r, g = pair(d, precision=32)
+    for s in range(1, 6):
+        r.step(s)
+        g.step(s)
+    for f in STATE:
+        e = rel_l2(g.get_field(f), r.get_field(f))
+        assert e <= 1e-5, f"{f}: rel L2 {e:.2e}"
