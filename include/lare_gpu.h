@@ -111,6 +111,14 @@ typedef struct lare_params {
    * energy_correction returns it to the internal energy after the remap.
    */
   int rke;
+  /*
+   * cooling_term (control.f90:205-206): exponential moving averages, weight
+   * alpha_av, of the viscous heating (lagran.F90:464-475) and of the ohmic
+   * heating (:1290-1302) are taken off the energy each step; the averages
+   * persist across steps (fields "cool_term_v", "cool_term_b").
+   */
+  int cooling_term;
+  double alpha_av;
 } lare_params;
 
 /* Scalars of shared_data that the step updates. */

@@ -78,6 +78,8 @@ class LareParams(C.Structure):
         ("rho_norm", C.c_double),
         ("mf", C.c_double),
         ("rke", C.c_int),
+        ("cooling_term", C.c_int),
+        ("alpha_av", C.c_double),
     ]
 
 
@@ -127,6 +129,8 @@ def default_params(**kw) -> LareParams:
     p.cowling_resistivity = 0
     p.radiation = 0
     p.rke = 0
+    p.cooling_term = 0
+    p.alpha_av = 0.05
     p.mf = 1.2
     for k, v in kw.items():
         if not hasattr(p, k):

@@ -37,6 +37,8 @@ struct Par {
   double f_bar, t_bar, r_bar, tr, eta_bar;
   int radiation;                                       // radiative.f90
   int rke;                                             // the remap's kinetic-energy correction
+  int cooling_term;                                    // lagran.F90:464, :1290
+  double alpha_av;
   double temp_norm, time_norm, rho_norm, mf;
   int bc[3][2];   // [dim][0=min,1=max]
   bool per[3];    // periodic communicator in this dimension (mpi_routines.F90:195-210)
@@ -64,6 +66,9 @@ struct Arrays {
   // rke: the remap's kinetic-energy defect (shared_data.F90:108) and the
   // three momentum fluxes before their product with dm
   A3<R> delta_ke, rke_f[3];
+  // cooling_term: moving averages of the viscous and ohmic heating
+  // (shared_data.F90:109), persistent across steps
+  A3<R> cool_term_v, cool_term_b;
   // 1-D metrics (pointers at Fortran index 0)
   A1<R> dxb, dxc, dyb, dyc, dzb, dzc, grav;
   // reciprocals for conduction: 1/dxb, 1/dxc, 1/(dxc(i) + dxc(i-1)), per axis

@@ -169,6 +169,8 @@ class EngineT : public EngineBase {
     p.f_bar = prm->f_bar; p.t_bar = prm->t_bar; p.r_bar = prm->r_bar; p.tr = prm->tr; p.eta_bar = prm->eta_bar;
     p.radiation = prm->radiation;
     p.rke = prm->rke;
+    p.cooling_term = prm->cooling_term;
+    p.alpha_av = prm->alpha_av;
     p.temp_norm = prm->temp_norm; p.time_norm = prm->time_norm; p.rho_norm = prm->rho_norm; p.mf = prm->mf;
     run.pip = p.eos_number != LARE_EOS_IDEAL;
     run.cowling = p.cowling_resistivity != 0;
@@ -213,6 +215,8 @@ class EngineT : public EngineBase {
     if (p.radiation) all.push_back(&run.a.erad);
     if (p.rke)
       for (A3<R>* x : {&run.a.delta_ke, &run.a.rke_f[0], &run.a.rke_f[1], &run.a.rke_f[2]}) all.push_back(x);
+    if (p.cooling_term)
+      for (A3<R>* x : {&run.a.cool_term_v, &run.a.cool_term_b}) all.push_back(x);
     for (A3<R>* x : all) {
       R* base = dalloc<R>(run.elems, err);
       if (!base) return LARE_ENOMEM;
@@ -323,6 +327,10 @@ class EngineT : public EngineBase {
     if (run.a.xi.p) add("xi_n", &run.a.xi, -1, X + 2, -1, Y + 2, -1, Z + 2);
     if (run.a.eta_perp.p) add("eta_perp", &run.a.eta_perp, -1, X + 2, -1, Y + 2, -1, Z + 2);
     if (run.a.delta_ke.p) add("delta_ke", &run.a.delta_ke, -1, X + 2, -1, Y + 2, -1, Z + 2);
+    if (run.a.cool_term_v.p) {  // (1:n in the reference; the padding here holds zeros)
+      add("cool_term_v", &run.a.cool_term_v, 1, X, 1, Y, 1, Z);
+      add("cool_term_b", &run.a.cool_term_b, 1, X, 1, Y, 1, Z);
+    }
     cudaError_t e = cudaStreamSynchronize(run.s);
     if (e != cudaSuccess) { err = cudaGetErrorString(e); return LARE_ECUDA; }
     return LARE_OK;

@@ -280,6 +280,8 @@ void resistive_update(Run<R>& run) {
   R* const ohmic = A.ohmic_dep.p;
   const R* curlb = A.curlb.p;
   const R* rho = A.rho.p;
+  R* const ctb = run.p.cooling_term ? A.cool_term_b.p : nullptr;  // :1290-1302
+  const R alpha = (R)run.p.alpha_av;
   box_sum<1>(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz, double* v) {
     const R dt = (R)sc[SC_DTSUB];
     const int c = ix + sx * iy + sxy * iz;
@@ -289,6 +291,14 @@ void resistive_update(Run<R>& run) {
                curlb[c - sx - sxy] + curlb[c - 1 - sx - sxy]) * dt / (R(8) * rho[c]);
       ohmic[c] = ohmic[c] + lh;
       e = e + lh;
+      if (ctb) {
+        // the moving average of the heating of the iz plane's four
+        // vertices only, as the reference writes it
+        const R lh4 = (curlb[c] + curlb[c - 1] + curlb[c - sx] + curlb[c - 1 - sx]) * dt / (R(4) * rho[c]);
+        const R t = alpha * lh4 + (R(1) - alpha) * ctb[c];
+        ctb[c] = t;
+        e = e - t;
+      }
     }
     energy[c] = e > R(0) ? e : R(0);
     if (ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz) {
@@ -889,6 +899,27 @@ void predictor_corrector_step(Run<R>& run) {
     rhow[c] = r / (R(1) + dv);
     v[0] = (double)(dt * vh * cv[c]);
   }, SC_VISC_TOT, true);
+  if (run.p.cooling_term) {
+    // :464-475: an exponential moving average of the viscous heating
+    // (weight alpha_av) is taken off the energy of cells 1:n, then
+    // energy = MAX(energy, 0) over the whole array
+    R* const ctv = A.cool_term_v.p;
+    const R* vhp2 = A.visc_heat.p;
+    const R* rho2 = A.rho.p;
+    R* const en = A.energy.p;
+    const R alpha = (R)run.p.alpha_av;
+    LARE_BOXW(run, 5, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+      const int c = ix + sx * iy + sxy * iz;
+      R e = en[c];
+      if (ix >= 1 && ix <= nx && iy >= 1 && iy <= ny && iz >= 1 && iz <= nz) {
+        const R dt = (R)sc[SC_DT];
+        const R t = alpha * dt * vhp2[c] / rho2[c] + (R(1) - alpha) * ctv[c];
+        ctv[c] = t;
+        e = e - t;
+      }
+      en[c] = e > R(0) ? e : R(0);
+    });
+  }
 }
 
 // ---------------------------------------------------------------------

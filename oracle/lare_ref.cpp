@@ -156,6 +156,7 @@ struct lare_ref {
   F3 xi_n, eta_perp;
   bool eos_error = false;  // neutral.f90:171-174 'Temperature bounds problem'
   F3 delta_ke;             // rke (shared_data.F90:108, allocated mpi_routines.F90:313)
+  F3 cool_term_v, cool_term_b;  // cooling_term (shared_data.F90:109, mpi_routines.F90:315-319)
 
   // shared_data scalars.
   double time = 0.0, dt = 0.0, dt2 = 0.0, dtr = 0.0;
@@ -212,6 +213,10 @@ struct lare_ref {
     xi_n.fill(p.xi_n);
     if (p.cowling_resistivity) cell(eta_perp);
     if (p.rke) cell(delta_ke);
+    if (p.cooling_term) {
+      cool_term_v.alloc(1, N, 1, M, 1, L);
+      cool_term_b.alloc(1, N, 1, M, 1, L);
+    }
 
     V[0] = &vx; V[1] = &vy; V[2] = &vz;
     V1[0] = &vx1; V1[1] = &vy1; V1[2] = &vz1;
@@ -232,6 +237,10 @@ struct lare_ref {
               {"xi_n", &xi_n}};
     if (p.cowling_resistivity) fields["eta_perp"] = &eta_perp;
     if (p.rke) fields["delta_ke"] = &delta_ke;
+    if (p.cooling_term) {
+      fields["cool_term_v"] = &cool_term_v;
+      fields["cool_term_b"] = &cool_term_b;
+    }
   }
 
   // ------------------------------------------------------------------
@@ -762,6 +771,15 @@ struct lare_ref {
         }
       }
     }
+    if (p.cooling_term) {  // :464-475
+      const double al = p.alpha_av;
+      box(1, nx, 1, ny, 1, nz, [&](int ix, int iy, int iz) {
+        cool_term_v(ix, iy, iz) = al * dt * visc_heat(ix, iy, iz) / rho(ix, iy, iz)
+                                + (1.0 - al) * cool_term_v(ix, iy, iz);
+        energy(ix, iy, iz) = energy(ix, iy, iz) - cool_term_v(ix, iy, iz);
+      });
+      for (size_t q = 0; q < energy.size(); ++q) energy.d[q] = fmax0(energy.d[q]);
+    }
   }
 
   // lagran.F90:483-524
@@ -1044,6 +1062,16 @@ struct lare_ref {
       ohmic_dep(ix, iy, iz) = ohmic_dep(ix, iy, iz) + lh;
       energy(ix, iy, iz) = energy(ix, iy, iz) + lh;
     });
+    if (p.cooling_term) {  // :1290-1302 (four curlb terms, the iz plane only)
+      const double al = p.alpha_av;
+      box(1, nx, 1, ny, 1, nz, [&](int ix, int iy, int iz) {
+        int ixm = ix - 1, iym = iy - 1;
+        double local_heating = (curlb(ix, iy, iz) + curlb(ixm, iy, iz) + curlb(ix, iym, iz) + curlb(ixm, iym, iz))
+                             * dt / (4.0 * rho(ix, iy, iz));
+        cool_term_b(ix, iy, iz) = al * local_heating + (1.0 - al) * cool_term_b(ix, iy, iz);
+        energy(ix, iy, iz) = energy(ix, iy, iz) - cool_term_b(ix, iy, iz);
+      });
+    }
     for (size_t q = 0; q < energy.size(); ++q) energy.d[q] = fmax0(energy.d[q]);
     energy_bcs();
     for (int iz = 0; iz <= nz; ++iz)

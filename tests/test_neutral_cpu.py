@@ -214,3 +214,28 @@ def test_energy_correction_needs_rke():
     s.start(d.state)
     with pytest.raises(LareError):
         s.energy_correction()
+
+
+# ---------------------------------------------------------------------
+# cooling_term (lagran.F90:464-475, :1290-1302): moving averages of the
+# heating taken off the energy.
+
+def test_cooling_term_first_step_is_the_weighted_heating():
+    """From zero averages, one Lagrangian step leaves cool_term_v =
+    alpha_av dt visc_heat / rho exactly, and the energy lower than without."""
+    n = 10
+    out = {}
+    for ct in (0, 1):
+        d = decks.orszag_tang(n, cooling_term=ct, alpha_av=0.05)
+        s = _sim(d)
+        s.lagrangian_step(1)
+        out[ct] = s
+    s = out[1]
+    dt = s.scalars().dt
+    vh = s.get_field("visc_heat")[1:n + 1, 1:n + 1, 1:n + 1]        # 0:n+1 -> 1:n
+    rho = s.get_field("rho")[2:n + 2, 2:n + 2, 2:n + 2]
+    want = 0.05 * dt * vh / rho + (1.0 - 0.05) * 0.0
+    assert np.array_equal(s.get_field("cool_term_v"), want)
+    assert np.all(s.get_field("cool_term_b") >= 0.0) and s.get_field("cool_term_b").max() > 0.0
+    inner = (slice(2, n + 2),) * 3
+    assert s.get_field("energy")[inner].sum() < out[0].get_field("energy")[inner].sum()

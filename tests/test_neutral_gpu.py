@@ -190,3 +190,15 @@ def test_rke_fp32(built):
     for f in STATE:
         e = rel_l2(g.get_field(f), r.get_field(f))
         assert e <= 1e-5, f"{f}: rel L2 {e:.2e}"
+
+
+@pytest.mark.parametrize("name", ["orszag_tang", "blast"])
+def test_cooling_term_bitwise(built, name):
+    """cooling_term's two moving averages (viscous in the corrector, ohmic
+    in each resistive sub-cycle) and the energies they cool, bit for bit."""
+    d = getattr(decks, name)(16, cooling_term=1, alpha_av=0.05)
+    r, g = pair(d)
+    for s in range(1, 5):
+        r.step(s)
+        g.step(s)
+        assert_bitwise(g, r, STATE + ["cool_term_v", "cool_term_b"], f"step {s}")
