@@ -42,7 +42,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--out-dir", default=os.path.join(ROOT, "bench_out"),
+                    help="where the clock samples and per-site profile tables go")
     return ap.parse_args()
+
+
+OUT_DIR = os.path.join(ROOT, "bench_out")
 
 
 def peaks():
@@ -63,7 +68,7 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = os.path.join(OUT_DIR, f"clocks_rank{index}.csv")
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -137,8 +142,8 @@ def cpu_baseline(deck, steps=1):
 
 
 def dump_profile(prof, name):
-    """Write the per-launch-site table of one profiled step to gpurun_out/."""
-    path = os.path.join(ROOT, "gpurun_out", name)
+    """Write the per-launch-site table of one profiled step to the output folder."""
+    path = os.path.join(OUT_DIR, name)
     os.makedirs(os.path.dirname(path), exist_ok=True)
     total = sum(p["ms"] for p in prof) or 1.0
     with open(path, "w") as f:
@@ -317,7 +322,9 @@ def run_reference(args):
 
 
 def main():
+    global OUT_DIR
     args = parse()
+    OUT_DIR = args.out_dir
     if args.impl == "reference":
         return run_reference(args)
     ws, rank, local = dist_setup(args)

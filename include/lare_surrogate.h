@@ -3,8 +3,8 @@
  *
  * The surrogate has no counterpart in the reference (Lare3d integrates
  * conduction only with RKL2, conduct.f90:299-416); it is the learned form
- * that sits beside the plain RKL2 step, which stays both its fallback and its
- * judge.  A 4-layer 3-D convolutional network (3^3 kernels, 32 channels,
+ * that sits beside the plain RKL2 step, which stays both its fallback and the
+ * arbiter of its accuracy.  A 4-layer 3-D convolutional network (3^3 kernels, 32 channels,
  * bf16 weights and activations, FP32 accumulation on the tensor cores) maps
  * a window of (T, rho, b-hat) to the temperature change of one RKL2 step on
  * the window's centre (valid convolutions: each layer trims one cell per

@@ -21,7 +21,7 @@ holds the orchestration:
                     patches are rejected is redone by plain RKL2 for the whole
                     grid (fallback).
 
-The surrogate has no counterpart in the reference; plain RKL2 is its judge.
+The surrogate has no counterpart in the reference; plain RKL2 arbitrates its accuracy.
 torch supplies device memory and streams only.
 """
 from __future__ import annotations

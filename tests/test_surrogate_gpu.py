@@ -1,7 +1,7 @@
 """GPU checks of the learned-conduction surrogate: every kernel of the
 forward and backward pass against the numpy oracle (oracle/surrogate_ref.py),
 training on the engine's own RKL2 pairs, what the trained network gains over
-the method without it, and the plain-RKL2 judge (exact column re-check,
+the method without it, and the plain-RKL2 arbiter (exact column re-check,
 patch-wise rejection and whole-grid fallback)."""
 import numpy as np
 import pytest
