@@ -167,6 +167,37 @@ def time_steps(sim, torch, stream, first, k):
     return e0.elapsed_time(e1) / 1000.0
 
 
+def physics_forms(torch, n, ref_value, steps=3):
+    """The widened physics at n^3, FP64, each through lare_gpu_run: open
+    (characteristic) boundaries, the partially ionised EOS with Cowling
+    resistivity at the default normalisation's physical eta_bar, optically
+    thin radiation, and rke with cooling_term on the Orszag-Tang vortex.
+    Whole steps (with their own dt and sub-cycles), after one warm-up step;
+    value = cell-updates/s, ratio = value / the plain FP64 step's."""
+    from lare3d_b200 import decks, gpu
+    cases = [
+        ("open_boundaries", lambda: decks.open_blast(n)),
+        ("partially_ionised_cowling", lambda: decks.partially_ionised(n)),
+        ("radiation", lambda: decks.radiative_blast(n)),
+        ("rke_cooling_term", lambda: decks.orszag_tang(n, rke=1, cooling_term=1)),
+    ]
+    out = {}
+    for name, make in cases:
+        d = make()
+        sim = gpu.simulation(d, precision=64)
+        sim.start(d.state)
+        sim.run(0, 1)
+        stream = torch.cuda.ExternalStream(gpu.stream_of(sim))
+        el = time_steps(sim, torch, stream, 1, steps)
+        v = n ** 3 * steps / el
+        out[name] = {"value": v, "unit": "cell-updates/s", "ms_per_step": 1e3 * el / steps,
+                     "ratio_to_plain_step": v / ref_value, "substeps": sim.scalars().last_substeps,
+                     "deck": d.name}
+        sim.close()
+        del sim, d
+    return out
+
+
 def surrogate_form(torch, cdeck, plain):
     """The learned conduction step at 256^3 (FP32 state) against plain FP32
     RKL2 from the same state, with the committed trained weights."""
@@ -450,6 +481,7 @@ def main():
             sc.close()
         forms["surrogate_conduction"] = surrogate_form(torch, cdeck, forms.get("conduction_rkl2_fp32"))
         forms["ensemble"] = ensemble_form(torch)
+        forms["physics_fp64"] = physics_forms(torch, n, value)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -202,3 +202,14 @@ def test_cooling_term_bitwise(built, name):
         r.step(s)
         g.step(s)
         assert_bitwise(g, r, STATE + ["cool_term_v", "cool_term_b"], f"step {s}")
+
+
+def test_cooling_term_fp32(built):
+    d = decks.orszag_tang(16, cooling_term=1, alpha_av=0.05)
+    r, g = pair(d, precision=32)
+    for s in range(1, 6):
+        r.step(s)
+        g.step(s)
+    for f in STATE:
+        e = rel_l2(g.get_field(f), r.get_field(f))
+        assert e <= 1e-5, f"{f}: rel L2 {e:.2e}"
