@@ -65,7 +65,7 @@ struct Arrays {
   A3<R> erad;
   // rke: the remap's kinetic-energy defect (shared_data.F90:108) and the
   // three momentum fluxes before their product with dm
-  A3<R> delta_ke, rke_f[3];
+  A3<R> delta_ke, rke_f[3], rke_dk[3];
   // cooling_term: moving averages of the viscous and ohmic heating
   // (shared_data.F90:109), persistent across steps
   A3<R> cool_term_v, cool_term_b;

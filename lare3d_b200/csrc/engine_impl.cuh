@@ -214,7 +214,9 @@ class EngineT : public EngineBase {
     if (run.cowling) all.push_back(&run.a.eta_perp);
     if (p.radiation) all.push_back(&run.a.erad);
     if (p.rke)
-      for (A3<R>* x : {&run.a.delta_ke, &run.a.rke_f[0], &run.a.rke_f[1], &run.a.rke_f[2]}) all.push_back(x);
+      for (A3<R>* x : {&run.a.delta_ke, &run.a.rke_f[0], &run.a.rke_f[1], &run.a.rke_f[2], &run.a.rke_dk[0],
+                       &run.a.rke_dk[1], &run.a.rke_dk[2]})
+        all.push_back(x);
     if (p.cooling_term)
       for (A3<R>* x : {&run.a.cool_term_v, &run.a.cool_term_b}) all.push_back(x);
     for (A3<R>* x : all) {

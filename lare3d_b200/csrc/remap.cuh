@@ -1090,10 +1090,11 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   if (run.p.rke) {
     // rke (xremap.f90:664-695 and siblings): the old velocities are still
     // in v (the new ones went to the q buffers).  R1 keeps the three fluxes
-    // before their product with dm (faces -1:n along A); R2 adds, per cell
-    // 1:n, the defect dk of each vertex whose update scatters into it, for
-    // the components in file order and the vertices in the reference's loop
-    // order, so the sums are the reference's bit for bit.
+    // before their product with dm (faces -1:n along A); R2 forms each
+    // vertex's defect dk per component; R3 adds, per cell 1:n, the dk of
+    // each vertex whose update scatters into it, for the components in file
+    // order and the vertices in the reference's loop order, so the sums are
+    // the reference's bit for bit.
     MomArgs<R> gm;
     gm.va = va;
     gm.rv = rv;
@@ -1125,17 +1126,29 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     const R* const vv0 = Ar.vx.p;
     const R* const vv1 = Ar.vy.p;
     const R* const vv2 = Ar.vz.p;
-    LARE_BOXW(run, 12, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
+    R* const dk0 = Ar.rke_dk[0].p;
+    R* const dk1 = Ar.rke_dk[1].p;
+    R* const dk2 = Ar.rke_dk[2].p;
+    // R2: each vertex's defect once (vertices 0:n-1 along A, 0:n across)
+    lo[A] = 0;
+    hi[A] = na - 1;
+    LARE_BOXW(run, 15, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
+      const int c = ix + sx * iy + sxy * iz;
+      dk0[c] = rke_dk(vv0, rf0, dmv, rv1, cv2v, c, SA);
+      dk1[c] = rke_dk(vv1, rf1, dmv, rv1, cv2v, c, SA);
+      dk2[c] = rke_dk(vv2, rf2, dmv, rv1, cv2v, c, SA);
+    });
+    // R3: the gather
+    LARE_BOXW(run, 14, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
       const int c = ix + sx * iy + sxy * iz;
       const int b = c - SA;  // the vertex below along A; its transverse neighbours below
       const int vtx[4] = {b - S1 - S2, b - S2, b - S1, b};
-      const R* const vq[3] = {vv0, vv1, vv2};
-      const R* const fq[3] = {rf0, rf1, rf2};
+      const R* const dq[3] = {dk0, dk1, dk2};
       R d = dke[c];
 #pragma unroll
       for (int comp = 0; comp < 3; ++comp)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) d = d + rke_dk(vq[comp], fq[comp], dmv, rv1, cv2v, vtx[q], SA);
+        for (int q = 0; q < 4; ++q) d = d + dq[comp][vtx[q]];
       dke[c] = d;
     });
   }
