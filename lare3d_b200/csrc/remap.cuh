@@ -555,6 +555,7 @@ struct MomArgs {
   const R* cv1v;
   const R* cv2v;
   const R* rv1;
+  R* fp[3];  // rke only: the fluxes before their product with dm
   A1<R> dct1, dct2;
   const double* sc;
   int dt_slot, nx, ny, nz, na, n3, sx, sxy, SA, S3;
@@ -563,11 +564,12 @@ struct MomArgs {
 // the three momentum fluxes through a face (K8's body) from its stencil
 // values: w[comp] = v at c-e_A, c, c+e_A, c+2e_A; db1 at c, c+e_A, c+2e_A;
 // dc1 at c, c+e_A; v1 (va), rho_v (rv) at c, c+e_A; dm at c
-// PRE: the flux before its product with dm (what rke's kinetic-energy
-// terms use, xremap.f90:664-695).
-template <class R, bool PRE = false>
+// PRE: F is the flux before its product with dm (what rke's
+// kinetic-energy terms use, xremap.f90:664-695); BOTH: F is the product and
+// fpre[comp] receives the flux before it.
+template <class R, bool PRE = false, bool BOTH = false>
 __device__ __forceinline__ void mom_flux_vals(R area, R va0, R va1, R rvc, R rvp, R dmc, R db0, R db1, R db2, R dc0,
-                                              R dc1, const R (&w)[3][4], R dt, R (&F)[3]) {
+                                              R dc1, const R (&w)[3][4], R dt, R (&F)[3], R* fpre = nullptr) {
   const R v_advect = (va0 + va1) * R(0.5);  // the face-averaged v1 of xremap.f90:257-265
   // The upwind choice, phi and dmu depend only on v_advect and the
   // geometry, so they are formed once for the three components (the same
@@ -592,12 +594,14 @@ __device__ __forceinline__ void mom_flux_vals(R area, R va0, R va1, R rvc, R rvp
     const R ss = R(0.5) * (copysign(R(1), dfi) + copysign(R(1), dfu));
     const R Di = sign_v * ss * fmin(fmin(fabs(Da) * dxbu, fabs(dfi)), fabs(dfu));
     const R f = fu + Di * (R(1) - dmu);
+    if constexpr (BOTH) fpre[comp] = f;
     F[comp] = PRE ? f : f * dmc;
   }
 }
 
-// the same, loading the stencil of face c
-template <class R, bool PRE = false>
+// the same, loading the stencil of face c (RKE: also store the fluxes
+// before their product with dm in g.fp)
+template <class R, bool RKE = false>
 __device__ __forceinline__ void mom_flux(const MomArgs<R>& g, int c, int i1, int i2, R dt, R (&F)[3]) {
   const int SA = g.SA;
   R w[3][4];
@@ -605,8 +609,13 @@ __device__ __forceinline__ void mom_flux(const MomArgs<R>& g, int c, int i1, int
   for (int comp = 0; comp < 3; ++comp)
 #pragma unroll
     for (int q = 0; q < 4; ++q) w[comp][q] = g.v[comp][c + (q - 1) * SA];
-  mom_flux_vals<R, PRE>(g.dct1(i1) * g.dct2(i2), g.va[c], g.va[c + SA], g.rv[c], g.rv[c + SA], g.dmv[c], g.db1[c],
-                        g.db1[c + SA], g.db1[c + 2 * SA], g.dc1[c], g.dc1[c + SA], w, dt, F);
+  R fpre[3];
+  mom_flux_vals<R, false, RKE>(g.dct1(i1) * g.dct2(i2), g.va[c], g.va[c + SA], g.rv[c], g.rv[c + SA], g.dmv[c],
+                               g.db1[c], g.db1[c + SA], g.db1[c + 2 * SA], g.dc1[c], g.dc1[c + SA], w, dt, F, fpre);
+  if constexpr (RKE) {
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) g.fp[comp][c] = fpre[comp];
+  }
 }
 
 // rke's kinetic-energy defect of one component through the vertex pair
@@ -634,7 +643,7 @@ __device__ __forceinline__ void mom_update(const MomArgs<R>& g, int c, const R (
   for (int comp = 0; comp < 3; ++comp) g.vn[comp][c] = (rvc * g.v[comp][c] * c1 + Fm[comp] - F[comp]) / den;
 }
 
-template <class R>
+template <class R, bool RKE>
 __global__ void __launch_bounds__(128) k_mom_x(MomArgs<R> g) {
   const int lane = (int)threadIdx.x;                        // blockDim.x == 32: one warp per row
   const int ix = -1 + (int)blockIdx.x * 31 + lane;          // face / vertex x position
@@ -644,14 +653,14 @@ __global__ void __launch_bounds__(128) k_mom_x(MomArgs<R> g) {
   const R dt = (R)g.sc[g.dt_slot];
   const int c = ix + g.sx * iy + g.sxy * iz;
   R F[3] = {R(0), R(0), R(0)};
-  if (ix <= g.nx) mom_flux(g, c, iy, iz, dt, F);            // faces -1..n
+  if (ix <= g.nx) mom_flux<R, RKE>(g, c, iy, iz, dt, F);    // faces -1..n
   R Fm[3];
 #pragma unroll
   for (int comp = 0; comp < 3; ++comp) Fm[comp] = __shfl_up_sync(0xffffffffu, F[comp], 1);
   if (lane >= 1 && ix >= 0 && ix <= g.nx) mom_update(g, c, Fm, F);
 }
 
-template <class R>
+template <class R, bool RKE>
 __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 6 : 8) k_mom_march(MomArgs<R> g) {
   const int t0 = (int)(blockIdx.x * blockDim.x + threadIdx.x);  // x, 0..nx
   const int t1 = (int)(blockIdx.y * blockDim.y + threadIdx.y);  // the third axis, 0..n3
@@ -671,8 +680,12 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 6 : 8) k_mom_march(MomAr
     for (int q = 0; q < 4; ++q) w[comp][q] = g.v[comp][c + (q - 1) * SA];
   R va0 = g.va[c], va1 = g.va[c + SA], rvc = g.rv[c], rvn = g.rv[c + SA];
   R dbw0 = g.db1[c], dbw1 = g.db1[c + SA], dbw2 = g.db1[c + 2 * SA], dcw0 = g.dc1[c], dcw1 = g.dc1[c + SA];
-  R Fm[3];
-  mom_flux_vals(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, Fm);
+  R Fm[3], fpre[3];
+  mom_flux_vals<R, false, RKE>(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, Fm, fpre);
+  if constexpr (RKE) {
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) g.fp[comp][c] = fpre[comp];
+  }
   for (int ia = ia0; ia <= ia1; ++ia) {
     c += SA;
 #pragma unroll
@@ -692,7 +705,11 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 6 : 8) k_mom_march(MomAr
     dcw0 = dcw1;
     dcw1 = g.dc1[c + SA];
     R F[3];
-    mom_flux_vals(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, F);
+    mom_flux_vals<R, false, RKE>(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, F, fpre);
+    if constexpr (RKE) {
+#pragma unroll
+      for (int comp = 0; comp < 3; ++comp) g.fp[comp][c] = fpre[comp];
+    }
     // K9's update at c: fluxes at faces c - e_A and c
     const R c1 = g.cv1v[c], den = g.cv2v[c] * g.rv1[c];
 #pragma unroll
@@ -1076,52 +1093,38 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     gm.sxy = sxy;
     gm.SA = SA;
     gm.S3 = A == 1 ? sxy : sx;
-    const int k = run.prof_begin(A == 0 ? "remap_sweep_mom_x" : "remap_sweep_mom_march", 0, 14, (double)(nx + 1) * (ny + 1) * (nz + 1));
+    const bool rke = run.p.rke != 0;
+    for (int q = 0; q < 3; ++q) gm.fp[q] = rke ? Ar.rke_f[q].p : nullptr;
+    const int k = run.prof_begin(A == 0 ? "remap_sweep_mom_x" : "remap_sweep_mom_march", 0, rke ? 17 : 14,
+                                 (double)(nx + 1) * (ny + 1) * (nz + 1));
     if (A == 0) {
       dim3 grd((nx + 1 + 30) / 31, (ny + 1 + 3) / 4, nz + 1);
-      k_mom_x<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gm);
+      if (rke)
+        k_mom_x<R, true><<<grd, dim3(32, 4, 1), 0, run.s>>>(gm);
+      else
+        k_mom_x<R, false><<<grd, dim3(32, 4, 1), 0, run.s>>>(gm);
     } else {
       dim3 grd((nx + 1 + 31) / 32, (gm.n3 + 1 + 3) / 4, (na + 1 + kMomA - 1) / kMomA);
-      k_mom_march<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gm);
+      if (rke)
+        k_mom_march<R, true><<<grd, dim3(32, 4, 1), 0, run.s>>>(gm);
+      else
+        k_mom_march<R, false><<<grd, dim3(32, 4, 1), 0, run.s>>>(gm);
     }
     run.prof_end(k);
     ++run.launches;
   }
   if (run.p.rke) {
     // rke (xremap.f90:664-695 and siblings): the old velocities are still
-    // in v (the new ones went to the q buffers).  R1 keeps the three fluxes
-    // before their product with dm (faces -1:n along A); R2 forms each
-    // vertex's defect dk per component; R3 adds, per cell 1:n, the dk of
-    // each vertex whose update scatters into it, for the components in file
-    // order and the vertices in the reference's loop order, so the sums are
-    // the reference's bit for bit.
-    MomArgs<R> gm;
-    gm.va = va;
-    gm.rv = rv;
-    gm.dmv = dmv;
-    gm.db1 = db1;
-    gm.dc1 = dc1;
-    gm.v[0] = Ar.vx.p;
-    gm.v[1] = Ar.vy.p;
-    gm.v[2] = Ar.vz.p;
-    gm.dct1 = dct1;
-    gm.dct2 = dct2;
-    gm.SA = SA;
-    R* const rf0 = Ar.rke_f[0].p;
-    R* const rf1 = Ar.rke_f[1].p;
-    R* const rf2 = Ar.rke_f[2].p;
+    // in v (the new ones went to the q buffers), and the momentum kernel
+    // above stored the three fluxes before their product with dm (faces
+    // -1:n along A).  R2 forms each vertex's defect dk per component; R3
+    // adds, per cell 1:n, the dk of each vertex whose update scatters into
+    // it, for the components in file order and the vertices in the
+    // reference's loop order, so the sums are the reference's bit for bit.
+    const R* const rf0 = Ar.rke_f[0].p;
+    const R* const rf1 = Ar.rke_f[1].p;
+    const R* const rf2 = Ar.rke_f[2].p;
     int lo[3] = {0, 0, 0}, hi[3] = {nx, ny, nz};
-    lo[A] = -1;
-    hi[A] = na;
-    LARE_BOXW(run, 13, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int ix, int iy, int iz) {
-      const int p3[3] = {ix, iy, iz};
-      const int c = ix + sx * iy + sxy * iz;
-      R F[3];
-      mom_flux<R, true>(gm, c, p3[T1], p3[T2], (R)sc[dt_slot], F);
-      rf0[c] = F[0];
-      rf1[c] = F[1];
-      rf2[c] = F[2];
-    });
     R* const dke = Ar.delta_ke.p;
     const R* const vv0 = Ar.vx.p;
     const R* const vv1 = Ar.vy.p;
