@@ -210,17 +210,73 @@ inline void rbox(Run<R>& run, const char* func, int line, int words, int i0, int
 // BC_USER ghost fills rewrite every ghost right after; an open side is never
 // refilled, so with an open side every point of the array's bounds [lo, hi]
 // outside the updated box [a, b] is carried from the old buffer.
+// The shell [lo, hi] minus [a, b] as six disjoint slabs (x below and above
+// over the whole y, z range, then y below and above within a's x range,
+// then z below and above within a's x and y ranges), walked by one flat
+// index; up to three arrays share the walk.
+template <class R>
+struct CarryArgs {
+  R* dst[3];
+  const R* src[3];
+  int narr, sx, sxy;
+  int box[6][6];         // i0, i1, j0, j1, k0, k1 per slab
+  long long start[7];    // first flat index of each slab; start[6] = total
+};
+
+template <class R>
+__global__ void __launch_bounds__(256) k_carry(CarryArgs<R> g) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.start[6]) return;
+  int s = 0;
+  while (t >= g.start[s + 1]) ++s;  // at most five steps
+  const int* q = g.box[s];
+  const long long r = t - g.start[s];
+  const long long e0 = q[1] - q[0] + 1, e1 = q[3] - q[2] + 1;
+  const int i = q[0] + (int)(r % e0);
+  const int j = q[2] + (int)((r / e0) % e1);
+  const int k = q[4] + (int)(r / (e0 * e1));
+  const int c = i + g.sx * j + g.sxy * k;
+  for (int m = 0; m < g.narr; ++m) g.dst[m][c] = g.src[m][c];
+}
+
+template <class R>
+inline void carry_outside_n(Run<R>& run, int narr, R* const* dst, const R* const* src, const int lo[3],
+                            const int hi[3], const int a[3], const int b[3]) {
+  if (!run.any_open) return;
+  CarryArgs<R> g;
+  g.narr = narr;
+  g.sx = run.sx;
+  g.sxy = run.sxy;
+  for (int m = 0; m < 3; ++m) {
+    g.dst[m] = m < narr ? dst[m] : nullptr;
+    g.src[m] = m < narr ? src[m] : nullptr;
+  }
+  const int slab[6][6] = {
+      {lo[0], a[0] - 1, lo[1], hi[1], lo[2], hi[2]}, {b[0] + 1, hi[0], lo[1], hi[1], lo[2], hi[2]},
+      {a[0], b[0], lo[1], a[1] - 1, lo[2], hi[2]},   {a[0], b[0], b[1] + 1, hi[1], lo[2], hi[2]},
+      {a[0], b[0], a[1], b[1], lo[2], a[2] - 1},     {a[0], b[0], a[1], b[1], b[2] + 1, hi[2]}};
+  long long tot = 0;
+  for (int s = 0; s < 6; ++s) {
+    for (int d = 0; d < 6; ++d) g.box[s][d] = slab[s][d];
+    g.start[s] = tot;
+    const long long n0 = slab[s][1] - slab[s][0] + 1, n1 = slab[s][3] - slab[s][2] + 1,
+                    n2 = slab[s][5] - slab[s][4] + 1;
+    if (n0 > 0 && n1 > 0 && n2 > 0) tot += n0 * n1 * n2;
+  }
+  g.start[6] = tot;
+  if (tot == 0) return;
+  const int k = run.prof_begin("carry_outside", 0, 2 * narr, (double)tot);
+  k_carry<R><<<(unsigned)((tot + 255) / 256), 256, 0, run.s>>>(g);
+  run.prof_end(k);
+  ++run.launches;
+}
+
 template <class R>
 inline void carry_outside(Run<R>& run, R* dst, const R* src, const int lo[3], const int hi[3], const int a[3],
                           const int b[3]) {
-  if (!run.any_open) return;
-  const int sx = run.sx, sxy = run.sxy;
-  const int a0 = a[0], a1 = a[1], a2 = a[2], b0 = b[0], b1 = b[1], b2 = b[2];
-  LARE_BOX(run, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], [=] __device__(int i, int j, int k) {
-    if (i >= a0 && i <= b0 && j >= a1 && j <= b1 && k >= a2 && k <= b2) return;
-    const int c = i + sx * j + sxy * k;
-    dst[c] = src[c];
-  });
+  R* const d[1] = {dst};
+  const R* const s[1] = {src};
+  carry_outside_n(run, 1, d, s, lo, hi, a, b);
 }
 
 // the three velocity components after an update of the nodes 0:n
@@ -228,7 +284,8 @@ template <class R>
 inline void carry_velocity(Run<R>& run, R* const nv[3], R* const ov[3]) {
   const int lo[3] = {-2, -2, -2}, hi[3] = {run.n[0] + 2, run.n[1] + 2, run.n[2] + 2};
   const int a[3] = {0, 0, 0}, b[3] = {run.n[0], run.n[1], run.n[2]};
-  for (int q = 0; q < 3; ++q) carry_outside(run, nv[q], ov[q], lo, hi, a, b);
+  const R* const src[3] = {ov[0], ov[1], ov[2]};
+  carry_outside_n(run, 3, nv, src, lo, hi, a, b);
 }
 
 template <class R>
