@@ -239,3 +239,25 @@ def test_cooling_term_first_step_is_the_weighted_heating():
     assert np.all(s.get_field("cool_term_b") >= 0.0) and s.get_field("cool_term_b").max() > 0.0
     inner = (slice(2, n + 2),) * 3
     assert s.get_field("energy")[inner].sum() < out[0].get_field("energy")[inner].sum()
+
+
+# ---------------------------------------------------------------------
+# The bounds-checked oracle build (every array access checked against the
+# reference's Fortran bounds) over the widened physics, six steps each (all
+# six Strang orderings of the remap).
+
+@pytest.mark.parametrize("case", ["pip_all", "radiation_open"])
+def test_widened_physics_bounds_checked(case):
+    from lare3d_b200.abi import BC_OPEN
+    from oracle import oracle
+    if case == "pip_all":
+        d = decks.partially_ionised(10, eta_bar=1e-2, rke=1, cooling_term=1, conduction=1, kappa_0=1e-2)
+    else:
+        d = decks.radiative_blast(10, rke=1, cooling_term=1, xbc_min=BC_OPEN, xbc_max=BC_OPEN)
+    s = oracle.simulation(d, checked=True)
+    s.start(d.state)
+    for k in range(1, 7):
+        s.step(k)
+    st = s.download()
+    for f in STATE:
+        assert np.isfinite(st[f]).all(), f
