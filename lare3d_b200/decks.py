@@ -7,6 +7,11 @@ and src/control.f90) for the three plain-method workloads:
 * ``conduction``     sheared arcade B = curl(A_y e_y), A_y = cos(kx) exp(-kz),
                      isobaric Gaussian hot spots, kappa_par ~ T^{5/2}, RKL2
 
+and for the widened physics: ``open_blast`` (characteristic boundaries),
+``partially_ionised`` (neutral fraction, Cowling resistivity) and
+``radiative_blast`` (optically thin losses); ``rke`` and ``cooling_term`` are
+switches on any deck.
+
 Each returns a :class:`Deck` with control parameters, grid metrics and the
 Fortran-bounded state; ghost cells are filled by the caller's
 boundary_conditions (lare3d.f90:65).  Random perturbations come from the
