@@ -119,6 +119,16 @@ typedef struct lare_params {
    */
   int cooling_term;
   double alpha_av;
+  /*
+   * coronal_heating (control.f90:142): each step, after the pressure is
+   * formed and before the shock viscosity (lagran.F90:127), the energy gains
+   * heat_in * dt / rho over the whole cell array, with the dt of the previous
+   * set_dt, then energy_bcs (radiative.f90:69-93 user_defined_heating).  The
+   * heating rate is the user hook's: set the cell field "heat_in" (Lare
+   * units, (-1:nx+2, -1:ny+2, -1:nz+2)) with lare_gpu_set_field; it is zero
+   * until set and is kept between steps.
+   */
+  int coronal_heating;
 } lare_params;
 
 /* Scalars of shared_data that the step updates. */

@@ -80,6 +80,7 @@ class LareParams(C.Structure):
         ("rke", C.c_int),
         ("cooling_term", C.c_int),
         ("alpha_av", C.c_double),
+        ("coronal_heating", C.c_int),
     ]
 
 
@@ -131,6 +132,7 @@ def default_params(**kw) -> LareParams:
     p.rke = 0
     p.cooling_term = 0
     p.alpha_av = 0.05
+    p.coronal_heating = 0
     p.mf = 1.2
     for k, v in kw.items():
         if not hasattr(p, k):

@@ -39,6 +39,7 @@ struct Par {
   int rke;                                             // the remap's kinetic-energy correction
   int cooling_term;                                    // lagran.F90:464, :1290
   double alpha_av;
+  int coronal_heating;                                 // lagran.F90:127
   double temp_norm, time_norm, rho_norm, mf;
   int bc[3][2];   // [dim][0=min,1=max]
   bool per[3];    // periodic communicator in this dimension (mpi_routines.F90:195-210)
@@ -69,6 +70,8 @@ struct Arrays {
   // cooling_term: moving averages of the viscous and ohmic heating
   // (shared_data.F90:109), persistent across steps
   A3<R> cool_term_v, cool_term_b;
+  // coronal_heating: the user's heating rate (user_defined_heating's heat_in)
+  A3<R> heat_in;
   // 1-D metrics (pointers at Fortran index 0)
   A1<R> dxb, dxc, dyb, dyc, dzb, dzc, grav;
   // reciprocals for conduction: 1/dxb, 1/dxc, 1/(dxc(i) + dxc(i-1)), per axis

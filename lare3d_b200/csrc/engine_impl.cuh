@@ -171,6 +171,7 @@ class EngineT : public EngineBase {
     p.rke = prm->rke;
     p.cooling_term = prm->cooling_term;
     p.alpha_av = prm->alpha_av;
+    p.coronal_heating = prm->coronal_heating;
     p.temp_norm = prm->temp_norm; p.time_norm = prm->time_norm; p.rho_norm = prm->rho_norm; p.mf = prm->mf;
     run.pip = p.eos_number != LARE_EOS_IDEAL;
     run.cowling = p.cowling_resistivity != 0;
@@ -219,6 +220,7 @@ class EngineT : public EngineBase {
         all.push_back(x);
     if (p.cooling_term)
       for (A3<R>* x : {&run.a.cool_term_v, &run.a.cool_term_b}) all.push_back(x);
+    if (p.coronal_heating) all.push_back(&run.a.heat_in);
     for (A3<R>* x : all) {
       R* base = dalloc<R>(run.elems, err);
       if (!base) return LARE_ENOMEM;
@@ -329,6 +331,7 @@ class EngineT : public EngineBase {
     if (run.a.xi.p) add("xi_n", &run.a.xi, -1, X + 2, -1, Y + 2, -1, Z + 2);
     if (run.a.eta_perp.p) add("eta_perp", &run.a.eta_perp, -1, X + 2, -1, Y + 2, -1, Z + 2);
     if (run.a.delta_ke.p) add("delta_ke", &run.a.delta_ke, -1, X + 2, -1, Y + 2, -1, Z + 2);
+    if (run.a.heat_in.p) add("heat_in", &run.a.heat_in, -1, X + 2, -1, Y + 2, -1, Z + 2);
     if (run.a.cool_term_v.p) {  // (1:n in the reference; the padding here holds zeros)
       add("cool_term_v", &run.a.cool_term_v, 1, X, 1, Y, 1, Z);
       add("cool_term_b", &run.a.cool_term_b, 1, X, 1, Y, 1, Z);

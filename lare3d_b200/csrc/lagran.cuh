@@ -366,6 +366,18 @@ void prologue_and_shock_viscosity(Run<R>& run) {
       cv_v[c] = R(0.125) * cvv;
     }
   });
+  if (run.p.coronal_heating) {
+    // lagran.F90:127 user_defined_heating (radiative.f90:88-91): after the
+    // pressure, before the viscosity; dt is still the previous set_dt's
+    R* const en = A.energy.p;
+    const R* hin = A.heat_in.p;
+    const double* scp = run.sc;
+    LARE_BOXW(run, 3, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+      const int c = ix + sx * iy + sxy * iz;
+      en[c] = en[c] + hin[c] * (R)scp[SC_DT] / rho[c];
+    });
+    energy_bcs(run);
+  }
   if (run.p.use_viscous_damping) viscous_damping(run);
   // LP2: cs_v (:561-581)
   R* const cs_v = A.cs_v.p;

@@ -234,6 +234,20 @@ def radiative_blast(n: int = 16, rho_norm: float = 1.0e-11, **over) -> Deck:
     return d
 
 
+def example_heating(d: Deck, time_norm: float, rho_norm: float, L_norm: float) -> np.ndarray:
+    """The heating rate of the reference's example hook (radiative.f90:69-93
+    user_defined_heating): 0.1 exp(-x^2 - y^2 - z^2) W/m^3 on cells 1:n,
+    zero on the ghosts, converted to Lare units; for the cell field
+    "heat_in" of a deck with coronal_heating on."""
+    from .abi import alloc
+    n0, n1, n2 = d.nx, d.ny, d.nz
+    h = alloc("cell", n0, n1, n2)
+    xc, yc, zc, *_ = _coords(d.metrics, n0, n1, n2)
+    rate = 0.1 * np.exp(-xc ** 2 - yc ** 2 - zc ** 2) * np.ones(h.shape)
+    h[2:n0 + 2, 2:n1 + 2, 2:n2 + 2] = rate[2:n0 + 2, 2:n1 + 2, 2:n2 + 2]
+    return np.asfortranarray(h * time_norm ** 3 / (rho_norm * L_norm ** 2))
+
+
 def _curl_edges(Ax, Ay, Az, m, n):
     """Discrete curl of periodic edge fields onto the face arrays.
 

@@ -157,6 +157,7 @@ struct lare_ref {
   bool eos_error = false;  // neutral.f90:171-174 'Temperature bounds problem'
   F3 delta_ke;             // rke (shared_data.F90:108, allocated mpi_routines.F90:313)
   F3 cool_term_v, cool_term_b;  // cooling_term (shared_data.F90:109, mpi_routines.F90:315-319)
+  F3 heat_in;                   // coronal_heating: user_defined_heating's rate (radiative.f90:73)
 
   // shared_data scalars.
   double time = 0.0, dt = 0.0, dt2 = 0.0, dtr = 0.0;
@@ -213,6 +214,7 @@ struct lare_ref {
     xi_n.fill(p.xi_n);
     if (p.cowling_resistivity) cell(eta_perp);
     if (p.rke) cell(delta_ke);
+    if (p.coronal_heating) cell(heat_in);
     if (p.cooling_term) {
       cool_term_v.alloc(1, N, 1, M, 1, L);
       cool_term_b.alloc(1, N, 1, M, 1, L);
@@ -237,6 +239,7 @@ struct lare_ref {
               {"xi_n", &xi_n}};
     if (p.cowling_resistivity) fields["eta_perp"] = &eta_perp;
     if (p.rke) fields["delta_ke"] = &delta_ke;
+    if (p.coronal_heating) fields["heat_in"] = &heat_in;
     if (p.cooling_term) {
       fields["cool_term_v"] = &cool_term_v;
       fields["cool_term_b"] = &cool_term_b;
@@ -630,6 +633,11 @@ struct lare_ref {
       cv_v(ix, iy, iz) = 0.125 * cvv;
     });
 
+    if (p.coronal_heating) {  // :127 user_defined_heating (radiative.f90:88-91)
+      for (size_t q = 0; q < energy.size(); ++q)
+        energy.d[q] = energy.d[q] + heat_in.d[q] * dt / rho.d[q];
+      energy_bcs();
+    }
     if (p.use_viscous_damping) viscous_damping();
     shock_viscosity();
     set_dt();

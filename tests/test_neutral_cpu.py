@@ -261,3 +261,37 @@ def test_widened_physics_bounds_checked(case):
     st = s.download()
     for f in STATE:
         assert np.isfinite(st[f]).all(), f
+
+
+# ---------------------------------------------------------------------
+# coronal_heating: the user_defined_heating hook (lagran.F90:127).
+
+def test_coronal_heating_adds_rate_times_previous_dt():
+    """A static uniform plasma under a uniform heating rate gains exactly
+    heat_in dt / rho in the first Lagrangian step, with the dt held before
+    set_dt (the hook runs first); the reference's example rate is zero on
+    the ghosts and positive inside."""
+    from lare3d_b200.abi import State, alloc
+    from oracle import oracle
+    n = 8
+    d = decks.blast(n, coronal_heating=1)
+    st = State.zeros(n, n, n)
+    st["rho"][...] = 2.0
+    st["energy"][...] = 1.5
+    d.state = st
+    norm = decks.normalisation()
+    ex = decks.example_heating(d, norm["time_norm"], norm["rho_norm"], 1.0e6)
+    assert ex[0].max() == 0.0 and ex[2:n + 2, 2:n + 2, 2:n + 2].min() > 0.0
+    heat = alloc("cell", n, n, n, 1.0e-3)
+    s = oracle.simulation(d)
+    s.upload(st)
+    s.set_field("heat_in", heat)
+    s.set_time(0.0, 0.01)
+    s.boundary_conditions()
+    s.eta_calc()
+    s.lagrangian_step(1)
+    inner = (slice(2, n + 2),) * 3
+    want = 1.5 + heat[inner] * 0.01 / 2.0
+    got = s.get_field("energy")[inner]
+    assert heat[inner].max() > 0.0
+    assert np.array_equal(got, want)

@@ -213,3 +213,19 @@ def test_cooling_term_fp32(built):
     for f in STATE:
         e = rel_l2(g.get_field(f), r.get_field(f))
         assert e <= 1e-5, f"{f}: rel L2 {e:.2e}"
+
+
+def test_coronal_heating_bitwise(built):
+    """The user_defined_heating hook with a caller-set heating rate."""
+    from lare3d_b200.abi import alloc
+    d = decks.orszag_tang(16, coronal_heating=1)
+    r, g = pair(d)
+    rng = np.random.default_rng(3)
+    heat = np.asfortranarray(alloc("cell", 16, 16, 16) + 1e-2 * rng.random(alloc("cell", 16, 16, 16).shape))
+    r.set_field("heat_in", heat)
+    g.set_field("heat_in", heat)
+    for s in range(1, 5):
+        r.step(s)
+        g.step(s)
+        assert_bitwise(g, r, STATE, f"step {s}")
+    assert np.array_equal(g.get_field("heat_in"), heat)
