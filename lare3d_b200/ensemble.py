@@ -105,12 +105,15 @@ class Ensemble:
     """Contexts for every deck, one eager step each, then one graph per
     launch of STEPS_PER_LAUNCH steps of all members."""
 
-    def __init__(self, deck_list: Sequence, precision=32, blocks: Optional[Dict[int, Tuple[int, int]]] = None):
+    def __init__(self, deck_list: Sequence, precision=32, blocks: Optional[Dict[int, Tuple[int, int]]] = None,
+                 fields: Optional[Dict[int, Dict[str, np.ndarray]]] = None):
         self.decks = list(deck_list)
         self.sims = []
-        for d in self.decks:
+        for i, d in enumerate(self.decks):
             s = gpu.simulation(d, precision=precision)
             s.start(d.state)
+            for name, arr in ((fields or {}).get(i) or {}).items():  # e.g. a member's heat_in
+                s.set_field(name, arr)
             if blocks and d.nx in blocks:
                 set_block(s, *blocks[d.nx])
             self.sims.append(s)

@@ -87,13 +87,17 @@ def test_ensemble_with_the_widened_physics(built):
     from lare3d_b200 import decks, gpu
     from lare3d_b200.ensemble import Ensemble
     ds = [decks.partially_ionised(12, eta_bar=1e-2), decks.radiative_blast(12),
-          decks.orszag_tang(12, rke=1), decks.partially_ionised(10, cowling=False, rke=1)]
-    ens = Ensemble(ds, precision=64)
+          decks.orszag_tang(12, rke=1), decks.partially_ionised(10, cowling=False, rke=1),
+          decks.open_blast(12, cooling_term=1), decks.orszag_tang(10, coronal_heating=1, cooling_term=1)]
+    heat = np.asfortranarray(np.full(ds[5].state["rho"].shape, 1e-3))
+    ens = Ensemble(ds, precision=64, fields={5: {"heat_in": heat}})
     ens.launch(1)
     ens.sync()
     for i, d in enumerate(ds):
         ref = gpu.simulation(d, precision=64)
         ref.start(d.state)
+        if i == 5:
+            ref.set_field("heat_in", heat)
         for s in range(1, 8):
             ref.step(s)
         got = ens.sims[i]
