@@ -564,10 +564,9 @@ struct MomArgs {
 // the three momentum fluxes through a face (K8's body) from its stencil
 // values: w[comp] = v at c-e_A, c, c+e_A, c+2e_A; db1 at c, c+e_A, c+2e_A;
 // dc1 at c, c+e_A; v1 (va), rho_v (rv) at c, c+e_A; dm at c
-// PRE: F is the flux before its product with dm (what rke's
-// kinetic-energy terms use, xremap.f90:664-695); BOTH: F is the product and
-// fpre[comp] receives the flux before it.
-template <class R, bool PRE = false, bool BOTH = false>
+// BOTH: fpre[comp] also receives the flux before its product with dm (what
+// rke's kinetic-energy terms use, xremap.f90:664-695).
+template <class R, bool BOTH = false>
 __device__ __forceinline__ void mom_flux_vals(R area, R va0, R va1, R rvc, R rvp, R dmc, R db0, R db1, R db2, R dc0,
                                               R dc1, const R (&w)[3][4], R dt, R (&F)[3], R* fpre = nullptr) {
   const R v_advect = (va0 + va1) * R(0.5);  // the face-averaged v1 of xremap.f90:257-265
@@ -595,7 +594,7 @@ __device__ __forceinline__ void mom_flux_vals(R area, R va0, R va1, R rvc, R rvp
     const R Di = sign_v * ss * fmin(fmin(fabs(Da) * dxbu, fabs(dfi)), fabs(dfu));
     const R f = fu + Di * (R(1) - dmu);
     if constexpr (BOTH) fpre[comp] = f;
-    F[comp] = PRE ? f : f * dmc;
+    F[comp] = f * dmc;
   }
 }
 
@@ -610,7 +609,7 @@ __device__ __forceinline__ void mom_flux(const MomArgs<R>& g, int c, int i1, int
 #pragma unroll
     for (int q = 0; q < 4; ++q) w[comp][q] = g.v[comp][c + (q - 1) * SA];
   R fpre[3];
-  mom_flux_vals<R, false, RKE>(g.dct1(i1) * g.dct2(i2), g.va[c], g.va[c + SA], g.rv[c], g.rv[c + SA], g.dmv[c],
+  mom_flux_vals<R, RKE>(g.dct1(i1) * g.dct2(i2), g.va[c], g.va[c + SA], g.rv[c], g.rv[c + SA], g.dmv[c],
                                g.db1[c], g.db1[c + SA], g.db1[c + 2 * SA], g.dc1[c], g.dc1[c + SA], w, dt, F, fpre);
   if constexpr (RKE) {
 #pragma unroll
@@ -681,7 +680,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 6 : 8) k_mom_march(MomAr
   R va0 = g.va[c], va1 = g.va[c + SA], rvc = g.rv[c], rvn = g.rv[c + SA];
   R dbw0 = g.db1[c], dbw1 = g.db1[c + SA], dbw2 = g.db1[c + 2 * SA], dcw0 = g.dc1[c], dcw1 = g.dc1[c + SA];
   R Fm[3], fpre[3];
-  mom_flux_vals<R, false, RKE>(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, Fm, fpre);
+  mom_flux_vals<R, RKE>(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, Fm, fpre);
   if constexpr (RKE) {
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) g.fp[comp][c] = fpre[comp];
@@ -705,7 +704,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 6 : 8) k_mom_march(MomAr
     dcw0 = dcw1;
     dcw1 = g.dc1[c + SA];
     R F[3];
-    mom_flux_vals<R, false, RKE>(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, F, fpre);
+    mom_flux_vals<R, RKE>(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, F, fpre);
     if constexpr (RKE) {
 #pragma unroll
       for (int comp = 0; comp < 3; ++comp) g.fp[comp][c] = fpre[comp];
