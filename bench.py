@@ -444,9 +444,10 @@ def main():
     e2e = {"value": replicas.whole_job_rate(ws, n3 * args.e2e_steps, e2e_el), "unit": "cell-updates/s",
            "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bi, "steps": args.e2e_steps}
 
-    # ---- the other forms (FP32, RKL2 conduction), rank 0 only
+    # ---- the other forms (FP32, RKL2 conduction, ...), one GPU only: with
+    # replicas the other ranks would wait for them at the closing barrier
     forms = {}
-    if rank == 0 and not args.no_forms:
+    if ws == 1 and not args.no_forms:
         s32 = gpu.simulation(deck, precision=32)
         s32.start(deck.state)
         s32.run(0, 2)
@@ -484,7 +485,7 @@ def main():
         forms["physics_fp64"] = physics_forms(torch, n, value)
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if ws == 1 and not args.no_cpu_baseline:  # the host-core baseline is an N = 1 figure
         cpu = cpu_baseline(deck, steps=1)
 
     if rank == 0:
