@@ -36,7 +36,7 @@ from typing import Optional
 import numpy as np
 
 from . import gpu
-from .abi import BC_USER, LARE_OK, LareError
+from .abi import BC_USER, EOS_IDEAL, LARE_OK, LareError
 
 # (cin padded, cout of the master weights, cin used, cout used by the forward)
 LAYERS = ((16, 32, 7, 32), (32, 32, 32, 32), (32, 32, 32, 32), (32, 16, 32, 1))
@@ -430,6 +430,9 @@ class SurrogateConduction:
 
     def __init__(self, sim, deck, net: Network, dt, bound=1e-3, col=64, fallback_fraction=0.5, seed=0,
                  check=True):
+        if sim.params.eos_number not in (0, EOS_IDEAL):
+            # the network and its re-check take T with one xi_n for the whole grid
+            raise ValueError("the conduction surrogate needs EOS_IDEAL (a constant neutral fraction)")
         torch = _torch()
         self.torch = torch
         self.sim, self.deck, self.net, self.dt = sim, deck, net, float(dt)

@@ -91,3 +91,14 @@ def test_window_metrics_repeat_on_a_power_of_two_grid():
     for i in range(-1, 13):
         gi = ((45 + i - 1) % 48) + 1
         assert w["dxb"][i + 1] == m2["dxb"][gi + 1]
+
+
+def test_surrogate_refuses_a_per_cell_neutral_fraction():
+    """The network and its exact re-check take the temperature with one xi_n
+    for the whole grid, so a partially ionised deck is refused up front."""
+    from types import SimpleNamespace
+    from lare3d_b200 import surrogate
+    from lare3d_b200.abi import EOS_ION
+    sim = SimpleNamespace(params=SimpleNamespace(eos_number=EOS_ION), nx=64, ny=64, nz=64)
+    with pytest.raises(ValueError, match="EOS_IDEAL"):
+        surrogate.SurrogateConduction(sim, None, None, 1.0)
