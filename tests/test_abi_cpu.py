@@ -130,3 +130,34 @@ def test_decks_are_consistent(built):
         assert a.flags.f_contiguous and np.isfinite(a).all(), k
     c = decks.conduction(8)
     assert c.dt_fixed > 0 and c.params.conduction == 1
+
+
+def test_widened_physics_argument_checks(built):
+    """lare_gpu_init rejects, on the host and before any device call, an
+    unknown EOS code and a partially ionised, Cowling or radiative run
+    without its constants; the oracle rejects the EOS code too."""
+    from lare3d_b200 import gpu
+    from lare3d_b200.abi import EOS_ION
+    lib = gpu.library()
+    d = decks.blast(8)
+    m = [np.ascontiguousarray(d.metrics[k]) for k in ("dxb", "dxc", "dyb", "dyc", "dzb", "dzc")]
+    ptr = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in m]
+    lib.lare_gpu_init.restype = C.c_int
+    out = C.c_void_p()
+    bad = [default_params(eos_number=4), default_params(eos_number=-1),
+           default_params(eos_number=EOS_ION),                      # no ionisation constants
+           default_params(cowling_resistivity=1),                   # likewise
+           default_params(radiation=1)]                             # no normalisation
+    for p in bad:
+        assert lib.lare_gpu_init(C.byref(p), 8, 8, 8, *ptr, 64, C.byref(out)) == -1
+        assert not out.value
+    c = decks.neutral_constants(EOS_ION)
+    ok = default_params(eos_number=EOS_ION, **c)
+    assert lib.lare_gpu_init(C.byref(ok), 8, 8, 8, *ptr, 64, C.byref(out)) in (0, -2)   # -2: no device here
+    if out.value:
+        lib.lare_gpu_destroy(out)
+    from oracle import oracle
+    rlib = oracle.library()
+    rout = C.c_void_p()
+    rlib.lare_ref_init.restype = C.c_int
+    assert rlib.lare_ref_init(C.byref(default_params(eos_number=5)), 8, 8, 8, *ptr, C.byref(rout)) == -1
