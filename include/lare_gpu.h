@@ -202,7 +202,9 @@ int lare_gpu_boundary_conditions(lare_ctx* ctx);
  * neutral.f90:158 neutral_fraction: xi_n over the whole cell array from rho
  * and energy by bisection on the temperature (a no-op under EOS_IDEAL).
  * LARE_EEOS where a cell's temperature bracket is empty (the reference
- * stops there).  lare_gpu_step and lare_gpu_run call it first in each step
+ * stops there); the context then keeps returning LARE_EEOS from the calls
+ * that check for it, like the run it replaces, so start a new context to
+ * continue.  lare_gpu_step and lare_gpu_run call it first in each step
  * (lare3d.f90:83), and the resistive sub-cycles and the RKL2 stages call it
  * where the reference does (lagran.F90:147, conduct.f90:404).
  */
