@@ -295,3 +295,28 @@ def test_coronal_heating_adds_rate_times_previous_dt():
     got = s.get_field("energy")[inner]
     assert heat[inner].max() > 0.0
     assert np.array_equal(got, want)
+
+
+def test_radiative_losses_power_law_band_closed_form():
+    """In the band where Q(T) = psi T^-2 (0.251-0.562 MK), dT/dt = -c psi T^-2
+    integrates to T'^3 = T^3 - 3 c psi dt, with the c of the constant band;
+    Townsend's exact step must reproduce it (its pow branch)."""
+    from lare3d_b200.abi import State
+    n = 8
+    d = decks.radiative_blast(n, rho_norm=1.0e-11)
+    p = d.params
+    g = p.gamma
+    T = 0.5e6
+    st = State.zeros(n, n, n)
+    st["rho"][...] = 1.0
+    st["energy"][...] = T * 2.0 / (g - 1.0) / p.temp_norm
+    d.state = st
+    s = _sim(d)
+    _, dt = s.step(1)
+    psi = 1e-13 * 10.0 ** -10.4
+    kb, mh = 1.3806488e-23, 1.672621777e-27
+    c = p.time_norm * 0.5 * (g - 1.0) * 1.0 * p.rho_norm / (kb * p.mf * mh)
+    T1 = (T ** 3 - 3.0 * c * psi * dt) ** (1.0 / 3.0)
+    assert 0.251e6 < T1 < 0.999 * T                    # a visible loss inside the band
+    got = s.get_field("energy")[2:n + 2, 2:n + 2, 2:n + 2]
+    assert np.allclose(got, T1 * 2.0 / (g - 1.0) / p.temp_norm, rtol=1e-9, atol=0.0)
