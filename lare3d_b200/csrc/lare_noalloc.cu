@@ -18,6 +18,7 @@
 // race on it; calls on one stream are ordered and safe.  Each call writes
 // every slot it later reads before reading it, so no slot has to start at
 // zero and nothing is cleared.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -28,29 +29,78 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr long long kPointsPerBlock = 8192;
-constexpr int kMaxBlocks = (int)(LARE_NOALLOC_MAX_POINTS / kPointsPerBlock);
+// One slot triple per block; a launch uses ceil(points / kPointsPerBlock)
+// blocks, so the array is sized by the same rounding.
+constexpr int kMaxBlocks = (int)((LARE_NOALLOC_MAX_POINTS + kPointsPerBlock - 1) / kPointsPerBlock);
+static_assert((long long)kMaxBlocks * kPointsPerBlock >= (long long)LARE_NOALLOC_MAX_POINTS,
+              "the scratch must hold one partial per block of the largest accepted grid");
 constexpr int kMaxDevices = 64;
 
 // Block partials: [block][0] en_b, [block][1] en_ke, [block][2] en_int.
 static __device__ __align__(256) double g_energy_scratch[3 * kMaxBlocks];
 
+// The scratch address is looked up once per CUDA context and cached with
+// that context's unique id (cuCtxGetId ids are never reused in a process).
+// After cudaDeviceReset, or when the primary context is released and made
+// again, the library image is loaded anew, possibly at another address; the
+// id then differs and the address is looked up again instead of reusing a
+// stale one.
+struct ScratchSlot {
+  unsigned long long ctx_id;
+  double* ptr;
+};
 std::mutex g_mu;
-double* g_scratch_ptr[kMaxDevices] = {};
+ScratchSlot g_slot[kMaxDevices] = {};
 
-// The device address of g_energy_scratch on the current device, resolved
-// once per device (cudaGetSymbolAddress with that device current).  In host
-// code the symbol name is only a stand-in and must not be passed to a kernel.
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+
+// The current context's id through the driver entry points the runtime
+// hands out (no link-time dependency on libcuda); 0 when unavailable, in
+// which case the address is looked up on every call.
+unsigned long long current_context_id() {
+  static PfnCtxGetCurrent get_current = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (PfnCtxGetCurrent)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (PfnCtxGetId)f;
+  }
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// The device address of g_energy_scratch in the current context
+// (cudaGetSymbolAddress with the caller's device current).  In host code
+// the symbol name is only a stand-in and must not be passed to a kernel.
 int scratch_for_current_device(double** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return LARE_ECUDA;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_ptr[dev]) {
+  // With no context current yet (id 0), the lookup below makes the device's
+  // primary context current, and its id is read after it.
+  const unsigned long long id = current_context_id();
+  ScratchSlot& s = g_slot[dev];
+  if (id == 0 || s.ctx_id != id || !s.ptr) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_energy_scratch);
     if (e != cudaSuccess || !p) return LARE_ECUDA;
-    g_scratch_ptr[dev] = (double*)p;
+    s.ptr = (double*)p;
+    s.ctx_id = id != 0 ? id : current_context_id();
   }
-  *out = g_scratch_ptr[dev];
+  *out = s.ptr;
   return LARE_OK;
 }
 

@@ -5,8 +5,11 @@ memory and cannot let the library call cudaMalloc (a fixed device pool, or
 no allocation between stream-ordered steps).  It must return what the
 context-based lare_gpu_energy returns for the same state, within the energy
 tolerance the other tests use (relative 1e-12), on consecutive calls that
-share its fixed scratch.  This file is collected last so that a run stopping
-at the first failure has already run every other test.
+share its fixed scratch.  Grids of one block (16^3: 4913 vertices, below the
+8192 points a block sums), of several blocks (32^3: 5 blocks) and a ragged
+grid (37 x 29 x 41: 6 blocks) cover the split of the cell and vertex loops
+across blocks and the strided final sum.  This file is collected last so that
+a run stopping at the first failure has already run every other test.
 """
 import ctypes as C
 
@@ -26,12 +29,32 @@ def entry():
     return fn
 
 
-def test_energy_noalloc_matches_context_energy(built):
+def _ragged_deck(nx, ny, nz, seed):
+    from lare3d_b200 import decks
+    from lare3d_b200.abi import State
+    from lare3d_b200.grid import grid
+    d = decks.orszag_tang(8)
+    m = grid(nx, ny, nz, (0, 1.1), (0, 0.9), (0, 1.6))
+    st = State.zeros(nx, ny, nz)
+    rng = np.random.default_rng(seed)
+    for k in STATE:
+        lo, hi = (0.5, 1.5) if k in ("rho", "energy") else (-0.3, 0.3)
+        st[k][...] = rng.uniform(lo, hi, st[k].shape)
+    return decks.Deck("ragged", d.params, nx, ny, nz, m, st, nsteps=2)
+
+
+def _decks():
+    from lare3d_b200 import decks
+    return [decks.orszag_tang(16), decks.orszag_tang(32), _ragged_deck(37, 29, 41, 5)]
+
+
+@pytest.mark.parametrize("case", [0, 1, 2], ids=["16^3-one-block", "32^3-five-blocks", "37x29x41-ragged"])
+def test_energy_noalloc_matches_context_energy(built, case):
     import torch
-    from lare3d_b200 import decks, gpu
+    from lare3d_b200 import gpu
     fn = entry()
-    n = 16
-    d = decks.orszag_tang(n)
+    d = _decks()[case]
+    nx, ny, nz = d.nx, d.ny, d.nz
     sim = gpu.simulation(d)
     sim.start(d.state)
     mets = [torch.from_numpy(np.ascontiguousarray(d.metrics[k])).cuda() for k in ("dxb", "dyb", "dzb")]
@@ -45,7 +68,7 @@ def test_energy_noalloc_matches_context_energy(built):
         st = sim.download()
         dev = [torch.from_numpy(st[k].ravel(order="F").copy()).cuda() for k in STATE]
         out = torch.full((3,), float("nan"), dtype=torch.float64, device="cuda")
-        rc = fn(n, n, n, *[t.data_ptr() for t in dev], *[t.data_ptr() for t in mets], out.data_ptr(), stream)
+        rc = fn(nx, ny, nz, *[t.data_ptr() for t in dev], *[t.data_ptr() for t in mets], out.data_ptr(), stream)
         assert rc == 0
         torch.cuda.synchronize()
         got = out.cpu().numpy()
