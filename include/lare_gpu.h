@@ -57,6 +57,11 @@ extern "C" {
 #define LARE_EEOS (-9)       /* neutral_fraction's temperature bracket is empty (neutral.f90:171-174) */
 
 /* Equations of state, shared_data.F90:73 (0 is taken as EOS_IDEAL). */
+/* Precision codes of lare_gpu_init. */
+#define LARE_FP64 64        /* FP64 drop-in: FMA contraction, shared reciprocals */
+#define LARE_FP64_EXACT 65  /* FP64, the reference's arithmetic bit for bit */
+#define LARE_FP32 32        /* FP32 form */
+
 #define LARE_EOS_IDEAL 1
 #define LARE_EOS_ION 2
 #define LARE_EOS_PI 3
@@ -147,10 +152,20 @@ typedef struct lare_ctx lare_ctx;
 /*
  * Create a context for an nx*ny*nz grid (each >= 4).  dxb/dxc etc. are the
  * Fortran grid metrics written by setup.F90:grid (:92-247); cv is formed on
- * the device as dxb*dyb*dzb exactly as setup.F90:239-245.  precision is 64
- * (FP64 drop-in) or 32 (FP32 form: field arithmetic in FP32, dt reduction,
- * budgets and RKL2 coefficients in FP64).  Replaces mpi_initialise's
- * allocation (mpi_routines.F90:295-334) for the device copy.
+ * the device as dxb*dyb*dzb exactly as setup.F90:239-245.  precision is
+ *   LARE_FP64 (64)        the FP64 drop-in: FP64 throughout, FMA contraction
+ *                         and reciprocals shared between quotients, so the
+ *                         last bits differ from the reference's (relative L2
+ *                         within 1e-10 per field after 100 steps);
+ *   LARE_FP64_EXACT (65)  FP64 with the reference's arithmetic: every multiply
+ *                         and add rounded separately, IEEE quotients in the
+ *                         reference's expression order, so the state equals a
+ *                         gfortran x86-64 build of the reference bit for bit
+ *                         (conduction's pow excepted); slower;
+ *   LARE_FP32 (32)        the FP32 form: field arithmetic in FP32, dt
+ *                         reduction, budgets and RKL2 coefficients in FP64.
+ * Replaces mpi_initialise's allocation (mpi_routines.F90:295-334) for the
+ * device copy.
  */
 int lare_gpu_init(const lare_params* params, int nx, int ny, int nz,
                   const double* dxb, const double* dxc,
@@ -283,9 +298,10 @@ int lare_gpu_energy(lare_ctx* ctx, double out[5]);
  * Its scratch is one fixed 96 KiB array in the library image that every GPU
  * loading the library keeps until the process exits.  All calls share it:
  * calls that overlap on the GPU (different streams without ordering) race
- * and give wrong sums; calls on one stream are safe.  The first call on each
- * device looks up the scratch address on that device (once); make that first
- * call before any stream capture begins.
+ * and give wrong sums; calls on one stream are safe.  The first call in each
+ * CUDA context (per device, and again after cudaDeviceReset) looks up the
+ * scratch address in that context; make that first call before any stream
+ * capture begins.
  */
 #define LARE_NOALLOC_MAX_POINTS 33554432
 int lare_gpu_energy_noalloc(int nx, int ny, int nz, const double* rho, const double* energy,

@@ -291,6 +291,7 @@ class Simulation:
         self.b = binding
         self.nx, self.ny, self.nz = nx, ny, nz
         self.params = params
+        self.precision = precision
         ctx = C.c_void_p()
         m = [np.ascontiguousarray(metrics[k], dtype=np.float64) for k in ("dxb", "dxc", "dyb", "dyc", "dzb", "dzc")]
         self._metrics = m

@@ -26,9 +26,11 @@ NVCC_COMMON = [
     "-Werror", "cross-execution-space-call", "-diag-suppress", "20011",
 ]
 
-# (source, extra flags).  The FP64 engine rounds every operation separately
-# (--fmad=false) to reproduce the reference's x86-64 arithmetic bit for bit.
+# (source, extra flags).  The exact FP64 engine rounds every operation
+# separately (--fmad=false) to reproduce the reference's x86-64 arithmetic bit
+# for bit; the product FP64 engine contracts multiply-adds.
 UNITS = [
+    ("engine_f64fast.cu", ["--fmad=true"]),
     ("engine_f64.cu", ["--fmad=false"]),
     ("engine_f32.cu", ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"]),
     ("lare_gpu.cu", []),

@@ -14,7 +14,9 @@
 #include <climits>
 #include <cstdint>
 
-namespace lare {
+#include "variant.h"
+
+LARE_BEGIN
 
 template <class R>
 struct A3 {
@@ -366,4 +368,4 @@ __device__ __forceinline__ void ghost_point(const GSpec& s, R* p0, R* p1, R* p2,
   }
 }
 
-}  // namespace lare
+LARE_END  // namespace lare

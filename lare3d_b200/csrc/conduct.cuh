@@ -27,7 +27,7 @@
 //   +Fz(c-ez), +Fy(c-ey), +Fx(c-ex), -Fx(c), -Fy(c), -Fz(c).
 #pragma once
 
-namespace lare {
+LARE_BEGIN
 
 constexpr int kCTX = 32, kCTY = 8, kCZ = 16;  // CTA tile (x, y) and z chunk
 constexpr int kCW = kCTX + 2;                 // plane row length with halo
@@ -270,4 +270,4 @@ void rkl2_stage(Run<R>& run, int line, const TempOf<R>& T, A3<R> y2, A3<R> y1, A
   ++run.launches;
 }
 
-}  // namespace lare
+LARE_END  // namespace lare

@@ -27,7 +27,7 @@
 #include "../../include/lare_gpu.h"
 #include "common.cuh"
 
-namespace lare {
+LARE_BEGIN
 
 struct Par {
   double gamma, visc1, visc2, eta_background, eta0, j_max, kappa_0, flux_limiter;
@@ -556,13 +556,13 @@ void copy_whole(Run<R>& run, A3<R> dst, A3<R> src) {
   run.prof_end(k);
 }
 
-}  // namespace lare
+LARE_END  // namespace lare
 
 #include "neutral.cuh"
 #include "radiative.cuh"
 #include "conduct.cuh"
 
-namespace lare {
+LARE_BEGIN
 
 // conduct.f90:299-416 heat_conduct_sts2, dt from sc[dt_slot]; the stage
 // count s must already be known on the host (run.n_s_stages).
@@ -708,11 +708,11 @@ __device__ __forceinline__ LimOut<R> limiter(R v_advect, R fm, R fi, R fp, R fp2
   return L;
 }
 
-}  // namespace lare
+LARE_END  // namespace lare
 
 #include "remap.cuh"
 
-namespace lare {
+LARE_BEGIN
 
 // remap.f90:33-131 eulerian_remap (the corrector's full remap; the
 // predictor's B-only remap is predictor_remap in lagran.cuh).
@@ -807,9 +807,9 @@ void energy_account(Run<R>& run) {
   }, SC_EN_KE, false);
 }
 
-}  // namespace lare
+LARE_END  // namespace lare
 
-namespace lare {
+LARE_BEGIN
 
 // diagnostics.F90:613-629 energy_correction, after eulerian_remap when rke
 // is on (lare3d.f90:86): the kinetic energy the remap lost, where it lost
@@ -828,11 +828,11 @@ void energy_correction(Run<R>& run) {
   energy_bcs(run);
 }
 
-}  // namespace lare
+LARE_END  // namespace lare
 
 #include "openbc.cuh"
 
-namespace lare {
+LARE_BEGIN
 
 template <int F, class R>
 inline void open_face(Run<R>& run, const OpenArgs<R>& g) {
@@ -872,6 +872,6 @@ void open_bcs(Run<R>& run) {
   open_face<5>(run, g);
 }
 
-}  // namespace lare
+LARE_END  // namespace lare
 
 #include "lagran.cuh"

@@ -47,10 +47,12 @@ class EngineBase {
   virtual void set_error(const std::string& e) = 0;
 };
 
-// Factories (engine_f64.cu, engine_f32.cu).  Return nullptr and fill err on
-// failure.
+// Factories (engine_f64fast.cu, engine_f64.cu, engine_f32.cu).  Return
+// nullptr and fill err on failure.
 EngineBase* make_engine_f64(const lare_params* p, int nx, int ny, int nz, const double* const* metrics6,
                             std::string& err);
+EngineBase* make_engine_f64_exact(const lare_params* p, int nx, int ny, int nz, const double* const* metrics6,
+                                  std::string& err);
 EngineBase* make_engine_f32(const lare_params* p, int nx, int ny, int nz, const double* const* metrics6,
                             std::string& err);
 

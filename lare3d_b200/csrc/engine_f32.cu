@@ -1,5 +1,8 @@
-// FP32 form: field arithmetic in FP32 (FMA contraction allowed); the CFL dt
-// reduction, budgets and RKL2 coefficients stay FP64 (engine.cuh).
+// FP32 form: field arithmetic in FP32 (FMA contraction, approximate
+// division); the CFL dt reduction, budgets and RKL2 coefficients stay FP64
+// (engine.cuh).
+#define LARE_VARIANT f32
+#define LARE_FAST 1
 #include "engine_impl.cuh"
 
 namespace lare {

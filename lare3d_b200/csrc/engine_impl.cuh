@@ -16,7 +16,7 @@
 #include "engine.cuh"
 #include "engine_base.h"
 
-namespace lare {
+LARE_BEGIN
 
 // Fortran bounds of each named array (mpi_routines.F90:295-334,
 // lagran.F90:56-81, xremap.f90:42-54, conduct.f90:41,319-321).
@@ -661,4 +661,4 @@ EngineBase* make_engine(const lare_params* p, int nx, int ny, int nz, const doub
   return e;
 }
 
-}  // namespace lare
+LARE_END  // namespace lare

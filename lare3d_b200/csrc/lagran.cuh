@@ -31,7 +31,7 @@
 
 #include <utility>
 
-namespace lare {
+LARE_BEGIN
 
 // Vertex current of eta_calc (lagran.F90:1190-1216), rkstep (:1479-1494)
 // and the predictor force (:358-373): the three places use the same
@@ -1069,4 +1069,4 @@ int lagrangian_step(Run<R>& run, int step) {
   return LARE_OK;
 }
 
-}  // namespace lare
+LARE_END  // namespace lare

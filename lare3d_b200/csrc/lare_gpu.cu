@@ -37,7 +37,7 @@ int lare_gpu_init(const lare_params* p, int nx, int ny, int nz, const double* dx
   *out = nullptr;
   if (!p || !dxb || !dxc || !dyb || !dyc || !dzb || !dzc) return LARE_EINVAL;
   if (nx < 4 || ny < 4 || nz < 4) return LARE_EINVAL;
-  if (precision != 64 && precision != 32) return LARE_EINVAL;
+  if (precision != LARE_FP64 && precision != LARE_FP64_EXACT && precision != LARE_FP32) return LARE_EINVAL;
   const int bcs[6] = {p->xbc_min, p->xbc_max, p->ybc_min, p->ybc_max, p->zbc_min, p->zbc_max};
   for (int q = 0; q < 6; ++q)
     if (!bc_supported(bcs[q])) return LARE_EINVAL;
@@ -56,8 +56,9 @@ int lare_gpu_init(const lare_params* p, int nx, int ny, int nz, const double* dx
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return LARE_ECUDA;
   const double* m6[6] = {dxb, dxc, dyb, dyc, dzb, dzc};
   std::string err;
-  lare::EngineBase* e = precision == 64 ? lare::make_engine_f64(p, nx, ny, nz, m6, err)
-                                        : lare::make_engine_f32(p, nx, ny, nz, m6, err);
+  lare::EngineBase* e = precision == LARE_FP64         ? lare::make_engine_f64(p, nx, ny, nz, m6, err)
+                       : precision == LARE_FP64_EXACT ? lare::make_engine_f64_exact(p, nx, ny, nz, m6, err)
+                                                      : lare::make_engine_f32(p, nx, ny, nz, m6, err);
   if (!e) return err.find("cudaMalloc") != std::string::npos ? LARE_ENOMEM : LARE_ECUDA;
   lare_ctx* c = new lare_ctx();
   c->e = e;

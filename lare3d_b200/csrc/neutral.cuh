@@ -17,7 +17,7 @@
 // identical paths on both.
 #pragma once
 
-namespace lare {
+LARE_BEGIN
 
 // exp(x) by Cody and Waite's argument reduction (W. J. Cody and W. Waite,
 // Software Manual for the Elementary Functions, 1980): x = k ln2 + r with
@@ -147,4 +147,4 @@ void perpendicular_resistivity(Run<R>& run) {
   });
 }
 
-}  // namespace lare
+LARE_END  // namespace lare

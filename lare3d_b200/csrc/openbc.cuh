@@ -13,7 +13,7 @@
 // within a face no point reads what another point writes.
 #pragma once
 
-namespace lare {
+LARE_BEGIN
 
 template <class R>
 struct OpenIn {
@@ -181,4 +181,4 @@ __global__ void __launch_bounds__(128) k_open_face(OpenArgs<R> g) {
   g.energy[at(gc)] = o.e0;
 }
 
-}  // namespace lare
+LARE_END  // namespace lare

@@ -13,7 +13,7 @@
 
 #include <cmath>
 
-namespace lare {
+LARE_BEGIN
 
 constexpr int kRadN = 7;  // temperature boundaries (radiative.f90:25)
 constexpr int kRadK = kRadN - 1;
@@ -117,4 +117,4 @@ void rad_losses(Run<R>& run, A3<R> er, A3<R> e0, int dt_slot) {
   ghost_flush(run, b);
 }
 
-}  // namespace lare
+LARE_END  // namespace lare

@@ -35,7 +35,7 @@
 
 #include <utility>
 
-namespace lare {
+LARE_BEGIN
 
 template <int A>
 __device__ __forceinline__ int acoord(int ix, int iy, int iz) {
@@ -1169,4 +1169,4 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   pass[A] = 0;
 }
 
-}  // namespace lare
+LARE_END  // namespace lare

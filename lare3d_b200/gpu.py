@@ -30,7 +30,13 @@ def binding() -> Binding:
     return Binding(library(), "lare_gpu_")
 
 
-def simulation(deck, precision: int = 64) -> Simulation:
+# Precision codes of lare_gpu_init (include/lare_gpu.h).
+FP64 = 64        # FP64 drop-in (product): FMA contraction, shared reciprocals
+EXACT64 = 65     # FP64 with the reference's arithmetic, bit for bit
+FP32 = 32        # FP32 form
+
+
+def simulation(deck, precision: int = FP64) -> Simulation:
     """A device context holding ``deck``'s grid and control parameters."""
     return Simulation(binding(), deck.params, deck.nx, deck.ny, deck.nz, deck.metrics, precision=precision)
 

@@ -485,7 +485,8 @@ class SurrogateConduction:
         m = dict(self.deck.metrics)
         m.update(window_metrics(self.deck.metrics, self.sim.nx, 0, wn, "x"))
         m.update(window_metrics(self.deck.metrics, self.sim.ny, 0, wn, "y"))
-        self.win = Simulation(gpu.binding(), wp, wn, wn, self.sim.nz, m, precision=32 if self.eb == 4 else 64)
+        self.win = Simulation(gpu.binding(), wp, wn, wn, self.sim.nz, m,
+                              precision=getattr(self.sim, "precision", 32 if self.eb == 4 else 64))
         self.halo_w = h
         self.wn = wn
 

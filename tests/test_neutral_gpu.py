@@ -19,11 +19,11 @@ from lare3d_b200.abi import BC_USER, EOS_ION, EOS_PI, LareError
 pytestmark = pytest.mark.gpu
 
 
-def pair(deck, precision=64):
+def pair(deck, precision=None):
     from lare3d_b200 import gpu
     from oracle import oracle
     r = oracle.simulation(deck)
-    g = gpu.simulation(deck, precision=precision)
+    g = gpu.simulation(deck, precision=gpu.EXACT64 if precision is None else precision)
     r.start(deck.state)
     g.start(deck.state)
     return r, g
