@@ -44,6 +44,10 @@ def parse():
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--out-dir", default=os.path.join(ROOT, "bench_out"),
                     help="where the clock samples and per-site profile tables go")
+    ap.add_argument("--case", default=None, choices=["mhd64", "mhd64x", "mhd32", "rkl64", "rkl32", "conv"],
+                    help="run one small case of a hot path and exit (for targeted ncu captures): "
+                         "two Orszag-Tang steps at --n^3 (FP64 product, FP64 exact, FP32), one RKL2 "
+                         "conduction step, or the surrogate network forward on --n windows")
     return ap.parse_args()
 
 
@@ -318,6 +322,37 @@ def ensemble_form(torch, count=48, launches=3):
             "autotune_s": t_tune, "dtype": "f32"}
 
 
+def workload(n):
+    """The workload name both arms print (same deck, same metric)."""
+    return f"resistive Orszag-Tang {n}^3 periodic, FP64, eta=1e-3, CFL 0.8"
+
+
+def run_case(what, n):
+    """A small, self-contained run of one hot path, for a targeted ncu
+    capture (ncu -k <kernel> -c 1 ... python bench.py --case <what> --n <n>)."""
+    import torch
+    from lare3d_b200 import decks, gpu
+    if what in ("mhd64", "mhd64x", "mhd32"):
+        d = decks.orszag_tang(n)
+        s = gpu.simulation(d, precision={"mhd64": 64, "mhd64x": gpu.EXACT64, "mhd32": 32}[what])
+        s.start(d.state)
+        for k in range(1, 3):
+            s.step(k)
+    elif what in ("rkl64", "rkl32"):
+        d = decks.conduction(n)
+        s = gpu.simulation(d, precision=64 if what == "rkl64" else 32)
+        s.start(d.state)
+        s.conduct_heat(d.dt_fixed)
+    else:
+        from lare3d_b200 import surrogate as S
+        net = S.Network(seed=0)
+        b = net.buffers(n, S.INFER_PATCH + 2 * S.HALO, False)
+        b["x"].normal_()
+        net.forward(b, n)
+    torch.cuda.synchronize()
+    print("ok", what, n)
+
+
 def run_reference(args):
     ws, rank, _ = dist_setup(args)
     if rank != 0:
@@ -343,8 +378,8 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded KISS perturbation of the Orszag-Tang state)",
-        "config": {"workload": f"resistive Orszag-Tang {args.n}^3 periodic, FP64, eta=1e-3, CFL 0.8",
-                   "grid": [args.n] * 3, "l2": "inputs larger than L2"},
+        "config": {"workload": workload(args.n), "grid": [args.n] * 3,
+                   "l2": "inputs larger than L2 (8 state arrays x 141 MB)"},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": oracle.num_threads(), "kind": "port",
                          "sample": f"{args.steps} steps after {args.warmup} warm-up steps (Fortran reference not buildable: no Fortran compiler)"},
         "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -356,6 +391,8 @@ def main():
     global OUT_DIR
     args = parse()
     OUT_DIR = args.out_dir
+    if args.case:
+        return run_case(args.case, args.n)
     if args.impl == "reference":
         return run_reference(args)
     ws, rank, local = dist_setup(args)
@@ -460,6 +497,15 @@ def main():
         forms["fp32"] = {"value": n3 * args.steps / el32, "unit": "cell-updates/s",
                          "ms_per_step": 1e3 * el32 / args.steps, "speedup_vs_fp64": (n3 * args.steps / el32) / value}
         s32.close()
+        sx = gpu.simulation(deck, precision=gpu.EXACT64)
+        sx.start(deck.state)
+        sx.run(0, 2)
+        stx = torch.cuda.ExternalStream(gpu.stream_of(sx))
+        elx = time_steps(sx, torch, stx, 2, args.steps)
+        forms["fp64_exact"] = {"value": n3 * args.steps / elx, "unit": "cell-updates/s",
+                               "ms_per_step": 1e3 * elx / args.steps,
+                               "note": "LARE_FP64_EXACT: the reference's arithmetic bit for bit (parity build)"}
+        sx.close()
         cdeck = decks.conduction(n)
         for prec in (64, 32):
             sc = gpu.simulation(cdeck, precision=prec)
@@ -494,12 +540,17 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded KISS perturbation of the Orszag-Tang state)",
-            "config": {"workload": f"resistive Orszag-Tang {n}^3 periodic, FP64 drop-in, eta=1e-3, CFL 0.8",
-                       "grid": [n, n, n], "l2": "inputs larger than L2 (8 state arrays x 141 MB)",
+            "config": {"workload": workload(n), "grid": [n, n, n],
+                       "l2": "inputs larger than L2 (8 state arrays x 141 MB)",
                        "parallelism": f"replicas x{ws}"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": launches,
-            "clocks": ck, "forms": forms,
+            "clocks": ck,
             "top_kernels": [{k: p[k] for k in ("site", "launches", "ms", "words")} for p in prof[:8]],
+            # last, so that a tail of the output keeps them: the widened
+            # physics and the ensemble first, the FP32 form at the very end
+            "forms": {k: forms[k] for k in ("physics_fp64", "ensemble", "surrogate_conduction",
+                                            "conduction_rkl2_fp64", "conduction_rkl2_fp32", "fp64_exact", "fp32")
+                      if k in forms},
         }
         print(json.dumps(line), flush=True)
     sim.close()
