@@ -322,6 +322,33 @@ def ensemble_form(torch, count=48, launches=3):
             "autotune_s": t_tune, "dtype": "f32"}
 
 
+def accuracy_forms(deck, steps=100):
+    """Per-field relative L2 after `steps` steps of the workload at its full
+    size: the FP64 product engine and the FP32 form against the exact FP64
+    engine, which reproduces the oracle bit for bit (the GPU parity tests
+    check that against the oracle itself on this workload at 128^3 for 100
+    steps); the oracle would need minutes per step here."""
+    import numpy as np
+    from lare3d_b200 import gpu
+    fields = ("rho", "energy", "vx", "vy", "vz", "bx", "by", "bz")
+    states = {}
+    for name, prec in (("exact", gpu.EXACT64), ("fp64", gpu.FP64), ("fp32", gpu.FP32)):
+        s = gpu.simulation(deck, precision=prec)
+        s.start(deck.state)
+        s.run(0, steps)
+        states[name] = s.download()
+        s.close()
+    ref = states["exact"]
+    out = {}
+    for name in ("fp64", "fp32"):
+        errs = {}
+        for f in fields:
+            b = ref[f]
+            errs[f] = float(np.linalg.norm(states[name][f] - b) / np.linalg.norm(b))
+        out[name] = {"steps": steps, "rel_l2_vs_fp64_exact": errs, "worst": max(errs.values())}
+    return out
+
+
 def workload(n):
     """The workload name both arms print (same deck, same metric)."""
     return f"resistive Orszag-Tang {n}^3 periodic, FP64, eta=1e-3, CFL 0.8"
@@ -480,6 +507,31 @@ def main():
     e2e_el = max_over_ranks(e0.elapsed_time(e1) / 1000.0, ws)
     e2e = {"value": replicas.whole_job_rate(ws, n3 * args.e2e_steps, e2e_el), "unit": "cell-updates/s",
            "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bi, "steps": args.e2e_steps}
+    # the floor a step through host buffers cannot beat: the same bytes copied
+    # by plain pinned-memory copies (one per array, each way) plus the
+    # device-resident step
+    big = max(v[0].numel() for v in host.values())
+    dev = torch.empty(big, dtype=torch.float64, device="cuda")
+    back = torch.empty(big, dtype=torch.float64, pin_memory=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for t, _ in host.values():
+            dev[:t.numel()].copy_(t, non_blocking=True)
+        e1.record(stream)
+    e1.synchronize()
+    t_h2d = e0.elapsed_time(e1) / 1000.0
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for t, _ in host.values():
+            back[:t.numel()].copy_(dev[:t.numel()], non_blocking=True)
+        e1.record(stream)
+    e1.synchronize()
+    t_d2h = e0.elapsed_time(e1) / 1000.0
+    del dev, back
+    floor_s = t_h2d + t_d2h + el_max / args.steps
+    e2e["copy_floor"] = {"h2d_gbs": bi / t_h2d / 1e9, "d2h_gbs": bi / t_d2h / 1e9,
+                         "ms_per_step": 1e3 * floor_s, "e2e_over_floor": (e2e_el / args.e2e_steps) / floor_s}
 
     # ---- the other forms (FP32, RKL2 conduction, ...), one GPU only: with
     # replicas the other ranks would wait for them at the closing barrier
@@ -529,6 +581,9 @@ def main():
         forms["surrogate_conduction"] = surrogate_form(torch, cdeck, forms.get("conduction_rkl2_fp32"))
         forms["ensemble"] = ensemble_form(torch)
         forms["physics_fp64"] = physics_forms(torch, n, value)
+        acc = accuracy_forms(deck)
+        forms["fp32"]["rel_l2_vs_fp64_exact"] = acc["fp32"]
+        forms["fp64_product_accuracy"] = acc["fp64"]
 
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:  # the host-core baseline is an N = 1 figure
@@ -549,7 +604,8 @@ def main():
             # last, so that a tail of the output keeps them: the widened
             # physics and the ensemble first, the FP32 form at the very end
             "forms": {k: forms[k] for k in ("physics_fp64", "ensemble", "surrogate_conduction",
-                                            "conduction_rkl2_fp64", "conduction_rkl2_fp32", "fp64_exact", "fp32")
+                                            "conduction_rkl2_fp64", "conduction_rkl2_fp32", "fp64_exact",
+                                            "fp64_product_accuracy", "fp32")
                       if k in forms},
         }
         print(json.dumps(line), flush=True)

@@ -251,3 +251,62 @@ def test_open_boundaries_let_waves_out(built):
     assert out["open"][0] < -1e-3
     assert abs(out["periodic"][0]) < 1e-13
     assert out["open"][1] < 0.2 * out["periodic"][1]
+
+
+def test_gravity_free_fall(built):
+    """Uniform state in a uniform gravity g (lagran.F90:379): no pressure or
+    magnetic force, so after one step every vertex has vz = -g dt."""
+    d = decks.blast(10)
+    st = d.state
+    st["energy"][...] = 0.1 / ((d.params.gamma - 1.0) * 1.0)
+    g0 = 0.7
+    s = oracle_sim(d)
+    s.start(st, grav=np.full(d.metrics["zc"].shape, g0))
+    s.step(1)
+    dt = s.scalars().dt
+    vz = s.get_field("vz")[2:-2, 2:-2, 2:-2]
+    assert np.abs(vz + g0 * dt).max() <= 1e-13 * g0 * dt
+    assert np.abs(s.get_field("vx")).max() <= 1e-13 * g0 * dt
+
+
+def test_gravity_bounds_checked(built):
+    d = decks.blast(8)
+    s = oracle_sim(d, checked=True)
+    zc = d.metrics["zc"]
+    s.start(d.state, grav=np.ascontiguousarray(0.5 * (1.0 + 0.3 * np.sin(2.0 * np.pi * zc))))
+    for st in range(1, 4):
+        s.step(st)
+
+
+def test_boris_limits_the_alfven_speed(built):
+    """boris with a binding va_max (lagran.F90:1104-1109): gamma_boris < 1
+    where B^2/rho >= va_max^2, equal to 1/(1 + B^2/(rho va_max^2)) there, and
+    the CFL step grows because the fast speed drops."""
+    va = 0.3
+    d = decks.orszag_tang(12, boris=1, va_max=va)
+    s = oracle_sim(d, checked=True)
+    s.start(d.state)
+    s.step(1)
+    d0 = decks.orszag_tang(12)
+    s0 = oracle_sim(d0)
+    s0.start(d0.state)
+    s0.step(1)
+    assert s.scalars().dt > s0.scalars().dt
+    gb = s.get_field("gamma_boris")
+    assert 0.0 < gb.min() < 0.6 and gb.max() == 1.0
+
+
+def test_restart_first_set_dt(built):
+    """A context created with restart set: its first set_dt takes
+    dt_from_restart and returns before advancing the time or recomputing
+    dtr (lagran.F90:1080-1086); the next one computes dt from the state."""
+    d = decks.blast(8)
+    d.params.restart, d.params.dt_from_restart = 1, 1.25e-3
+    s = oracle_sim(d, checked=True)
+    s.start(d.state, time=0.5)
+    s.step(1)
+    sc = s.scalars()
+    assert sc.dt == 1.25e-3 and sc.time == 0.5
+    s.step(2)
+    sc = s.scalars()
+    assert sc.dt != 1.25e-3 and sc.time == 0.5 + sc.dt
