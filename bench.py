@@ -267,11 +267,18 @@ def surrogate_form(torch, cdeck, plain):
            "plain_rkl2_fp32_ms_same_dt": 1e3 * t_plain, "speedup_vs_plain_rkl2": t_plain / times[True],
            "stages": stages, "network_forward_ms": 1e3 * t_fwd,
            "network_tflops": flops / t_fwd / 1e12, "network_flops_per_step": flops,
-           "rel_T_err_vs_rkl2": {"rms": float(np.sqrt(np.mean(rel ** 2))), "max": float(rel.max()),
-                                 "frac_cells_over_1e-3": float(np.mean(rel > 1e-3))},
+           # after the step (re-checked patches already replaced where they
+           # failed), over every cell of the grid: the 1e-3 bound is enforced
+           # on the re-checked patches only (1/16 of the grid per step); the
+           # other patches keep the network's error
+           "rel_T_err_vs_rkl2": {"rms": float(np.sqrt(np.mean(rel ** 2))), "max_all_patches": float(rel.max()),
+                                 "frac_cells_over_1e-3": float(np.mean(rel > 1e-3)),
+                                 "frac_patches_over_1e-3": float(np.mean(
+                                     rel.reshape(n // 16, 16, n // 16, 16, n // 16, 16).max(axis=(1, 3, 5)) > 1e-3))},
            "rel_T_err_without_network": {"rms": float(np.sqrt(np.mean(rel0 ** 2))), "max": float(rel0.max()),
                                          "frac_cells_over_1e-3": float(np.mean(rel0 > 1e-3))},
-           "recheck": {"patches": info.checked, "rejected": info.rejected, "max_err": info.max_err,
+           "recheck": {"patches": info.checked, "rejected": info.rejected,
+                       "max_err_rechecked_patches_before_rejection": info.max_err, "bound": 1e-3,
                        "fallback": info.fallback},
            "weights": os.path.relpath(S.DEFAULT_WEIGHTS, ROOT)}
     return out
@@ -513,21 +520,22 @@ def main():
     big = max(v[0].numel() for v in host.values())
     dev = torch.empty(big, dtype=torch.float64, device="cuda")
     back = torch.empty(big, dtype=torch.float64, pin_memory=True)
+    cs = torch.cuda.Stream()  # a stream of torch's own (the engine's is destroyed with the context)
     torch.cuda.synchronize()
-    with torch.cuda.stream(stream):
-        e0.record(stream)
+    with torch.cuda.stream(cs):
+        e0.record(cs)
         for t, _ in host.values():
             dev[:t.numel()].copy_(t, non_blocking=True)
-        e1.record(stream)
-    e1.synchronize()
-    t_h2d = e0.elapsed_time(e1) / 1000.0
-    with torch.cuda.stream(stream):
-        e0.record(stream)
+        e1.record(cs)
+        e1.synchronize()
+        t_h2d = e0.elapsed_time(e1) / 1000.0
+        e0.record(cs)
         for t, _ in host.values():
             back[:t.numel()].copy_(dev[:t.numel()], non_blocking=True)
-        e1.record(stream)
-    e1.synchronize()
-    t_d2h = e0.elapsed_time(e1) / 1000.0
+        e1.record(cs)
+        e1.synchronize()
+        t_d2h = e0.elapsed_time(e1) / 1000.0
+    torch.cuda.synchronize()
     del dev, back
     floor_s = t_h2d + t_d2h + el_max / args.steps
     e2e["copy_floor"] = {"h2d_gbs": bi / t_h2d / 1e9, "d2h_gbs": bi / t_d2h / 1e9,
@@ -609,6 +617,7 @@ def main():
                       if k in forms},
         }
         print(json.dumps(line), flush=True)
+    torch.cuda.synchronize()
     sim.close()
     barrier(ws)
     replicas.finish(ws)

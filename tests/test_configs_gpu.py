@@ -10,13 +10,21 @@ Each oracle run is made once and compared with every engine:
 * FP64 product engine (LARE_FP64: FMA contraction, shared reciprocals):
   relative L2 <= 1e-10 per field after the run, energy budgets within 1e-10;
 * FP64 exact engine (LARE_FP64_EXACT): bit for bit (conduction, whose T^2.5
-  is formed differently from the reference's pow, at relative L2 1e-12) and
-  energy budgets within 1e-12 (parallel sums);
+  is formed differently from the reference's pow, at relative L2 1e-12);
+* energy budgets: the oracle sums in the reference's serial order, whose own
+  rounding error over 10^6 - 10^7 positive terms reaches 1e-12 - 1e-11
+  relative, while the engines sum in a tree; so both are compared with the
+  exactly rounded sum (math.fsum) of the same FP64 products for the internal
+  energy: the engines within 1e-13, the oracle within 1e-10; the three
+  budgets of engine and oracle agree within 1e-10, and so does the drift of
+  the total energy over the run;
 * FP32 form: relative L2 <= 1e-5 per field against the FP64 oracle.
 
 div B stays at round-off on every engine: max |div B| * dx / max |B| < 1e-12.
 The measured errors are printed (pytest -s shows them).
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -77,6 +85,18 @@ def div_b_scaled(st, d):
     return float(np.abs(div_b(st, d.metrics, n)).max()) * dx / bmax
 
 
+def en_int_exact(st, d):
+    """diagnostics.F90:536-556's internal energy, sum of energy*rho*cv over
+    cells 1..n with cv = dxb*dyb*dzb (setup.F90:239-245), every product
+    rounded in FP64 as the reference forms it and the sum exactly rounded."""
+    n = d.nx
+    m = d.metrics
+    cv = (m["dxb"][2:n + 2][:, None, None] * m["dyb"][2:n + 2][None, :, None]) * m["dzb"][2:n + 2][None, None, :]
+    e = st["energy"][2:n + 2, 2:n + 2, 2:n + 2]
+    r = st["rho"][2:n + 2, 2:n + 2, 2:n + 2]
+    return math.fsum(((e * r) * cv).ravel())
+
+
 def _fields(case):
     return ["energy"] if oracle_run(case)[0].dt_fixed is not None else STATE
 
@@ -110,7 +130,14 @@ def test_fp64_exact_engine(built, case):
     got = gpu_run(case, gpu.EXACT64)
     errs = {f: rel_l2(got["fields"][f], ref["fields"][f]) for f in _fields(case)}
     de = max(abs(a - b) / max(abs(b), 1e-300) for a, b in zip(got["energy"][:3], ref["energy"][:3]))
-    _report(case, "FP64 exact", errs, f" energy {de:.2e}")
+    exact = en_int_exact(got["fields"], d)
+    eg = abs(got["energy"][2] - exact) / exact
+    eo = abs(ref["energy"][2] - en_int_exact(ref["fields"], d)) / exact
+    drift = sum(got["energy"][:3]) - sum(got["energy0"][:3])
+    drift_ref = sum(ref["energy"][:3]) - sum(ref["energy0"][:3])
+    dd = abs(drift - drift_ref) / abs(sum(ref["energy0"][:3]))
+    _report(case, "FP64 exact", errs, f" budgets {de:.2e} en_int vs exact sum: engine {eg:.1e} oracle {eo:.1e}"
+                                      f" drift {dd:.1e}")
     assert got["stages"] == ref["stages"]
     if d.dt_fixed is not None:
         for f, e in errs.items():
@@ -118,11 +145,10 @@ def test_fp64_exact_engine(built, case):
     else:
         for f in STATE:
             assert np.array_equal(got["fields"][f], ref["fields"][f]), f
-    assert de <= 1e-12
+    assert eg <= 1e-13 and eo <= 1e-10
+    assert de <= 1e-10
     # total-energy drift over the run equals the oracle's
-    drift = sum(got["energy"][:3]) - sum(got["energy0"][:3])
-    drift_ref = sum(ref["energy"][:3]) - sum(ref["energy0"][:3])
-    assert abs(drift - drift_ref) <= 1e-12 * abs(sum(ref["energy0"][:3]))
+    assert dd <= 1e-10
 
 
 @pytest.mark.parametrize("case", list(CASES))

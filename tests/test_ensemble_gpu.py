@@ -106,3 +106,46 @@ def test_ensemble_with_the_widened_physics(built):
             assert np.array_equal(a, b), (i, f, float(np.abs(a - b).max()))
         ref.close()
     ens.close()
+
+
+def test_snapshot_pairs_match_single_run_pairs(built):
+    """Training pairs from ensemble members (ensemble.snapshot_pairs): the
+    member state after a graph launch, loaded into a conduction context and
+    advanced by one plain RKL2 step, gives the same features and dT, bit for
+    bit, as the same deck stepped alone through lare_gpu_step and turned
+    into a pair by hand."""
+    import torch
+    from lare3d_b200 import decks, gpu
+    from lare3d_b200 import surrogate as S
+    from lare3d_b200.ensemble import Ensemble, member_deck, snapshot_pairs
+    ds = [member_deck(s) for s in specs()[:2]]
+    ens = Ensemble(ds, precision=32)
+    ens.launch(1)
+    ens.sync()
+    pairs = snapshot_pairs(ens, [0, 1])
+    meta = {"t_scale": 0.1, "rho_scale": 1.0}
+    for i, d in enumerate(ds):
+        ref = gpu.simulation(d, precision=32)
+        ref.start(d.state)
+        for s in range(1, ens.steps + 1):
+            ref.step(s)
+        st = ref.download()
+        ref.close()
+        p = decks.default_params(gamma=d.params.gamma, conduction=1, heat_flux_limiter=1, flux_limiter=0.1,
+                                 kappa_0=1.0e-3, dt_multiplier=0.9)
+        cd = decks.Deck("pair", p, d.nx, d.ny, d.nz, d.metrics, st, nsteps=1)
+        dt = 50.0 * decks.dt_parab_estimate(st, d.metrics, p, d.nx)
+        sim = gpu.simulation(cd, precision=32)
+        sim.start(st)
+        n = d.nx
+        feat = torch.empty((5, n, n, n), dtype=torch.float32, device="cuda")
+        dT = torch.empty((n, n, n), dtype=torch.float32, device="cuda")
+        S.extract(sim, feat, dT, 0, meta)
+        sim.conduct_heat(dt)
+        S.extract(sim, None, dT, 1, meta)
+        torch.cuda.synchronize()
+        sim.close()
+        assert torch.equal(pairs[i][0], feat), i
+        assert torch.equal(pairs[i][1], dT), i
+        assert float(dT.abs().max()) > 0.0, "the conduction step moves heat"
+    ens.close()
