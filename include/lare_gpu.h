@@ -56,12 +56,12 @@ extern "C" {
 #define LARE_ETOOLARGE (-8)  /* grid beyond a fixed-capacity entry point's limit */
 #define LARE_EEOS (-9)       /* neutral_fraction's temperature bracket is empty (neutral.f90:171-174) */
 
-/* Equations of state, shared_data.F90:73 (0 is taken as EOS_IDEAL). */
 /* Precision codes of lare_gpu_init. */
 #define LARE_FP64 64        /* FP64 drop-in: FMA contraction, shared reciprocals */
 #define LARE_FP64_EXACT 65  /* FP64, the reference's arithmetic bit for bit */
 #define LARE_FP32 32        /* FP32 form */
 
+/* Equations of state, shared_data.F90:73 (0 is taken as EOS_IDEAL). */
 #define LARE_EOS_IDEAL 1
 #define LARE_EOS_ION 2
 #define LARE_EOS_PI 3
@@ -374,6 +374,15 @@ const char* lare_gpu_last_error(lare_ctx* ctx);
  * equal the IEEE quotient bit for bit.  No counterpart in the reference.
  */
 int lare_gpu_check_division(const double* a, const double* b, long long n, double* out, void* stream);
+
+/*
+ * Self-check of the reciprocal the FP64 product engine (LARE_FP64) divides
+ * with: out[i] = 1 / b[i] by the hardware approximation refined by Newton-
+ * Raphson steps, for b of magnitude in [2^-1000, 2^1000]; each result must be
+ * within one ulp of the IEEE reciprocal.  Device pointers, enqueued on the
+ * given CUDA stream.  No counterpart in the reference.
+ */
+int lare_gpu_check_reciprocal(const double* b, long long n, double* out, void* stream);
 
 void lare_gpu_destroy(lare_ctx* ctx);
 

@@ -55,6 +55,11 @@ struct Num<float> {
 // a b, whose quotient a*rb is exact (a signed zero).  FP32 keeps the build's
 // division.
 __device__ __forceinline__ double div_rcp(double a, double b, double rb) {
+#if LARE_FAST
+  // product build: the product with the reciprocal (within 1.5 ulp)
+  (void)b;
+  return a * rb;
+#endif
   const unsigned ea = ((unsigned)__double2hiint(a) >> 20) & 0x7ffu;
   const unsigned eb = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
   if (ea - 523u > 1000u || eb - 523u > 1000u) return (a == 0.0 && eb - 523u <= 1000u) ? a * rb : a / b;
@@ -65,6 +70,55 @@ __device__ __forceinline__ double div_rcp(double a, double b, double rb) {
   return fma(r, rb, q);
 }
 __device__ __forceinline__ float div_rcp(float a, float b, float) { return a / b; }
+
+// Reciprocal of the product build: the hardware's approximate FP64
+// reciprocal (PTX rcp.approx.ftz.f64) refined by two steps of the
+// third-order Newton-Raphson iteration for 1/x: with e = 1 - x*y,
+// y <- y + y*(e + e^2) cubes the relative error, so any start better than
+// 2^-8 ends below 2^-53 before rounding (result within about one ulp of
+// 1/x).  For finite, normal x with |x| in [2^-1000, 2^1000]; the product
+// build divides only by cell widths, volumes, densities and similar
+// positive quantities in that range.  No branch, no slow path.
+__device__ __forceinline__ double fast_rcp(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(fma(e, e, e), y, y);
+  e = fma(-x, y, 1.0);
+  return fma(fma(e, e, e), y, y);
+}
+__device__ __forceinline__ float fast_rcp(float x) { return 1.0f / x; }
+
+// A quotient in the engine variant's arithmetic: IEEE a / b in the exact
+// builds, a times the reciprocal above in the product build (LARE_FAST),
+// within about two ulps of a / b.
+template <class R>
+__device__ __forceinline__ R qdiv(R a, R b) {
+#if LARE_FAST
+  return a * fast_rcp(b);
+#else
+  return a / b;
+#endif
+}
+// A divisor in the form a kernel carries between neighbouring points: the
+// value in the exact builds, its reciprocal in the product build; dv_div
+// divides by it.
+template <class R>
+__device__ __forceinline__ R dv_of(R x) {
+#if LARE_FAST
+  return fast_rcp(x);
+#else
+  return x;
+#endif
+}
+template <class R>
+__device__ __forceinline__ R dv_div(R a, R dv) {
+#if LARE_FAST
+  return a * dv;
+#else
+  return a / dv;
+#endif
+}
 
 // Scalar slots kept in device memory so that a whole step can run (and be
 // captured in a CUDA graph) without the host knowing dt.

@@ -104,13 +104,23 @@ __device__ __forceinline__ R face_q(R k0, R T0, R T1, R kn, R k1, R s1, R k2, R 
   return -k0 * pow25(tb) * (kn * (T1 - T0) + k1 * s1 + k2 * s2);
 }
 
-// Per-plane operands of one thread, loaded a plane ahead.  Thread (tx, ty)
-// owns the x face below its cell (plus the last face of the row for
-// tx = 31), the y face below its cell (plus the last one for ty = 7), the z
-// face above its cell, and the cell's own stage data.
+// Stage kernel.  A CTA of 32 x 8 threads owns a tile of 31 x 8 cells and
+// walks a chunk of z.  Each thread forms the x face flux on the low side of
+// its cell; lane 31's cell belongs to the next tile and only hands its low
+// face to lane 30 (the high face of every cell comes from the lane above by
+// a shuffle, so no lane forms a face twice).  Each thread also forms the y
+// face flux on the low side of its cell into shared memory, where the row
+// above reads it as its high face; the top row forms its high face itself.
+// The z face flux on the high side is carried to the next plane.  The
+// temperature of planes z-1, z, z+1 with a one-cell x/y halo sits in shared
+// memory, loaded a plane ahead.
+constexpr int kSTX = 31;  // cells per tile along x (a warp of 32 lanes)
+constexpr int kSW = kSTX + 2;
+constexpr int kSPlane = kSW * (kCTY + 2);
+
 template <class R>
 struct StagePre {
-  R kx[3], kx2[3], ky[3], ky2[3], kz[3];
+  R kx[3], ky[3], ky2[3], kz[3];
   R rho, y0, y1, y2, lc;
 };
 
@@ -119,66 +129,87 @@ struct StagePre {
 // else:  stage j: out = mu Y2 + nu Y1 + (1 - mu - nu) Y0 + mt dt Lc + gt dt Lc_Y0
 //        with Lc the flux of T(Y2) / rho.
 template <class R, bool FIRST>
-__global__ void __launch_bounds__(kCTX* kCTY, sizeof(R) == 4 ? 4 : 2) k_rkl2_stage(StageArgs<R> a, const double* __restrict__ sc) {
-  __shared__ R Ts[3][kCPlane];
-  __shared__ R fx[kCTY][kCTX + 1];
-  __shared__ R fy[kCTY + 1][kCTX];
+__global__ void __launch_bounds__(32 * kCTY, sizeof(R) == 4 ? 4 : 2)
+    k_rkl2_stage(StageArgs<R> a, const double* __restrict__ sc) {
+  __shared__ R Ts[3][kSPlane];
+  __shared__ R fy[kCTY + 1][32];
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const int tid = threadIdx.x;
-  const int tx = tid % kCTX, ty = tid / kCTX;
-  const int ix0 = 1 + blockIdx.x * kCTX, iy0 = 1 + blockIdx.y * kCTY;
+  const int lane = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * 32 + lane;
+  const int ix0 = 1 + blockIdx.x * kSTX, iy0 = 1 + blockIdx.y * kCTY;
   const int iz0 = 1 + blockIdx.z * kCZ;
   const int iz1 = min(nz, iz0 + kCZ - 1);
-  const int ix = ix0 + tx, iy = iy0 + ty;
-  const bool active = ix <= nx && iy <= ny;
-  // faces owned by this thread (see StagePre)
-  const bool hx = ix - 1 <= nx && iy <= ny;                              // x face at ix - 1
-  const bool hx2 = tx == kCTX - 1 && ix <= nx && iy <= ny;               // x face at ix (row end)
-  const bool hy = ix <= nx && iy - 1 <= ny;                              // y face at iy - 1
-  const bool hy2 = ty == kCTY - 1 && ix <= nx && iy <= ny;               // y face at iy (column end)
+  const int ix = ix0 + lane, iy = iy0 + ty;
+  // lane 31 only forms the x face below its cell (the high x face of lane 30)
+  const bool own = lane < kSTX;
+  const bool active = own && ix <= nx && iy <= ny;            // cells this tile updates
+  const bool hx = ix - 1 <= nx && iy <= ny;                   // x face at ix - 1 (low side)
+  const bool hy = own && ix <= nx && iy - 1 <= ny;            // y face at iy - 1 (low side)
+  const bool top = ty == kCTY - 1;                            // the top row also forms its high y face
+  const bool hy2 = own && top && ix <= nx && iy <= ny;
+  const bool cell = active;                                   // z faces of the cells updated here
+  const int sx = a.T.y.sx, sxy = a.T.y.sxy;
+  const int cxy = min(ix, nx + 2) + sx * min(iy, ny + 2);     // this thread's column (clamped)
+  // the (up to two) plane elements this thread loads, as column offsets
+  int off[2];
+  bool has[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int e = tid + q * 32 * kCTY;
+    has[q] = e < kSPlane;
+    const int jj = has[q] ? e / kSW : 0, ii = has[q] ? e - jj * kSW : 0;
+    off[q] = min(ix0 - 1 + ii, nx + 2) + sx * min(iy0 - 1 + jj, ny + 2);
+  }
+  const R tc = a.T.c, te0 = a.T.e0;
+  const R* __restrict__ ysrc = a.T.y.p;
   const R dt = (R)sc[a.dt_slot];
   auto load_plane = [&](int k) {
     R* d = Ts[(k + 3) % 3];
-    for (int e = tid; e < kCPlane; e += kCTX * kCTY) {
-      const int jj = e / kCW, ii = e - jj * kCW;
-      const int i = min(ix0 - 1 + ii, nx + 2), j = min(iy0 - 1 + jj, ny + 2);
-      d[e] = a.T(i, j, k);
-    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+      if (has[q]) d[tid + q * 32 * kCTY] = tc * (ysrc[off[q] + sxy * k] - te0);
   };
   auto fetch = [&](int k) {
     StagePre<R> q;
+    const int c = cxy + sxy * k;
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      q.kx[m] = hx ? a.k[m](ix - 1, iy, k) : R(0);
-      q.kx2[m] = hx2 ? a.k[m](ix, iy, k) : R(0);
-      q.ky[m] = hy ? a.k[3 + m](ix, iy - 1, k) : R(0);
-      q.ky2[m] = hy2 ? a.k[3 + m](ix, iy, k) : R(0);
-      q.kz[m] = active ? a.k[6 + m](ix, iy, k) : R(0);
+      q.kx[m] = hx ? a.k[m].p[c - 1] : R(0);
+      q.ky[m] = hy ? a.k[3 + m].p[c - sx] : R(0);
+      q.ky2[m] = hy2 ? a.k[3 + m].p[c] : R(0);
+      q.kz[m] = cell ? a.k[6 + m].p[c] : R(0);
     }
-    q.rho = active ? a.rho(ix, iy, k) : R(1);
-    q.y0 = active ? a.y0(ix, iy, k) : R(0);
-    q.y1 = (active && !FIRST) ? a.y1(ix, iy, k) : R(0);
-    q.y2 = (active && !FIRST) ? a.y2(ix, iy, k) : R(0);
-    q.lc = (active && !FIRST) ? a.lc0(ix, iy, k) : R(0);
+    q.rho = active ? a.rho.p[c] : R(1);
+    q.y0 = active ? a.y0.p[c] : R(0);
+    q.y1 = (active && !FIRST) ? a.y1.p[c] : R(0);
+    q.y2 = (active && !FIRST) ? a.y2.p[c] : R(0);
+    q.lc = (active && !FIRST) ? a.lc0.p[c] : R(0);
     return q;
   };
-  // z face above cell (lr, lc) of plane slots pm (lower) and pp (upper)
+  // z face above cell e of plane slots pm (lower) and pp (upper)
   auto zface = [&](const R* pm, const R* pp, int e, R k6, R k7, R k8) {
     return face_q(a.k0, pm[e], pp[e], k6, k7, (pp[e + 1] + pm[e + 1]) - (pp[e - 1] + pm[e - 1]), k8,
-                  (pp[e + kCW] + pm[e + kCW]) - (pp[e - kCW] + pm[e - kCW]));
+                  (pp[e + kSW] + pm[e + kSW]) - (pp[e - kSW] + pm[e - kSW]));
   };
-  const int ec = (ty + 1) * kCW + tx + 1;  // this thread's cell in a plane slot
+  // y face between cell e - kSW and cell e of plane slots Pm, P0, Pp
+  auto yface = [&](const R* Pm, const R* P0, const R* Pp, int e, const R (&k)[3]) {
+    const int b = e - kSW;
+    return face_q(a.k0, P0[b], P0[e], k[0], k[1], (P0[b + 1] + P0[e + 1]) - (P0[b - 1] + P0[e - 1]), k[2],
+                  (Pp[b] + Pp[e]) - (Pm[b] + Pm[e]));
+  };
+  const int ec = (ty + 1) * kSW + lane + 1;  // this thread's cell in a plane slot
   load_plane(iz0 - 1);
   load_plane(iz0);
   R fz_m = R(0);
   R b6 = R(0), b7 = R(0), b8 = R(0);
-  if (active) {
-    b6 = a.k[6](ix, iy, iz0 - 1);
-    b7 = a.k[7](ix, iy, iz0 - 1);
-    b8 = a.k[8](ix, iy, iz0 - 1);
+  if (cell) {
+    const int c = cxy + sxy * (iz0 - 1);
+    b6 = a.k[6].p[c];
+    b7 = a.k[7].p[c];
+    b8 = a.k[8].p[c];
   }
   __syncthreads();
-  if (active) fz_m = zface(Ts[(iz0 + 2) % 3], Ts[iz0 % 3], ec, b6, b7, b8);
+  if (cell) fz_m = zface(Ts[(iz0 + 2) % 3], Ts[iz0 % 3], ec, b6, b7, b8);
   StagePre<R> nxt = fetch(iz0);
   for (int iz = iz0; iz <= iz1; ++iz) {
     const StagePre<R> cur = nxt;
@@ -188,51 +219,38 @@ __global__ void __launch_bounds__(kCTX* kCTY, sizeof(R) == 4 ? 4 : 2) k_rkl2_sta
     const R* Pm = Ts[(iz + 2) % 3];
     const R* P0 = Ts[iz % 3];
     const R* Pp = Ts[(iz + 1) % 3];
+    R fx_lo = R(0);
     if (hx) {
-      const int e = ec - 1;  // cell ix - 1
-      fx[ty][tx] = face_q(a.k0, P0[e], P0[e + 1], cur.kx[0], cur.kx[1],
-                          (P0[e + kCW + 1] + P0[e + kCW]) - (P0[e - kCW + 1] + P0[e - kCW]), cur.kx[2],
-                          (Pp[e + 1] + Pp[e]) - (Pm[e + 1] + Pm[e]));
+      const int e = ec - 1;  // face between cells ix - 1 and ix
+      fx_lo = face_q(a.k0, P0[e], P0[e + 1], cur.kx[0], cur.kx[1],
+                     (P0[e + kSW + 1] + P0[e + kSW]) - (P0[e - kSW + 1] + P0[e - kSW]), cur.kx[2],
+                     (Pp[e + 1] + Pp[e]) - (Pm[e + 1] + Pm[e]));
     }
-    if (hx2) {
-      const int e = ec;
-      fx[ty][kCTX] = face_q(a.k0, P0[e], P0[e + 1], cur.kx2[0], cur.kx2[1],
-                            (P0[e + kCW + 1] + P0[e + kCW]) - (P0[e - kCW + 1] + P0[e - kCW]), cur.kx2[2],
-                            (Pp[e + 1] + Pp[e]) - (Pm[e + 1] + Pm[e]));
-    }
-    if (hy) {
-      const int e = ec - kCW;  // cell iy - 1
-      fy[ty][tx] = face_q(a.k0, P0[e], P0[e + kCW], cur.ky[0], cur.ky[1],
-                          (P0[e + 1] + P0[e + kCW + 1]) - (P0[e - 1] + P0[e + kCW - 1]), cur.ky[2],
-                          (Pp[e] + Pp[e + kCW]) - (Pm[e] + Pm[e + kCW]));
-    }
-    if (hy2) {
-      const int e = ec;
-      fy[kCTY][tx] = face_q(a.k0, P0[e], P0[e + kCW], cur.ky2[0], cur.ky2[1],
-                            (P0[e + 1] + P0[e + kCW + 1]) - (P0[e - 1] + P0[e + kCW - 1]), cur.ky2[2],
-                            (Pp[e] + Pp[e + kCW]) - (Pm[e] + Pm[e + kCW]));
-    }
+    const R fx_hi = __shfl_down_sync(0xffffffffu, fx_lo, 1);
+    if (hy) fy[ty][lane] = yface(Pm, P0, Pp, ec, cur.ky);
+    if (hy2) fy[kCTY][lane] = yface(Pm, P0, Pp, ec + kSW, cur.ky2);
     R fz_p = R(0);
-    if (active) fz_p = zface(P0, Pp, ec, cur.kz[0], cur.kz[1], cur.kz[2]);
+    if (cell) fz_p = zface(P0, Pp, ec, cur.kz[0], cur.kz[1], cur.kz[2]);
     __syncthreads();
     if (active) {
       R f = R(0);
       f = f + fz_m;
-      f = f + fy[ty][tx];
-      f = f + fx[ty][tx];
-      f = f - fx[ty][tx + 1];
-      f = f - fy[ty + 1][tx];
+      f = f + fy[ty][lane];
+      f = f + fx_lo;
+      f = f - fx_hi;
+      f = f - fy[ty + 1][lane];
       f = f - fz_p;
+      const int c = cxy + sxy * iz;
       if (FIRST) {
         const R lc = (R(1) / cur.rho) * f;
-        a.lc0(ix, iy, iz) = lc;
-        a.out(ix, iy, iz) = cur.y0 + a.mt * dt * lc;
+        a.lc0.p[c] = lc;
+        a.out.p[c] = cur.y0 + a.mt * dt * lc;
       } else {
         const R c0 = a.gt * dt * cur.lc;
         const R Lc = (R(1) / cur.rho) * f;
         const R c1 = a.mt * dt * Lc;
         const R v = a.mu * cur.y2 + a.nu * cur.y1 + a.omn * cur.y0;
-        a.out(ix, iy, iz) = v + c1 + c0;
+        a.out.p[c] = v + c1 + c0;
       }
     }
     fz_m = fz_p;
@@ -262,10 +280,10 @@ void rkl2_stage(Run<R>& run, int line, const TempOf<R>& T, A3<R> y2, A3<R> y1, A
   a.nx = nx;
   a.ny = ny;
   a.nz = nz;
-  dim3 grid((nx + kCTX - 1) / kCTX, (ny + kCTY - 1) / kCTY, (nz + kCZ - 1) / kCZ);
+  dim3 grid((nx + kSTX - 1) / kSTX, (ny + kCTY - 1) / kCTY, (nz + kCZ - 1) / kCZ);
   // words per point: T stencil input, 9 coefficients, rho, Lc_Y0, output (+ Y1, Y0 after stage 1)
   const int k = run.prof_begin("rkl2_stage", line, FIRST ? 13 : 15, (double)nx * ny * nz);
-  k_rkl2_stage<R, FIRST><<<grid, kCTX * kCTY, 0, run.s>>>(a, run.sc);
+  k_rkl2_stage<R, FIRST><<<grid, dim3(32, kCTY, 1), 0, run.s>>>(a, run.sc);
   run.prof_end(k);
   ++run.launches;
 }

@@ -304,14 +304,15 @@ inline void ghost(Run<R>& run, const GSpec& g, A3<R> a, A3<R>* b = nullptr, A3<R
 }
 
 // Deterministic sum of NV values over a box, into sc[slot..] (+=).
+// words: the algorithmic words per point the kernel moves (for the profile).
 template <int NV, class R, class Fn>
 inline void box_sum(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn, int slot, bool acc,
-                    int planes = kSumPlanes) {
+                    int words = 0, int planes = kSumPlanes) {
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   dim3 blk(64, 4, 1);
   dim3 grd((ni + 63) / 64, (nj + 3) / 4, (nk + planes - 1) / planes);
   int nb = grd.x * grd.y * grd.z;
-  int k = run.prof_begin("box_sum", 0, 0, (double)ni * nj * nk);
+  int k = run.prof_begin("box_sum", 0, words, (double)ni * nj * nk);
   k_box_sum<NV><<<grd, blk, 0, run.s>>>(i0, j0, k0, ni, nj, nk, planes, fn, run.partial);
   k_sum_partials<NV><<<1, 1024, 0, run.s>>>(run.partial, nb, run.sc + slot, acc ? 1 : 0);
   run.prof_end(k);
@@ -319,11 +320,11 @@ inline void box_sum(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1,
 }
 
 template <int NV, class R, class Fn>
-inline void box_min(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn, int uslot) {
+inline void box_min(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn, int uslot, int words = 0) {
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   dim3 blk(64, 4, 1);
   dim3 grd((ni + 63) / 64, (nj + 3) / 4, nk);
-  int k = run.prof_begin("box_min", 0, 0, (double)ni * nj * nk);
+  int k = run.prof_begin("box_min", 0, words, (double)ni * nj * nk);
   k_box_min<NV><<<grd, blk, 0, run.s>>>(i0, j0, k0, ni, nj, fn, run.us + uslot);
   run.prof_end(k);
   ++run.launches;
@@ -440,13 +441,13 @@ template <class R>
 __device__ __forceinline__ R edge_viscosity(R dvdots, R r1, R r2, R c1, R c2, R dvx, R dvy, R dvz, R dx, R dt,
                                             R visc1, R visc2_norm) {
   dvdots = -fabs(dvdots);
-  R rho_edge = R(2) * r1 * r2 / (r1 + r2);
+  R rho_edge = qdiv(R(2) * r1 * r2, r1 + r2);
   R cs_edge = fmin(c1, c2);
   R dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
   R dv = sqrt(dv2);
   R psi = R(0);
-  if (dv * dt / dx < R(1.e-14)) dvdots = R(0);
-  else dvdots = dvdots / dv;
+  if (qdiv(dv * dt, dx) < R(1.e-14)) dvdots = R(0);
+  else dvdots = qdiv(dvdots, dv);
   R vc = visc1 * cs_edge;
   R q_k_bar = rho_edge * (visc2_norm * dv + sqrt(visc2_norm * visc2_norm * dv2 + vc * vc));
   return q_k_bar * (R(1) - psi) * dvdots;
@@ -679,13 +680,20 @@ void heat_conduct_sts2(Run<R>& run, int dt_slot) {
 
 // ---------------------------------------------------------------------
 // Limited Van Leer flux shared by the *_flux routines of [xyz]remap.f90.
+//
+// Divisors arrive in carried form (dv_of): the value itself in the exact
+// builds, its reciprocal in the product build, so a kernel that moves along
+// a line forms each reciprocal once per point.  The exact builds evaluate
+// the reference's expressions unchanged; the product build takes the upwind
+// divisors by selection (vad_p is exactly 0 or 1, so the reference's
+// weighted sums dxcm*vad_p + dxcp*vad_m equal one of the two) and multiplies.
 template <class R>
 struct LimOut {
   R sign_v, vad_p, vad_m, fu, Di, dxbu, phi;
 };
 template <class R>
-__device__ __forceinline__ LimOut<R> limiter(R v_advect, R fm, R fi, R fp, R fp2, R dxci, R dxcm, R dxcp, R dxbi,
-                                             R dxbp, R dxu_p, R dxu_m, R dt, bool phi_from_dxu) {
+__device__ __forceinline__ LimOut<R> limiter_dv(R v_advect, R fm, R fi, R fp, R fp2, R dvci, R dvcm, R dvcp,
+                                                R dxbi, R dxbp, R dvu_p, R dvu_m, R dt, bool phi_from_dxu) {
   LimOut<R> L;
   R dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
   L.sign_v = copysign(R(1), v_advect);
@@ -693,19 +701,36 @@ __device__ __forceinline__ LimOut<R> limiter(R v_advect, R fm, R fi, R fp, R fp2
   L.vad_m = R(1) - L.vad_p;
   L.fu = fi * L.vad_p + fp * L.vad_m;
   R dfu = dfm * L.vad_p + dfp * L.vad_m;
-  R dxcu = dxcm * L.vad_p + dxcp * L.vad_m;
   L.dxbu = dxbi * L.vad_p + dxbp * L.vad_m;
+#if LARE_FAST
+  const bool up = !signbit(v_advect);
+  const R dvcu = up ? dvcm : dvcp;
   if (phi_from_dxu) {
-    R dxu = dxu_p * L.vad_p + dxu_m * L.vad_m;
+    L.phi = fabs(v_advect) * dt * (up ? dvu_p : dvu_m);
+  } else {
+    L.phi = fabs(v_advect) * dt * fast_rcp(L.dxbu);
+  }
+#else
+  R dvcu = dvcm * L.vad_p + dvcp * L.vad_m;
+  if (phi_from_dxu) {
+    R dxu = dvu_p * L.vad_p + dvu_m * L.vad_m;
     L.phi = fabs(v_advect) * dt / dxu;
   } else {
     L.phi = fabs(v_advect) * dt / L.dxbu;
   }
-  R Da = (R(2) - L.phi) * fabs(dfi) / dxci + (R(1) + L.phi) * fabs(dfu) / dxcu;
+#endif
+  R Da = dv_div((R(2) - L.phi) * fabs(dfi), dvci) + dv_div((R(1) + L.phi) * fabs(dfu), dvcu);
   Da = Da * (R(1) / R(6));
   R ss = R(0.5) * (copysign(R(1), dfi) + copysign(R(1), dfu));
   L.Di = L.sign_v * ss * fmin(fmin(fabs(Da) * L.dxbu, fabs(dfi)), fabs(dfu));
   return L;
+}
+// The same with plain divisors.
+template <class R>
+__device__ __forceinline__ LimOut<R> limiter(R v_advect, R fm, R fi, R fp, R fp2, R dxci, R dxcm, R dxcp, R dxbi,
+                                             R dxbp, R dxu_p, R dxu_m, R dt, bool phi_from_dxu) {
+  return limiter_dv(v_advect, fm, fi, fp, fp2, dv_of(dxci), dv_of(dxcm), dv_of(dxcp), dxbi, dxbp,
+                    phi_from_dxu ? dv_of(dxu_p) : dxu_p, phi_from_dxu ? dv_of(dxu_m) : dxu_m, dt, phi_from_dxu);
 }
 
 LARE_END  // namespace lare

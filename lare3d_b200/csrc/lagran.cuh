@@ -287,14 +287,15 @@ void resistive_update(Run<R>& run) {
     const int c = ix + sx * iy + sxy * iz;
     R e = energy[c];
     if (ix >= 1 && ix <= nx && iy >= 1 && iy <= ny && iz >= 1 && iz <= nz) {
-      R lh = +(curlb[c] + curlb[c - 1] + curlb[c - sx] + curlb[c - 1 - sx] + curlb[c - sxy] + curlb[c - 1 - sxy] +
-               curlb[c - sx - sxy] + curlb[c - 1 - sx - sxy]) * dt / (R(8) * rho[c]);
+      R lh = qdiv(+(curlb[c] + curlb[c - 1] + curlb[c - sx] + curlb[c - 1 - sx] + curlb[c - sxy] + curlb[c - 1 - sxy] +
+                    curlb[c - sx - sxy] + curlb[c - 1 - sx - sxy]) * dt,
+                  R(8) * rho[c]);
       ohmic[c] = ohmic[c] + lh;
       e = e + lh;
       if (ctb) {
         // the moving average of the heating of the iz plane's four
         // vertices only, as the reference writes it
-        const R lh4 = (curlb[c] + curlb[c - 1] + curlb[c - sx] + curlb[c - 1 - sx]) * dt / (R(4) * rho[c]);
+        const R lh4 = qdiv((curlb[c] + curlb[c - 1] + curlb[c - sx] + curlb[c - 1 - sx]) * dt, R(4) * rho[c]);
         const R t = alpha * lh4 + (R(1) - alpha) * ctb[c];
         ctb[c] = t;
         e = e - t;
@@ -308,7 +309,7 @@ void resistive_update(Run<R>& run) {
       if (iz == 0 || iz == nz) w1 = w1 * R(0.5);
       v[0] = (double)w1;
     }
-  }, SC_OHM_TOT, true);
+  }, SC_OHM_TOT, true, ctb ? 8 : 6);
   energy_bcs(run);
 }
 
@@ -352,7 +353,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
     pressure[c] = pr;
     R rmin = fmax(r, Num<R>::tiny());
     R b2 = bx1 * bx1 + by1 * by1 + bz1 * bz1;
-    cs[c] = sqrt((g * pr + gamma_boris[c] * b2) / rmin);
+    cs[c] = sqrt(qdiv(g * pr + gamma_boris[c] * b2, rmin));
     if (ix == -1 || ix == nx + 2 || iy == -1 || iy == ny + 2 || iz == -1 || iz == nz + 2)
       p_visc[c] = R(0);  // p_visc = 0 (:548) outside the 0:n+1 MAX loop
     if (ix <= nx + 1 && iy <= ny + 1 && iz <= nz + 1) {
@@ -362,7 +363,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
              rho[c + o4] * cv[c + o4] + rho[c + o5] * cv[c + o5] + rho[c + o6] * cv[c + o6] +
              rho[c + o7] * cv[c + o7];
       R cvv = cv[c] + cv[c + o1] + cv[c + o2] + cv[c + o3] + cv[c + o4] + cv[c + o5] + cv[c + o6] + cv[c + o7];
-      rho_v[c] = rv / cvv;
+      rho_v[c] = qdiv(rv, cvv);
       cv_v[c] = R(0.125) * cvv;
     }
   });
@@ -386,7 +387,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
     const int o1 = 1, o2 = sx, o3 = 1 + sx, o4 = sxy, o5 = 1 + sxy, o6 = sx + sxy, o7 = 1 + sx + sxy;
     R s = cs[c] * cv[c] + cs[c + o1] * cv[c + o1] + cs[c + o2] * cv[c + o2] + cs[c + o3] * cv[c + o3] +
           cs[c + o4] * cv[c + o4] + cs[c + o5] * cv[c + o5] + cs[c + o6] * cv[c + o6] + cs[c + o7] * cv[c + o7];
-    cs_v[c] = R(0.125) * s / cv_v[c];
+    cs_v[c] = qdiv(R(0.125) * s, cv_v[c]);
   });
   // LP3: alpha1 (0:n+1, 0:n+2, 0:n+2), alpha2 (-1:n+1, 0:n+1, 0:n+2),
   // alpha3 (-1:n+1, -1:n+1, 0:n+1)
@@ -449,7 +450,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
            R(0.25) * ddy * ddz * alpha1[c + Y + Z] * a7 - R(0.25) * ddx * ddz * alpha2[c - X + Z] * a8 -
            R(0.25) * ddx * ddy * alpha3[c] * a9 - R(0.25) * ddx * ddy * alpha3[c - X] * a10 -
            R(0.25) * ddx * ddy * alpha3[c - X - Y] * a11 - R(0.25) * ddx * ddy * alpha3[c - Y] * a12;
-    visc_heat[c] = vh / cv[c];
+    visc_heat[c] = qdiv(vh, cv[c]);
     if (ix <= nx && iy <= ny && iz <= nz) {
       R b1 = alpha1[c + Y + Z] * dyc(iy) * dzc(iz);
       R b2 = alpha1[c + X + Y + Z] * dyc(iy) * dzc(iz);
@@ -457,11 +458,12 @@ void prologue_and_shock_viscosity(Run<R>& run) {
       R b4 = alpha2[c + Y + Z] * dxc(ix) * dzc(iz);
       R b5 = alpha3[c] * dxc(ix) * dyc(iy);
       R b6 = alpha3[c + Z] * dxc(ix) * dyc(iy);
-      R cvv = cv_v[c];
+      const R cvv = dv_of(cv_v[c]);
       auto f = [&](const R* v) {
         R v0 = v[c];
-        return (b1 * (v0 - v[c - X]) + b2 * (v0 - v[c + X]) + b3 * (v0 - v[c - Y]) + b4 * (v0 - v[c + Y]) +
-                b5 * (v0 - v[c - Z]) + b6 * (v0 - v[c + Z])) / cvv;
+        return dv_div(b1 * (v0 - v[c - X]) + b2 * (v0 - v[c + X]) + b3 * (v0 - v[c - Y]) + b4 * (v0 - v[c + Y]) +
+                          b5 * (v0 - v[c - Z]) + b6 * (v0 - v[c + Z]),
+                      cvv);
       };
       fxv[c] = f(vx);
       fyv[c] = f(vy);
@@ -520,19 +522,20 @@ void set_dt(Run<R>& run) {
     const int c = ix + sx * iy + sxy * iz;
     R w1 = bx[c] * bx[c] + by[c] * by[c] + bz[c] * bz[c];
     R rho0 = fmax(rho[c], Num<R>::tiny());
-    R w2 = w1 / rho0;
+    const R dr = dv_of(rho0);
+    R w2 = dv_div(w1, dr);
     R gb = gamma_boris[c];
     if (boris && (w2 >= va_max2)) {
       gb = R(1) / (R(1) + w2 / va_max2);
       gamma_boris[c] = gb;
     }
-    R cs2 = (g * pressure[c] + gb * w1) / rho0;
-    R c_visc2 = p_visc[c] / rho0;
+    R cs2 = dv_div(g * pressure[c] + gb * w1, dr);
+    R c_visc2 = dv_div(p_visc[c], dr);
     R length = fmin(fmin(dxb(ix), dyb(iy)), dzb(iz));
-    R dt1 = length / (sqrt(c_visc2) + sqrt(cs2 + c_visc2));
+    R dt1 = qdiv(length, sqrt(c_visc2) + sqrt(cs2 + c_visc2));
     R dt_local = fmin(Num<R>::huge(), dt1);
-    R dt2 = fmin(fmin(dxb(ix) / fmax(fabs(vx[c]), Num<R>::tiny()), dyb(iy) / fmax(fabs(vy[c]), Num<R>::tiny())),
-                 dzb(iz) / fmax(fabs(vz[c]), Num<R>::tiny()));
+    R dt2 = fmin(fmin(qdiv(dxb(ix), fmax(fabs(vx[c]), Num<R>::tiny())), qdiv(dyb(iy), fmax(fabs(vy[c]), Num<R>::tiny()))),
+                 qdiv(dzb(iz), fmax(fabs(vz[c]), Num<R>::tiny())));
     dt_local = fmin(dt_local, dt2);
     R dt3 = Num<R>::huge();
     if (cowling) {  // lagran.F90:1132-1134
@@ -544,7 +547,7 @@ void set_dt(Run<R>& run) {
     }
     v[0] = (double)dt_local;
     v[1] = (double)dt3;
-  }, U_DTMIN);
+  }, U_DTMIN, cowling ? 11 : (resistive ? 10 : 9));
   const double mult = run.p.dt_multiplier;
   const bool f32 = sizeof(R) == 4;
   launch_scalar(run.s, run.launches, [=] __device__() {
@@ -719,7 +722,7 @@ __global__ void __launch_bounds__(128) k_shock_march(ShockArgs<R> g) {
            R(0.25) * ddy * ddz * al1yz * a7 - R(0.25) * ddx * ddz * al2xz * a8 -
            R(0.25) * ddx * ddy * alpha3_r[c] * a9 - R(0.25) * ddx * ddy * alpha3_r[c - X] * a10 -
            R(0.25) * ddx * ddy * alpha3_r[c - X - Y] * a11 - R(0.25) * ddx * ddy * alpha3_r[c - Y] * a12;
-    R v = vh / cv_r[c];
+    R v = qdiv(vh, cv_r[c]);
     vhp_r[c] = v > R(0) ? v : R(0);
     if (ix <= g.nx && iy <= g.ny && iz <= g.nz) {
 #pragma unroll
@@ -781,11 +784,12 @@ void predictor_corrector_step(Run<R>& run) {
     energy[c] = e;
     if (ix >= 0 && ix <= nx + 1 && iy >= 0 && iy <= ny + 1 && iz >= 0 && iz <= nz + 1) {
       const R dt2 = (R)sc[SC_DT2];
-      R dv = cv1[c] / cv[c] - R(1);
-      R e1 = e - pressure[c] * dv / rho[c];
-      e1 = e1 + visc_heat[c] * dt2 / rho[c];
+      const R rr = dv_of(rho[c]);
+      R dv = qdiv(cv1[c], cv[c]) - R(1);
+      R e1 = e - dv_div(pressure[c] * dv, rr);
+      e1 = e1 + dv_div(visc_heat[c] * dt2, rr);
       const R x = xin ? xin[c] : xi;
-      pressure[c] = (e1 - (R(1) - x) * ip) * (g - R(1)) * rho[c] * cv[c] / cv1[c];
+      pressure[c] = qdiv((e1 - (R(1) - x) * ip) * (g - R(1)) * rho[c] * cv[c], cv1[c]);
     }
   });
   // PC2 (0:n): vertex forces with the predicted B; half-step velocity
@@ -833,9 +837,10 @@ void predictor_corrector_step(Run<R>& run) {
     fz = fz + gb * (jx * byv - jy * bxv);
     R rv = rho_v[c];
     fz = fz - rv * grav(iz);
-    vx1[c] = vx[c] + dt2 * (fxv[c] + fx) / rv;
-    vy1[c] = vy[c] + dt2 * (fyv[c] + fy) / rv;
-    vz1[c] = vz[c] + dt2 * (fzv[c] + fz) / rv;
+    const R drv = dv_of(rv);
+    vx1[c] = vx[c] + dv_div(dt2 * (fxv[c] + fx), drv);
+    vy1[c] = vy[c] + dv_div(dt2 * (fyv[c] + fy), drv);
+    vz1[c] = vz[c] + dv_div(dt2 * (fzv[c] + fz), drv);
   });
   // B = B0 (:389-393)
   std::swap(A.bx.p, A.bx0.p);
@@ -892,6 +897,7 @@ void predictor_corrector_step(Run<R>& run) {
   R* const cv1w = A.cv1.p;
   R* const rhow = A.rho.p;
   R* const visc_dep = A.visc_dep.p;
+  const A1<R> rbx = A.rdb[0], rby = A.rdb[1], rbz = A.rdb[2];
   box_sum<1>(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
     const R dt = (R)sc[SC_DT];
     const int c = ix + sx * iy + sxy * iz;
@@ -902,15 +908,19 @@ void predictor_corrector_step(Run<R>& run) {
     R vybm = (vy1[c - Y] + vy1[c - X - Y] + vy1[c - Y - Z] + vy1[c - X - Y - Z]) * R(0.25);
     R vzb = (vz1[c] + vz1[c - X] + vz1[c - Y] + vz1[c - X - Y]) * R(0.25);
     R vzbm = (vz1[c - Z] + vz1[c - X - Z] + vz1[c - Y - Z] + vz1[c - X - Y - Z]) * R(0.25);
+#if LARE_FAST
+    R dv = ((vxb - vxbm) * rbx(ix) + (vyb - vybm) * rby(iy) + (vzb - vzbm) * rbz(iz)) * dt;
+#else
     R dv = ((vxb - vxbm) / dxb(ix) + (vyb - vybm) / dyb(iy) + (vzb - vzbm) / dzb(iz)) * dt;
+#endif
     cv1w[c] = cv[c] * (R(1) + dv);
     R vh = vhp[c];
     R r = rhow[c];
-    energy[c] = energy[c] + (dt * vh - dv * pressure[c]) / r;
+    energy[c] = energy[c] + qdiv(dt * vh - dv * pressure[c], r);
     visc_dep[c] = visc_dep[c] + dt * vh;
-    rhow[c] = r / (R(1) + dv);
+    rhow[c] = qdiv(r, R(1) + dv);
     v[0] = (double)(dt * vh * cv[c]);
-  }, SC_VISC_TOT, true);
+  }, SC_VISC_TOT, true, 13);
   if (run.p.cooling_term) {
     // :464-475: an exponential moving average of the viscous heating
     // (weight alpha_av) is taken off the energy of cells 1:n, then

@@ -26,6 +26,11 @@ __global__ void k_check_division(const double* a, const double* b, long long n, 
     out[i] = lare::div_rcp(a[i], b[i], rb);
   }
 }
+
+__global__ void k_check_reciprocal(const double* b, long long n, double* out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = lare::fast_rcp(b[i]);
+}
 }  // namespace
 
 extern "C" {
@@ -239,6 +244,14 @@ int lare_gpu_check_division(const double* a, const double* b, long long n, doubl
   if (n == 0) return LARE_OK;
   const long long blocks = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
   k_check_division<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(a, b, n, out);
+  return cudaGetLastError() == cudaSuccess ? LARE_OK : LARE_ECUDA;
+}
+
+int lare_gpu_check_reciprocal(const double* b, long long n, double* out, void* stream) {
+  if (n < 0 || (n > 0 && (!b || !out))) return LARE_EINVAL;
+  if (n == 0) return LARE_OK;
+  const long long blocks = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
+  k_check_reciprocal<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(b, n, out);
   return cudaGetLastError() == cudaSuccess ? LARE_OK : LARE_ECUDA;
 }
 

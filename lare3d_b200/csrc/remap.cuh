@@ -69,10 +69,11 @@ struct BfArgs {
   int n0, n1;                  // extents of the thread grid (-1..n+1 each)
 };
 
+// B / dbv at q, with dbv (in the carried divisor form dv_of) returned in dvb
 template <class R>
-__device__ __forceinline__ R bf_quot(const R* Bb, const R* db1, int q, int SB, R& dbv) {
-  dbv = (db1[q] + db1[q + SB]) * R(0.5);
-  return Bb[q] / dbv;
+__device__ __forceinline__ R bf_quot(const R* Bb, const R* db1, int q, int SB, R& dvb) {
+  dvb = dv_of((db1[q] + db1[q + SB]) * R(0.5));
+  return dv_div(Bb[q], dvb);
 }
 
 template <class R>
@@ -102,9 +103,9 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
     q20 = bf_quot(a.b2, a.db1, c, a.SB2, d20);
     q2p = bf_quot(a.b2, a.db1, cp, a.SB2, d2p);
     q2p2 = bf_quot(a.b2, a.db1, cp2, a.SB2, d2p2);
-    dcm = a.dc1[cm];
-    dc0 = a.dc1[c];
-    dcp = a.dc1[cp];
+    dcm = dv_of(a.dc1[cm]);
+    dc0 = dv_of(a.dc1[c]);
+    dcp = dv_of(a.dc1[cp]);
     dbc0 = a.db1[c];
     dbcp = a.db1[cp];
   }
@@ -132,12 +133,12 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
     const R va0 = a.va[c], va1 = a.va[c - a.SO1], va2 = a.va[c - a.SO2];
     {
       const R v_advect = (va0 + va1) * R(0.5);
-      LimOut<R> L = limiter<R>(v_advect, q1m, q10, q1p, q1p2, dc0, dcm, dcp, dbc0, dbcp, d10, d1p, dt, true);
+      LimOut<R> L = limiter_dv<R>(v_advect, q1m, q10, q1p, q1p2, dc0, dcm, dcp, dbc0, dbcp, d10, d1p, dt, true);
       a.f1[c] = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
     }
     {
       const R v_advect = (va0 + va2) * R(0.5);
-      LimOut<R> L = limiter<R>(v_advect, q2m, q20, q2p, q2p2, dc0, dcm, dcp, dbc0, dbcp, d20, d2p, dt, true);
+      LimOut<R> L = limiter_dv<R>(v_advect, q2m, q20, q2p, q2p2, dc0, dcm, dcp, dbc0, dbcp, d20, d2p, dt, true);
       a.f2[c] = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
     }
     if (!more) break;
@@ -149,12 +150,12 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
       q1p2 = q1p; d1p2 = d1p;
       q2p2 = q2p; d2p2 = d2p;
     } else {
-      d1p2 = (nd + nd1) * R(0.5);
-      q1p2 = nb1 / d1p2;
-      d2p2 = (nd + nd2) * R(0.5);
-      q2p2 = nb2 / d2p2;
+      d1p2 = dv_of((nd + nd1) * R(0.5));
+      q1p2 = dv_div(nb1, d1p2);
+      d2p2 = dv_of((nd + nd2) * R(0.5));
+      q2p2 = dv_div(nb2, d2p2);
     }
-    dcm = dc0; dc0 = dcp; dcp = ndc;
+    dcm = dc0; dc0 = dcp; dcp = dv_of(ndc);
     dbc0 = dbcp; dbcp = ndb;
     c = cn;
   }
@@ -182,7 +183,7 @@ __global__ void __launch_bounds__(128, 10) k_bflux_x(BfArgs<R> a, int sx, int sx
   R d1, d2;
   const R q1 = bf_quot(a.b1, a.db1, c, a.SB1, d1);
   const R q2 = bf_quot(a.b2, a.db1, c, a.SB2, d2);
-  const R dc = a.dc1[c], db = a.db1[c];
+  const R dc = dv_of(a.dc1[c]), db = a.db1[c];
   const unsigned all = 0xffffffffu;
   const R q1m = __shfl_up_sync(all, q1, 1), q1p = __shfl_down_sync(all, q1, 1), q1p2 = __shfl_down_sync(all, q1, 2);
   const R q2m = __shfl_up_sync(all, q2, 1), q2p = __shfl_down_sync(all, q2, 1), q2p2 = __shfl_down_sync(all, q2, 2);
@@ -196,13 +197,13 @@ __global__ void __launch_bounds__(128, 10) k_bflux_x(BfArgs<R> a, int sx, int sx
   const R va0 = a.va[c], va1 = a.va[c - a.SO1], va2 = a.va[c - a.SO2];
   {
     const R v_advect = (va0 + va1) * R(0.5);
-    LimOut<R> L = limiter<R>(v_advect, left ? q1m : q1, q1, q1p, right ? q1p2 : q1p, dc, left ? dcm : dc, dcp, db,
+    LimOut<R> L = limiter_dv<R>(v_advect, left ? q1m : q1, q1, q1p, right ? q1p2 : q1p, dc, left ? dcm : dc, dcp, db,
                              dbp, d1, d1p, dt, true);
     a.f1[c] = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
   }
   {
     const R v_advect = (va0 + va2) * R(0.5);
-    LimOut<R> L = limiter<R>(v_advect, left ? q2m : q2, q2, q2p, right ? q2p2 : q2p, dc, left ? dcm : dc, dcp, db,
+    LimOut<R> L = limiter_dv<R>(v_advect, left ? q2m : q2, q2, q2p, right ? q2p2 : q2p, dc, left ? dcm : dc, dcp, db,
                              dbp, d2, d2p, dt, true);
     a.f2[c] = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
   }
@@ -237,9 +238,9 @@ __global__ void __launch_bounds__(128) k_bflux_march1(BfArgs<R> a) {
     q0 = bf_quot(B, a.db1, c, SB, d0);
     qp = bf_quot(B, a.db1, cp, SB, dp);
     qp2 = bf_quot(B, a.db1, cp2, SB, dp2);
-    dcm = a.dc1[cm];
-    dc0 = a.dc1[c];
-    dcp = a.dc1[cp];
+    dcm = dv_of(a.dc1[cm]);
+    dc0 = dv_of(a.dc1[c]);
+    dcp = dv_of(a.dc1[cp]);
     dbc0 = a.db1[c];
     dbcp = a.db1[cp];
   }
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(128) k_bflux_march1(BfArgs<R> a) {
       ndb = a.db1[cn + SA];
     }
     const R v_advect = (a.va[c] + a.va[c - SO]) * R(0.5);
-    LimOut<R> L = limiter<R>(v_advect, qm, q0, qp, qp2, dc0, dcm, dcp, dbc0, dbcp, d0, dp, dt, true);
+    LimOut<R> L = limiter_dv<R>(v_advect, qm, q0, qp, qp2, dc0, dcm, dcp, dbc0, dbcp, d0, dp, dt, true);
     fo[c] = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
     if (!more) break;
     qm = q0; q0 = qp; qp = qp2;
@@ -269,10 +270,10 @@ __global__ void __launch_bounds__(128) k_bflux_march1(BfArgs<R> a) {
     if (clamp) {
       qp2 = qp; dp2 = dp;
     } else {
-      dp2 = (nd + nds) * R(0.5);
-      qp2 = nb / dp2;
+      dp2 = dv_of((nd + nds) * R(0.5));
+      qp2 = dv_div(nb, dp2);
     }
-    dcm = dc0; dc0 = dcp; dcp = ndc;
+    dcm = dc0; dc0 = dcp; dcp = dv_of(ndc);
     dbc0 = dbcp; dbcp = ndb;
     c = cn;
   }
@@ -381,7 +382,11 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
     // quotients by the metrics: through their reciprocals for the z sweep;
     // the x sweep's form (three x faces live) is faster with plain division
     auto quot = [&](R a, int d) {
+#if LARE_FAST
+      return a * g.rdbm[d](pp[d]);
+#else
       return A == 0 ? a / g.dbm[d](pp[d]) : div_rcp(a, g.dbm[d](pp[d]), g.rdbm[d](pp[d]));
+#endif
     };
     const R term_t1 = quot(g.pass_t1 * dvv[T1], T1);
     const R term_t2 = quot(g.pass_t2 * dvv[T2], T2);
@@ -483,7 +488,7 @@ __global__ void __launch_bounds__(128) k_vert_march(VertArgs<R> g) {
       s = s + pu[q];
       w = w + cu1[q];
     }
-    const R rvc = s / w;
+    const R rvc = qdiv(s, w);
     g.rv[c] = rvc;
     R tp = d[0];
 #pragma unroll
@@ -511,7 +516,7 @@ __global__ void __launch_bounds__(128) k_vert_march(VertArgs<R> g) {
       }
       const R dmm = tm * R(0.125);
       const R dmp = tp * R(0.125);
-      g.rv1[c] = (rvc * cc1 + dmm - dmp) / cc2;
+      g.rv1[c] = qdiv(rvc * cc1 + dmm - dmp, cc2);
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -577,18 +582,30 @@ __device__ __forceinline__ void mom_flux_vals(R area, R va0, R va1, R rvc, R rvp
   const R sign_v = copysign(R(1), v_advect);
   const R vad_p = (sign_v + R(1)) * R(0.5);
   const R vad_m = R(1) - vad_p;
-  const R dxcu = dxcm * vad_p + dxcp * vad_m;
   const R dxbu = dxbi * vad_p + dxbp * vad_m;
-  const R phi = fabs(v_advect) * dt / dxbu;
   const R rhou = rvc * vad_p + rvp * vad_m;
+#if LARE_FAST
+  // product build: the upwind widths by selection (vad_p is 0 or 1) and one
+  // reciprocal per divisor, shared by the three components
+  const R rci = fast_rcp(dxci), rcu = fast_rcp(signbit(v_advect) ? dxcp : dxcm), rbu = fast_rcp(dxbu);
+  const R phi = fabs(v_advect) * dt * rbu;
+  const R dmu = fabs(dmc) * rbu * fast_rcp(area * rhou);
+#else
+  const R dxcu = dxcm * vad_p + dxcp * vad_m;
+  const R phi = fabs(v_advect) * dt / dxbu;
   const R dmu = fabs(dmc) / area / dxbu / rhou;
+#endif
 #pragma unroll
   for (int comp = 0; comp < 3; ++comp) {
     const R fm = w[comp][0], fi = w[comp][1], fp = w[comp][2], fp2 = w[comp][3];
     const R dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
     const R fu = fi * vad_p + fp * vad_m;
     const R dfu = dfm * vad_p + dfp * vad_m;
+#if LARE_FAST
+    R Da = (R(2) - phi) * fabs(dfi) * rci + (R(1) + phi) * fabs(dfu) * rcu;
+#else
     R Da = (R(2) - phi) * fabs(dfi) / dxci + (R(1) + phi) * fabs(dfu) / dxcu;
+#endif
     Da = Da * (R(1) / R(6));
     const R ss = R(0.5) * (copysign(R(1), dfi) + copysign(R(1), dfu));
     const R Di = sign_v * ss * fmin(fmin(fabs(Da) * dxbu, fabs(dfi)), fabs(dfu));
@@ -637,9 +654,9 @@ __device__ __forceinline__ R rke_dk(const R* v, const R* f, const R* dmv, const 
 // K9's update at c from the fluxes at faces c - e_A (Fm) and c (F)
 template <class R>
 __device__ __forceinline__ void mom_update(const MomArgs<R>& g, int c, const R (&Fm)[3], const R (&F)[3]) {
-  const R rvc = g.rv[c], c1 = g.cv1v[c], den = g.cv2v[c] * g.rv1[c];
+  const R rvc = g.rv[c], c1 = g.cv1v[c], den = dv_of(g.cv2v[c] * g.rv1[c]);
 #pragma unroll
-  for (int comp = 0; comp < 3; ++comp) g.vn[comp][c] = (rvc * g.v[comp][c] * c1 + Fm[comp] - F[comp]) / den;
+  for (int comp = 0; comp < 3; ++comp) g.vn[comp][c] = dv_div(rvc * g.v[comp][c] * c1 + Fm[comp] - F[comp], den);
 }
 
 template <class R, bool RKE>
@@ -710,10 +727,10 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 6 : 8) k_mom_march(MomAr
       for (int comp = 0; comp < 3; ++comp) g.fp[comp][c] = fpre[comp];
     }
     // K9's update at c: fluxes at faces c - e_A and c
-    const R c1 = g.cv1v[c], den = g.cv2v[c] * g.rv1[c];
+    const R c1 = g.cv1v[c], den = dv_of(g.cv2v[c] * g.rv1[c]);
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
-      g.vn[comp][c] = (rvc * w[comp][1] * c1 + Fm[comp] - F[comp]) / den;
+      g.vn[comp][c] = dv_div(rvc * w[comp][1] * c1 + Fm[comp] - F[comp], den);
       Fm[comp] = F[comp];
     }
   }
@@ -777,6 +794,204 @@ __global__ void __launch_bounds__(128) k_bupdate(BUpdArgs<R> g) {
     if (r2b) b = b + f2c[p] - f2b[p];
     g.Ba[c] = b;
   }
+}
+
+// K4 + K5 + K6 for the y and z sweeps as one marching kernel.  A thread owns
+// a line along A at one (x, transverse) position of the cell box and walks a
+// chunk of it: at each point it forms the mass flux dm (K4, with the ghost
+// values of dm_[yz]_bcs taken at their source index), the new density from
+// the dm below and here (K5), the energy flux (K5) and the new energy from
+// the energy flux below and here (K6).  The fluxes of the point below are
+// carried in registers, so the energy flux never reaches memory, and the new
+// energy goes to a second buffer (swapped in after the launch) because the
+// limiter of the next chunk still reads the old values.  The same
+// expressions over the same operands as the three point kernels.
+constexpr int kMEChunk = 32;
+
+template <class R>
+struct MEArgs {
+  const R* va;       // velocity component along A (v1)
+  const R* rho;      // old density (rho1)
+  R* rho_new;
+  const R* energy;   // old energy
+  R* energy_new;
+  R* dm;
+  const R* cv1;
+  const R* cv2;
+  const R* db1;
+  const R* dc1;
+  A1<R> dbt1, dbt2;  // widths of the transverse axes
+  const double* sc;
+  int dt_slot;
+  int SA, S1, S2, SY;  // strides along A, T1 (= x), T2, and the thread grid's second axis (= T2)
+  int na, nt1, nt2;
+  bool per;
+};
+
+template <class R>
+__global__ void __launch_bounds__(128) k_mass_energy_march(MEArgs<R> a) {
+  const int x = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 1;  // T1 = x, -1..nt1+2
+  const int t = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 1;  // T2, -1..nt2+2
+  if (x > a.nt1 + 2 || t > a.nt2 + 2) return;
+  const int na = a.na, SA = a.SA, S1 = a.S1, S2 = a.S2;
+  const int ia0 = -1 + (int)blockIdx.z * kMEChunk;
+  const int ia1 = min(ia0 + kMEChunk - 1, na + 2);
+  const bool inside_t = x >= 0 && x <= a.nt1 + 1 && t >= 0 && t <= a.nt2 + 1;  // dm's transverse range
+  const bool line0 = x <= a.nt1 && t <= a.nt2 && x >= 0 && t >= 0;          // the energy flux's
+  const bool line1 = line0 && x >= 1 && t >= 1;                              // the updates'
+  const R dt = (R)a.sc[a.dt_slot];
+  const R area = inside_t ? a.dbt1(x) * a.dbt2(t) : R(0);
+  const R* __restrict__ rho = a.rho;
+  const R* __restrict__ en = a.energy;
+  const R* __restrict__ va = a.va;
+  const R* __restrict__ dc1 = a.dc1;
+  const R* __restrict__ db1 = a.db1;
+  // K4 at ia (cell c), from its source index
+  auto mass_flux = [&](int ia, int c) -> R {
+    if (!inside_t) return R(0);
+    int sa = ia;
+    if (a.per) {
+      if (ia == na + 1) sa = 1;
+      else if (ia == na + 2) sa = 2;
+      else if (ia == -1) sa = na - 1;
+      else if (ia == 0) sa = na;
+    } else {
+      if (ia == na + 1) sa = na;
+      else if (ia == -1) sa = 0;
+      else if (ia == na + 2) return R(0);
+    }
+    const int q = c + (sa - ia) * SA;
+    const int qm = q - SA, qp = q + SA, qp2 = q + 2 * SA;
+    const R v_advect = (va[q] + va[q - S1] + va[q - S2] + va[q - S1 - S2]) * R(0.25);
+    LimOut<R> L = limiter<R>(v_advect, rho[qm], rho[q], rho[qp], rho[qp2], dc1[q], dc1[qm], dc1[qp], db1[q],
+                             db1[qp], R(0), R(0), dt, false);
+    return (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt * area;
+  };
+  // K5's energy flux at ia (cell c), 0 <= ia <= na on line0
+  auto energy_flux = [&](int c, R dmc) -> R {
+    const int cm = c - SA, cp = c + SA, cp2 = c + 2 * SA;
+    const R v_advect = (va[c] + va[c - S1] + va[c - S2] + va[c - S1 - S2]) * R(0.25);
+    LimOut<R> L = limiter<R>(v_advect, en[cm], en[c], en[cp], en[cp2], dc1[c], dc1[cm], dc1[cp], db1[c], db1[cp],
+                             R(0), R(0), dt, false);
+    const R rhou = rho[c] * L.vad_p + rho[cp] * L.vad_m;
+#if LARE_FAST
+    const R dmu = fabs(dmc) * fast_rcp(area * L.dxbu * rhou);
+#else
+    const R dmu = fabs(dmc) / area / L.dxbu / rhou;
+#endif
+    return (L.fu + L.Di * (R(1) - dmu)) * dmc;
+  };
+  int c = x + t * a.SY + ia0 * SA;
+  // the fluxes at ia0 - 1, which the first updates of the chunk read
+  R dm_prev = R(0), ef_prev = R(0);
+  if (ia0 >= 1 && ia0 - 1 <= na) {
+    dm_prev = mass_flux(ia0 - 1, c - SA);
+    if (line0) ef_prev = energy_flux(c - SA, dm_prev);
+  }
+  for (int ia = ia0; ia <= ia1; ++ia, c += SA) {
+    const R dmc = mass_flux(ia, c);
+    a.dm[c] = dmc;
+    const bool in1 = line1 && ia >= 1 && ia <= na;
+    const R r = rho[c];
+    R rn = r;
+    if (in1) rn = qdiv(r * a.cv1[c] + dm_prev - dmc, a.cv2[c]);
+    a.rho_new[c] = rn;
+    R ef = R(0);
+    if (line0 && ia >= 0 && ia <= na) ef = energy_flux(c, dmc);
+    R e = en[c];
+    if (in1) e = qdiv(e * a.cv1[c] * r + ef_prev - ef, a.cv2[c] * rn);
+    a.energy_new[c] = e;
+    dm_prev = dmc;
+    ef_prev = ef;
+  }
+}
+
+// The same for the x sweep: the lanes of a warp hold consecutive x
+// positions and take their stencil neighbours (one to the left, two to the
+// right) and the fluxes of the point to their left by shuffles.  A warp
+// spans 32 positions and writes the kMEXOut = 28 whose stencils and left
+// fluxes lie inside it; ghost values of dm (dm_x_bcs) are formed from their
+// source index by direct loads.
+constexpr int kMEXOut = 28;
+
+template <class R>
+__global__ void __launch_bounds__(128) k_mass_energy_x(MEArgs<R> a, int sx, int sxy, int nx) {
+  const int lane = (int)threadIdx.x;                               // blockDim.x == 32: one warp per row
+  const int ix = -3 + (int)blockIdx.x * kMEXOut + lane;            // lane 2 holds the first output
+  const int iy = -1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int iz = -1 + (int)blockIdx.z;
+  if (iy > a.nt1 + 2) return;                                      // uniform over the warp
+  const int S1 = a.S1, S2 = a.S2;
+  const int xl = min(max(ix, -2), nx + 2);                         // in-box load position
+  const int c = xl + sx * iy + sxy * iz;
+  const bool inside_t = iy >= 0 && iy <= a.nt1 + 1 && iz >= 0 && iz <= a.nt2 + 1;
+  const bool line0 = iy >= 0 && iy <= a.nt1 && iz >= 0 && iz <= a.nt2;
+  const bool line1 = line0 && iy >= 1 && iz >= 1;
+  const R dt = (R)a.sc[a.dt_slot];
+  const R area = inside_t ? a.dbt1(iy) * a.dbt2(iz) : R(0);
+  const R* __restrict__ rho = a.rho;
+  const R* __restrict__ en = a.energy;
+  const R* __restrict__ va = a.va;
+  const R* __restrict__ dc1 = a.dc1;
+  const R* __restrict__ db1 = a.db1;
+  const R r0 = rho[c], e0 = en[c], dc = dc1[c], db = db1[c];
+  const unsigned all = 0xffffffffu;
+  const R rm = __shfl_up_sync(all, r0, 1), rp = __shfl_down_sync(all, r0, 1), rp2 = __shfl_down_sync(all, r0, 2);
+  const R em = __shfl_up_sync(all, e0, 1), ep = __shfl_down_sync(all, e0, 1), ep2 = __shfl_down_sync(all, e0, 2);
+  const R dcm = __shfl_up_sync(all, dc, 1), dcp = __shfl_down_sync(all, dc, 1);
+  const R dbp = __shfl_down_sync(all, db, 1);
+  const R v_c = (va[c] + va[c - S1] + va[c - S2] + va[c - S1 - S2]) * R(0.25);
+  const int na = a.na;
+  // K4 at ix: from the lane neighbours, or from the source index for a ghost
+  R dmc = R(0);
+  if (inside_t && lane >= 1 && lane <= 29) {
+    int sa = ix;
+    bool compute = true;
+    if (a.per) {
+      if (ix == na + 1) sa = 1;
+      else if (ix == na + 2) sa = 2;
+      else if (ix == -1) sa = na - 1;
+      else if (ix == 0) sa = na;
+    } else {
+      if (ix == na + 1) sa = na;
+      else if (ix == -1) sa = 0;
+      else if (ix == na + 2) compute = false;
+    }
+    if (compute && ix >= -1 && ix <= na + 2) {
+      if (sa == ix) {
+        LimOut<R> L = limiter<R>(v_c, rm, r0, rp, rp2, dc, dcm, dcp, db, dbp, R(0), R(0), dt, false);
+        dmc = (L.fu + L.Di * (R(1) - L.phi)) * v_c * dt * area;
+      } else {
+        const int q = c + (sa - ix), qm = q - 1, qp = q + 1, qp2 = q + 2;
+        const R v_advect = (va[q] + va[q - S1] + va[q - S2] + va[q - S1 - S2]) * R(0.25);
+        LimOut<R> L = limiter<R>(v_advect, rho[qm], rho[q], rho[qp], rho[qp2], dc1[q], dc1[qm], dc1[qp], db1[q],
+                                 db1[qp], R(0), R(0), dt, false);
+        dmc = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt * area;
+      }
+    }
+  }
+  // K5's energy flux at ix (0 <= ix <= na on line0)
+  R ef = R(0);
+  if (line0 && ix >= 0 && ix <= na && lane >= 1 && lane <= 29) {
+    LimOut<R> L = limiter<R>(v_c, em, e0, ep, ep2, dc, dcm, dcp, db, dbp, R(0), R(0), dt, false);
+    const R rhou = r0 * L.vad_p + rp * L.vad_m;
+#if LARE_FAST
+    const R dmu = fabs(dmc) * fast_rcp(area * L.dxbu * rhou);
+#else
+    const R dmu = fabs(dmc) / area / L.dxbu / rhou;
+#endif
+    ef = (L.fu + L.Di * (R(1) - dmu)) * dmc;
+  }
+  const R dm_prev = __shfl_up_sync(all, dmc, 1), ef_prev = __shfl_up_sync(all, ef, 1);
+  if (lane < 2 || lane > 29 || ix > na + 2) return;
+  a.dm[c] = dmc;
+  const bool in1 = line1 && ix >= 1 && ix <= na;
+  R rn = r0;
+  if (in1) rn = qdiv(r0 * a.cv1[c] + dm_prev - dmc, a.cv2[c]);
+  a.rho_new[c] = rn;
+  R e = e0;
+  if (in1) e = qdiv(e0 * a.cv1[c] * r0 + ef_prev - ef, a.cv2[c] * rn);
+  a.energy_new[c] = e;
 }
 
 template <int A, class R>
@@ -965,64 +1180,48 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   const bool per = run.p.per[A];
   const int nt1 = nn[T1], nt2 = nn[T2];
 
-  // ---- K4: mass flux with dm_[xyz]_bcs over the whole cell box
-  LARE_BOXWH(run, 0, 2, 5, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
-    const int c = ix + sx * iy + sxy * iz;
-    const int pp[3] = {ix, iy, iz};
-    const int ia = pp[A], i1 = pp[T1], i2 = pp[T2];
-    R out = R(0);
-    bool inside_t = i1 >= 0 && i1 <= nt1 + 1 && i2 >= 0 && i2 <= nt2 + 1;
-    int sa = ia;  // source index along A
-    bool compute = inside_t;
-    if (per) {
-      if (ia == na + 1) sa = 1;
-      else if (ia == na + 2) sa = 2;
-      else if (ia == -1) sa = na - 1;
-      else if (ia == 0) sa = na;
+  {
+    // ---- K4 + K5 + K6 in one kernel (marching along A for the y and z
+    // sweeps, warp shuffles along x for the x sweep); the new energy is
+    // swapped in
+    MEArgs<R> me;
+    me.va = va;
+    me.rho = rho;
+    me.rho_new = rho_new;
+    me.energy = energy;
+    me.energy_new = eflux;  // the energy-flux array is free in this form
+    me.dm = dm;
+    me.cv1 = cv1;
+    me.cv2 = cv2;
+    me.db1 = db1;
+    me.dc1 = dc1;
+    me.dbt1 = dbt1;
+    me.dbt2 = dbt2;
+    me.sc = sc;
+    me.dt_slot = dt_slot;
+    me.SA = SA;
+    me.S1 = S1;
+    me.S2 = S2;
+    me.SY = S2;
+    me.na = na;
+    me.nt1 = nt1;
+    me.nt2 = nt2;
+    me.per = per;
+    dim3 blk(32, 4, 1);
+    // words: rho, energy, va, dc1, db1, cv1, cv2 read; dm, rho_new, energy written
+    const int k = run.prof_begin(A == 0 ? "remap_sweep_mass_energy_x" : "remap_sweep_mass_energy_march", 0, 10,
+                                 (double)(nx + 4) * (ny + 4) * (nz + 4));
+    if (A == 0) {
+      dim3 grd((nx + 4 + kMEXOut - 1) / kMEXOut, (ny + 4 + 3) / 4, nz + 4);
+      k_mass_energy_x<R><<<grd, blk, 0, run.s>>>(me, sx, sxy, nx);
     } else {
-      if (ia == na + 1) sa = na;
-      else if (ia == -1) sa = 0;
-      else if (ia == na + 2) compute = false;
+      dim3 grd((nt1 + 4 + 31) / 32, (nt2 + 4 + 3) / 4, (na + 4 + kMEChunk - 1) / kMEChunk);
+      k_mass_energy_march<R><<<grd, blk, 0, run.s>>>(me);
     }
-    if (compute) {
-      const R dt = (R)sc[dt_slot];
-      const int q = c + (sa - ia) * SA;
-      const int qm = q - SA, qp = q + SA, qp2 = q + 2 * SA;
-      R area = dbt1(i1) * dbt2(i2);
-      R v_advect = (va[q] + va[q - S1] + va[q - S2] + va[q - S1 - S2]) * R(0.25);
-      LimOut<R> L = limiter<R>(v_advect, rho[qm], rho[q], rho[qp], rho[qp2], dc1[q], dc1[qm], dc1[qp], db1[q],
-                               db1[qp], R(0), R(0), dt, false);
-      out = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt * area;
-    }
-    dm[c] = out;
-  });
-
-  // ---- K5: new rho (second buffer) and the energy flux (0:n)
-  LARE_BOXWH(run, 6, 4, 10, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
-    const int c = ix + sx * iy + sxy * iz;
-    const bool in0 = ix >= 0 && ix <= nx && iy >= 0 && iy <= ny && iz >= 0 && iz <= nz;
-    const bool in1 = ix >= 1 && iy >= 1 && iz >= 1 && in0;
-    if (in1) rho_new[c] = (rho[c] * cv1[c] + dm[c - SA] - dm[c]) / cv2[c];
-    else rho_new[c] = rho[c];
-    if (in0) {
-      const R dt = (R)sc[dt_slot];
-      const int pp[3] = {ix, iy, iz};
-      const int cm = c - SA, cp = c + SA, cp2 = c + 2 * SA;
-      R area = dbt1(pp[T1]) * dbt2(pp[T2]);
-      R v_advect = (va[c] + va[c - S1] + va[c - S2] + va[c - S1 - S2]) * R(0.25);
-      LimOut<R> L = limiter<R>(v_advect, energy[cm], energy[c], energy[cp], energy[cp2], dc1[c], dc1[cm], dc1[cp],
-                               db1[c], db1[cp], R(0), R(0), dt, false);
-      R rhou = rho[c] * L.vad_p + rho[cp] * L.vad_m;
-      R dmu = fabs(dm[c]) / area / L.dxbu / rhou;
-      eflux[c] = (L.fu + L.Di * (R(1) - dmu)) * dm[c];
-    }
-  });
-
-  // ---- K6: energy update (1:n)
-  LARE_BOXWH(run, 0, 2, 7, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) {
-    const int c = ix + sx * iy + sxy * iz;
-    energy[c] = (energy[c] * cv1[c] * rho[c] + eflux[c - SA] - eflux[c]) / (cv2[c] * rho_new[c]);
-  });
+    run.prof_end(k);
+    ++run.launches;
+    std::swap(Ar.energy.p, Ar.flux.p);
+  }
 
   // ---- K7: vertex quantities.  rho_v over a -1:n+1, the rest over 0:n;
   // dm vertex averages over a -1:n.

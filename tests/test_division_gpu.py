@@ -65,3 +65,26 @@ def test_quotients_at_the_edges():
     # significands of all ones (the reciprocal sits next to a power of two)
     m = np.nextafter(2.0, 0.0)
     _check(_random(rng, n, -40, 40), np.ldexp(np.full(n, m), rng.integers(-40, 40, n)))
+
+
+def test_product_engine_reciprocal():
+    """The FP64 product engine divides through lare::fast_rcp (hardware
+    approximation plus Newton-Raphson steps): within one ulp of 1/b over the
+    range it serves."""
+    import torch
+    from lare3d_b200 import gpu
+    f = gpu.library().lare_gpu_check_reciprocal
+    f.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    rng = np.random.default_rng(13)
+    n = 1 << 22
+    b = _random(rng, n, -1000, 1000)
+    b[:4] = [1.0, np.nextafter(2.0, 0.0), 2.0 ** -1000, 2.0 ** 1000]
+    db = torch.from_numpy(b).cuda()
+    out = torch.empty_like(db)
+    assert f(db.data_ptr(), n, out.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    want = 1.0 / b
+    ulps = np.abs(got - want) / np.spacing(np.abs(want))
+    assert ulps.max() <= 1.0, f"max {ulps.max():.2f} ulp"
