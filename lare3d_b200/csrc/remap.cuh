@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
   }
   (void)d1m;
   (void)d2m;
+  R va0 = a.va[c], va1 = a.va[c - a.SO1], va2 = a.va[c - a.SO2];
   for (int ia = ia0; ia <= ia1; ++ia) {
     // issue the next step's loads before this step's arithmetic
     const int cn = c + SA;
@@ -119,6 +120,7 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
     const int qn = cn + 2 * SA;
     const bool fetch = more && !clamp;
     R nb1 = R(0), nb2 = R(0), nd = R(0), nd1 = R(0), nd2 = R(0), ndc = R(0), ndb = R(0);
+    R nva0 = R(0), nva1 = R(0), nva2 = R(0);
     if (fetch) {
       nb1 = a.b1[qn];
       nb2 = a.b2[qn];
@@ -130,7 +132,11 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
       ndc = a.dc1[cn + SA];
       ndb = a.db1[cn + SA];
     }
-    const R va0 = a.va[c], va1 = a.va[c - a.SO1], va2 = a.va[c - a.SO2];
+    if (more) {
+      nva0 = a.va[cn];
+      nva1 = a.va[cn - a.SO1];
+      nva2 = a.va[cn - a.SO2];
+    }
     {
       const R v_advect = (va0 + va1) * R(0.5);
       LimOut<R> L = limiter_dv<R>(v_advect, q1m, q10, q1p, q1p2, dc0, dcm, dcp, dbc0, dbcp, d10, d1p, dt, true);
@@ -157,6 +163,7 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
     }
     dcm = dc0; dc0 = dcp; dcp = dv_of(ndc);
     dbc0 = dbcp; dbcp = ndb;
+    va0 = nva0; va1 = nva1; va2 = nva2;
     c = cn;
   }
 }
@@ -245,13 +252,14 @@ __global__ void __launch_bounds__(128) k_bflux_march1(BfArgs<R> a) {
     dbcp = a.db1[cp];
   }
   (void)dm;
+  R va = a.va[c], vo = a.va[c - SO];
   for (int ia = ia0; ia <= ia1; ++ia) {
     const int cn = c + SA;
     const bool more = ia < ia1;
     const bool clamp = ia + 3 > a.na + 2;
     const int qn = cn + 2 * SA;
     const bool fetch = more && !clamp;
-    R nb = R(0), nd = R(0), nds = R(0), ndc = R(0), ndb = R(0);
+    R nb = R(0), nd = R(0), nds = R(0), ndc = R(0), ndb = R(0), nva = R(0), nvo = R(0);
     if (fetch) {
       nb = B[qn];
       nd = a.db1[qn];
@@ -261,7 +269,11 @@ __global__ void __launch_bounds__(128) k_bflux_march1(BfArgs<R> a) {
       ndc = a.dc1[cn + SA];
       ndb = a.db1[cn + SA];
     }
-    const R v_advect = (a.va[c] + a.va[c - SO]) * R(0.5);
+    if (more) {
+      nva = a.va[cn];
+      nvo = a.va[cn - SO];
+    }
+    const R v_advect = (va + vo) * R(0.5);
     LimOut<R> L = limiter_dv<R>(v_advect, qm, q0, qp, qp2, dc0, dcm, dcp, dbc0, dbcp, d0, dp, dt, true);
     fo[c] = (L.fu + L.Di * (R(1) - L.phi)) * v_advect * dt;
     if (!more) break;
@@ -275,6 +287,7 @@ __global__ void __launch_bounds__(128) k_bflux_march1(BfArgs<R> a) {
     }
     dcm = dc0; dc0 = dcp; dcp = dv_of(ndc);
     dbc0 = dbcp; dbcp = ndb;
+    va = nva; vo = nvo;
     c = cn;
   }
 }
@@ -285,7 +298,7 @@ __global__ void __launch_bounds__(128) k_bflux_march1(BfArgs<R> a) {
 // carried from the previous step instead of reloaded, and the z face below a
 // cell is the previous step's z face above it: 12 to 15 loads per cell
 // instead of 28, the same expressions, the same results bit for bit.
-constexpr int kGeomZ = 64;
+constexpr int kGeomZ = 16;
 
 template <class R>
 struct GeomArgs {
@@ -677,7 +690,7 @@ __global__ void __launch_bounds__(128) k_mom_x(MomArgs<R> g) {
 }
 
 template <class R, bool RKE>
-__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 6 : 8) k_mom_march(MomArgs<R> g) {
+__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 4 : 8) k_mom_march(MomArgs<R> g) {
   const int t0 = (int)(blockIdx.x * blockDim.x + threadIdx.x);  // x, 0..nx
   const int t1 = (int)(blockIdx.y * blockDim.y + threadIdx.y);  // the third axis, 0..n3
   if (t0 > g.nx || t1 > g.n3) return;
@@ -702,32 +715,55 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 6 : 8) k_mom_march(MomAr
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) g.fp[comp][c] = fpre[comp];
   }
+  // the loads of face c + SA are issued one step ahead (a face's own values
+  // and the new far points of the windows), so each step's arithmetic waits
+  // on loads issued a step earlier
+  struct Next {
+    R w[3], va, rv, db, dc, dm, c1, c2, r1;
+  };
+  auto fetch = [&](int q) {
+    Next n;
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) n.w[comp] = g.v[comp][q + 2 * SA];
+    n.va = g.va[q + SA];
+    n.rv = g.rv[q + SA];
+    n.db = g.db1[q + 2 * SA];
+    n.dc = g.dc1[q + SA];
+    n.dm = g.dmv[q];
+    n.c1 = g.cv1v[q];
+    n.c2 = g.cv2v[q];
+    n.r1 = g.rv1[q];
+    return n;
+  };
+  Next nx = fetch(c + SA);
   for (int ia = ia0; ia <= ia1; ++ia) {
     c += SA;
+    const Next cur = nx;
+    if (ia < ia1) nx = fetch(c + SA);
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
       w[comp][0] = w[comp][1];
       w[comp][1] = w[comp][2];
       w[comp][2] = w[comp][3];
-      w[comp][3] = g.v[comp][c + 2 * SA];
+      w[comp][3] = cur.w[comp];
     }
     va0 = va1;
-    va1 = g.va[c + SA];
+    va1 = cur.va;
     rvc = rvn;
-    rvn = g.rv[c + SA];
+    rvn = cur.rv;
     dbw0 = dbw1;
     dbw1 = dbw2;
-    dbw2 = g.db1[c + 2 * SA];
+    dbw2 = cur.db;
     dcw0 = dcw1;
-    dcw1 = g.dc1[c + SA];
+    dcw1 = cur.dc;
     R F[3];
-    mom_flux_vals<R, RKE>(area, va0, va1, rvc, rvn, g.dmv[c], dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, F, fpre);
+    mom_flux_vals<R, RKE>(area, va0, va1, rvc, rvn, cur.dm, dbw0, dbw1, dbw2, dcw0, dcw1, w, dt, F, fpre);
     if constexpr (RKE) {
 #pragma unroll
       for (int comp = 0; comp < 3; ++comp) g.fp[comp][c] = fpre[comp];
     }
     // K9's update at c: fluxes at faces c - e_A and c
-    const R c1 = g.cv1v[c], den = dv_of(g.cv2v[c] * g.rv1[c]);
+    const R c1 = cur.c1, den = dv_of(cur.c2 * cur.r1);
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
       g.vn[comp][c] = dv_div(rvc * w[comp][1] * c1 + Fm[comp] - F[comp], den);
@@ -806,7 +842,7 @@ __global__ void __launch_bounds__(128) k_bupdate(BUpdArgs<R> g) {
 // energy goes to a second buffer (swapped in after the launch) because the
 // limiter of the next chunk still reads the old values.  The same
 // expressions over the same operands as the three point kernels.
-constexpr int kMEChunk = 32;
+constexpr int kMEChunk = 16;
 
 template <class R>
 struct MEArgs {
@@ -881,28 +917,85 @@ __global__ void __launch_bounds__(128) k_mass_energy_march(MEArgs<R> a) {
 #endif
     return (L.fu + L.Di * (R(1) - dmu)) * dmc;
   };
-  int c = x + t * a.SY + ia0 * SA;
+  const int base = x + t * a.SY;
+  // loads along the line, clamped to the cell box (a clamped value is never
+  // used: the windows reach past n + 2 only at points whose dm is a ghost
+  // value and whose energy flux is not formed)
+  auto at = [&](int ia) { return base + min(ia, na + 2) * SA; };
+  auto vface = [&](int q) { return (va[q] + va[q - S1] + va[q - S2] + va[q - S1 - S2]) * R(0.25); };
   // the fluxes at ia0 - 1, which the first updates of the chunk read
   R dm_prev = R(0), ef_prev = R(0);
   if (ia0 >= 1 && ia0 - 1 <= na) {
-    dm_prev = mass_flux(ia0 - 1, c - SA);
-    if (line0) ef_prev = energy_flux(c - SA, dm_prev);
+    dm_prev = mass_flux(ia0 - 1, at(ia0 - 1));
+    if (line0) ef_prev = energy_flux(at(ia0 - 1), dm_prev);
   }
-  for (int ia = ia0; ia <= ia1; ++ia, c += SA) {
-    const R dmc = mass_flux(ia, c);
+  // register windows of step ia: rho and energy at ia-1..ia+2, dc1 at
+  // ia-1..ia+1, db1 at ia..ia+1, and the point's face velocity, cv1, cv2
+  R r[4], e[4], dcw[3], dbw[2];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    r[k] = rho[at(ia0 - 1 + k)];
+    e[k] = en[at(ia0 - 1 + k)];
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) dcw[k] = dc1[at(ia0 - 1 + k)];
+  dbw[0] = db1[at(ia0)];
+  dbw[1] = db1[at(ia0 + 1)];
+  R vf = vface(at(ia0)), c1 = a.cv1[at(ia0)], c2 = a.cv2[at(ia0)];
+  for (int ia = ia0; ia <= ia1; ++ia) {
+    const int c = at(ia);
+    // the next step's new points, a step ahead
+    const bool more = ia < ia1;
+    R nr = R(0), ne = R(0), ndc = R(0), ndb = R(0), nvf = R(0), nc1 = R(0), nc2 = R(0);
+    if (more) {
+      nr = rho[at(ia + 3)];
+      ne = en[at(ia + 3)];
+      ndc = dc1[at(ia + 2)];
+      ndb = db1[at(ia + 2)];
+      const int cn = at(ia + 1);
+      nvf = vface(cn);
+      nc1 = a.cv1[cn];
+      nc2 = a.cv2[cn];
+    }
+    // K4 at ia: from the windows, or from the source index for a ghost value
+    R dmc = R(0);
+    if (inside_t) {
+      const bool ghost = a.per ? (ia <= 0 || ia >= na + 1) : (ia == -1 || ia >= na + 1);
+      if (!ghost) {
+        LimOut<R> L = limiter<R>(vf, r[0], r[1], r[2], r[3], dcw[1], dcw[0], dcw[2], dbw[0], dbw[1], R(0), R(0),
+                                 dt, false);
+        dmc = (L.fu + L.Di * (R(1) - L.phi)) * vf * dt * area;
+      } else {
+        dmc = mass_flux(ia, c);
+      }
+    }
     a.dm[c] = dmc;
     const bool in1 = line1 && ia >= 1 && ia <= na;
-    const R r = rho[c];
-    R rn = r;
-    if (in1) rn = qdiv(r * a.cv1[c] + dm_prev - dmc, a.cv2[c]);
+    R rn = r[1];
+    if (in1) rn = qdiv(r[1] * c1 + dm_prev - dmc, c2);
     a.rho_new[c] = rn;
     R ef = R(0);
-    if (line0 && ia >= 0 && ia <= na) ef = energy_flux(c, dmc);
-    R e = en[c];
-    if (in1) e = qdiv(e * a.cv1[c] * r + ef_prev - ef, a.cv2[c] * rn);
-    a.energy_new[c] = e;
+    if (line0 && ia >= 0 && ia <= na) {
+      LimOut<R> L = limiter<R>(vf, e[0], e[1], e[2], e[3], dcw[1], dcw[0], dcw[2], dbw[0], dbw[1], R(0), R(0), dt,
+                               false);
+      const R rhou = r[1] * L.vad_p + r[2] * L.vad_m;
+#if LARE_FAST
+      const R dmu = fabs(dmc) * fast_rcp(area * L.dxbu * rhou);
+#else
+      const R dmu = fabs(dmc) / area / L.dxbu / rhou;
+#endif
+      ef = (L.fu + L.Di * (R(1) - dmu)) * dmc;
+    }
+    R eo = e[1];
+    if (in1) eo = qdiv(e[1] * c1 * r[1] + ef_prev - ef, c2 * rn);
+    a.energy_new[c] = eo;
     dm_prev = dmc;
     ef_prev = ef;
+    r[0] = r[1]; r[1] = r[2]; r[2] = r[3]; r[3] = nr;
+    e[0] = e[1]; e[1] = e[2]; e[2] = e[3]; e[3] = ne;
+    dcw[0] = dcw[1]; dcw[1] = dcw[2]; dcw[2] = ndc;
+    dbw[0] = dbw[1]; dbw[1] = ndb;
+    vf = nvf; c1 = nc1; c2 = nc2;
   }
 }
 
@@ -1030,9 +1123,10 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   const bool write_cv2 = !predictor;
 
   // ---- K1: cv1, cv2, db1, dc1 over the whole cell box -1..n+2 (z-marching for the
-  // z sweep and the FP64 x sweep; per cell for the y sweep and the FP32 x sweep,
-  // where the marching form measured slower)
-  if (A == 2 || (A == 0 && sizeof(R) == 8)) {
+  // z sweep and, in the exact FP64 build, the x sweep; per cell for the y
+  // sweep, the FP32 x sweep and the product FP64 x sweep, where the marching
+  // form measured slower)
+  if (A == 2 || (A == 0 && sizeof(R) == 8 && !LARE_FAST)) {
     GeomArgs<R> ga;
     ga.vx1 = vx1;
     ga.vy1 = Ar.vy1.p;
@@ -1065,7 +1159,7 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     run.prof_end(k);
     ++run.launches;
   } else {
-    LARE_BOXW(run, 8, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
+    LARE_BOXWH(run, 0, 2, 8, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz) {
       const R dt = (R)sc[dt_slot];
       const int c = ix + sx * iy + sxy * iz;
       // v at the two faces normal to each axis (xremap.f90:64-86)
