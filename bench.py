@@ -487,7 +487,10 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": traffic, "kernel": top["site"], "share": top["ms"] / total_ms,
                 "peak_kind": peak_kind, "algorithmic_bytes_per_launch": per_launch_bytes,
-                "step_achieved": step_gbs, "step_frac": step_gbs / hbm}
+                "step_achieved": step_gbs, "step_frac": step_gbs / hbm,
+                # algorithmic bytes of the whole step per cell (16 words = 128 B is the
+                # irreducible read and write of the eight state fields)
+                "step_bytes_per_cell": step_bytes / n ** 3, "step_words_per_cell": step_bytes / n ** 3 / 8}
 
     # ---- end to end through the C ABI with pinned host buffers
     host = {}

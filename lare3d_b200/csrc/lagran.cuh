@@ -103,20 +103,22 @@ __global__ void __launch_bounds__(128) k_eta_march(EtaArgs<R> g) {
   const int z1 = min(z0 + kEtaZ - 1, g.nz + 1);
   const int sx = g.sx, sxy = g.sxy;
   const R dxc = g.dxc(ix), dyc = g.dyc(iy);
+  const R vxc = dv_of(dxc), vyc = dv_of(dyc);  // divisors in the variant's form
   int c = ix + sx * iy + sxy * z0;
   // plane z0 values of bx (c, c+Y) and by (c, c+X), and the jz1 quotients
   R bx0 = bx_r[c], bxy = bx_r[c + sx], by0 = by_r[c], byx = by_r[c + 1];
-  R qa = (byx - by0) / dxc, qb = (bxy - bx0) / dyc;
+  R qa = dv_div(byx - by0, vxc), qb = dv_div(bxy - bx0, vyc);
   const bool inxy = ix >= 0 && ix <= g.nx && iy >= 0 && iy <= g.ny;
   for (int iz = z0; iz <= z1; ++iz, c += sxy) {
     const R dzc = g.dzc(iz);
+    const R vzc = dv_of(dzc);
     const R bz0 = bz_r[c], bzx = bz_r[c + 1], bzy = bz_r[c + sx], bzxy = bz_r[c + 1 + sx];
     const R bxz = bx_r[c + sxy], bxyz = bx_r[c + sx + sxy], byz = by_r[c + sxy], byxz = by_r[c + 1 + sxy];
-    const R jx1 = (bzy - bz0) / dyc - (byz - by0) / dzc;
-    const R jx2 = (bzxy - bzx) / dyc - (byxz - byx) / dzc;
-    const R jy1 = (bxz - bx0) / dzc - (bzx - bz0) / dxc;
-    const R jy2 = (bxyz - bxy) / dzc - (bzxy - bzy) / dxc;
-    const R qa2 = (byxz - byz) / dxc, qb2 = (bxyz - bxz) / dyc;
+    const R jx1 = dv_div(bzy - bz0, vyc) - dv_div(byz - by0, vzc);
+    const R jx2 = dv_div(bzxy - bzx, vyc) - dv_div(byxz - byx, vzc);
+    const R jy1 = dv_div(bxz - bx0, vzc) - dv_div(bzx - bz0, vxc);
+    const R jy2 = dv_div(bxyz - bxy, vzc) - dv_div(bzxy - bzy, vxc);
+    const R qa2 = dv_div(byxz - byz, vxc), qb2 = dv_div(bxyz - bxz, vyc);
     const R jz1 = qa - qb;
     const R jz2 = qa2 - qb2;
     const R jx = (jx1 + jx2) * R(0.5);
@@ -133,9 +135,10 @@ __global__ void __launch_bounds__(128) k_eta_march(EtaArgs<R> g) {
         const R magn_b = bxv * bxv + byv * byv + bzv * bzv;
         R jpx = R(0), jpy = R(0), jpz = R(0);
         if (magn_b > Num<R>::tiny()) {
-          jpx = (jx * bxv + jy * byv + jz * bzv) * bxv / magn_b;
-          jpy = (jx * bxv + jy * byv + jz * bzv) * byv / magn_b;
-          jpz = (jx * bxv + jy * byv + jz * bzv) * bzv / magn_b;
+          const R vmb = dv_of(magn_b);
+          jpx = dv_div((jx * bxv + jy * byv + jz * bzv) * bxv, vmb);
+          jpy = dv_div((jx * bxv + jy * byv + jz * bzv) * byv, vmb);
+          jpz = dv_div((jx * bxv + jy * byv + jz * bzv) * bzv, vmb);
         }
         const R jqx = jx - jpx, jqy = jy - jpy, jqz = jz - jpz;
         const R mpar = sqrt(jpx * jpx + jpy * jpy + jpz * jpz);
@@ -244,18 +247,21 @@ void resistive_update(Run<R>& run) {
     const int c = ix + sx * iy + sxy * iz;
     if (iy >= 1 && iz >= 1) {
       R area = dyb(iy) * dzb(iz);
-      bxn[c] = bxo[c] + (kz[c] - kz[c - sx] + kz[c - sxy] - kz[c - sx - sxy] - ky[c] + ky[c - sxy] - ky[c - sx] +
-                         ky[c - sx - sxy]) * dt / area;
+      bxn[c] = bxo[c] + qdiv((kz[c] - kz[c - sx] + kz[c - sxy] - kz[c - sx - sxy] - ky[c] + ky[c - sxy] - ky[c - sx] +
+                              ky[c - sx - sxy]) * dt,
+                             area);
     }
     if (ix >= 1 && iz >= 1) {
       R area = dxb(ix) * dzb(iz);
-      byn[c] = byo[c] + (kx[c] - kx[c - sxy] + kx[c - 1] - kx[c - 1 - sxy] - kz[c] + kz[c - 1] - kz[c - sxy] +
-                         kz[c - 1 - sxy]) * dt / area;
+      byn[c] = byo[c] + qdiv((kx[c] - kx[c - sxy] + kx[c - 1] - kx[c - 1 - sxy] - kz[c] + kz[c - 1] - kz[c - sxy] +
+                              kz[c - 1 - sxy]) * dt,
+                             area);
     }
     if (ix >= 1 && iy >= 1) {
       R area = dxb(ix) * dyb(iy);
-      bzn[c] = bzo[c] + (ky[c] - ky[c - 1] + ky[c - sx] - ky[c - 1 - sx] - kx[c] + kx[c - sx] - kx[c - 1] +
-                         kx[c - 1 - sx]) * dt / area;
+      bzn[c] = bzo[c] + qdiv((ky[c] - ky[c - 1] + ky[c - sx] - ky[c - 1 - sx] - kx[c] + kx[c - sx] - kx[c - 1] +
+                              kx[c - 1 - sx]) * dt,
+                             area);
     }
   });
   std::swap(A.bx.p, A.bx1.p);
