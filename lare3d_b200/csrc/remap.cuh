@@ -367,20 +367,51 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
   R vz_prev = vzf(c);          // z face of plane z0 - 1
   c += sxy;
   R vz_cur = vzf(c);           // z face of plane z0
-  for (int iz = z0; iz <= z1; ++iz, c += sxy) {
-    R vxfc[NX], vyfc[NY];
+  // the loads of each plane are issued one plane ahead: x and y face pairs,
+  // the next z face (its four corners) and cv
+  struct Plane {
+    R xa[NX], xb[NX], ya[NY], yb[NY], z[4], cv;
+  };
+  auto fetch = [&](int q, int iz) {
+    Plane P;
 #pragma unroll
     for (int k = 0; k < NX; ++k) {
       const bool ok = k < 2 || ahead;
-      const R a = ok ? vx1[c + xo(k)] : R(0), b = ok ? vx1[c + xo(k) - sx] : R(0);
+      P.xa[k] = ok ? vx1[q + xo(k)] : R(0);
+      P.xb[k] = ok ? vx1[q + xo(k) - sx] : R(0);
+    }
+#pragma unroll
+    for (int k = 0; k < NY; ++k) {
+      const bool ok = k < 2 || ahead;
+      P.ya[k] = ok ? vy1[q + yo(k)] : R(0);
+      P.yb[k] = ok ? vy1[q + yo(k) - 1] : R(0);
+    }
+    // the z face above this plane: read by the z sweep (vz_next) and, for
+    // the other sweeps, carried as the next plane's current z face
+    const bool zok = A == 2 ? iz < g.nz + 2 : iz < z1;
+    const int qz = q + sxy;
+    P.z[0] = zok ? vz1[qz] : R(0);
+    P.z[1] = zok ? vz1[qz - 1] : R(0);
+    P.z[2] = zok ? vz1[qz - sx] : R(0);
+    P.z[3] = zok ? vz1[qz - 1 - sx] : R(0);
+    P.cv = cv_r[q];
+    return P;
+  };
+  Plane nxt = fetch(c, z0);
+  for (int iz = z0; iz <= z1; ++iz, c += sxy) {
+    const Plane cur = nxt;
+    if (iz < z1) nxt = fetch(c + sxy, iz + 1);
+    R vxfc[NX], vyfc[NY];
+#pragma unroll
+    for (int k = 0; k < NX; ++k) {
+      const R a = cur.xa[k], b = cur.xb[k];
       vxfc[k] = (a + b + xa[k] + xb[k]) * q4;
       xa[k] = a;
       xb[k] = b;
     }
 #pragma unroll
     for (int k = 0; k < NY; ++k) {
-      const bool ok = k < 2 || ahead;
-      const R a = ok ? vy1[c + yo(k)] : R(0), b = ok ? vy1[c + yo(k) - 1] : R(0);
+      const R a = cur.ya[k], b = cur.yb[k];
       vyfc[k] = (a + b + ya[k] + yb[k]) * q4;
       ya[k] = a;
       yb[k] = b;
@@ -388,8 +419,9 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
     const R vxb = vxfc[1], vxbm = vxfc[0];
     const R vyb = vyfc[1], vybm = vyfc[0];
     const R vzb = vz_cur, vzbm = vz_prev;
+    const R vz_above = (cur.z[0] + cur.z[1] + cur.z[2] + cur.z[3]) * q4;
     R vz_next = R(0);
-    if (A == 2 && iz < g.nz + 2) vz_next = vzf(c + sxy);
+    if (A == 2 && iz < g.nz + 2) vz_next = vz_above;
     const R dvv[3] = {vxb - vxbm, vyb - vybm, vzb - vzbm};
     const int pp[3] = {ix, iy, iz};
     // quotients by the metrics: through their reciprocals for the z sweep;
@@ -405,7 +437,7 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
     const R term_t2 = quot(g.pass_t2 * dvv[T2], T2);
     const R term_a = quot(dvv[A], A);
     R dv = (term_t1 + term_t2 + term_a) * dt;
-    const R cvc = cv_r[c];
+    const R cvc = cur.cv;
     cv1_r[c] = cvc * (R(1) + dv);
     if (g.write_cv2) {
       dv = (term_t1 + term_t2) * dt;
@@ -421,7 +453,7 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
     }
     dc1_r[c] = R(0.5) * (d0 + d1);
     vz_prev = vz_cur;
-    vz_cur = A == 2 ? vz_next : (iz < z1 ? vzf(c + sxy) : R(0));
+    vz_cur = A == 2 ? vz_next : (iz < z1 ? vz_above : R(0));
   }
 }
 
