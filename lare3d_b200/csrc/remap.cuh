@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(128) k_geom_march(GeomArgs<R> g) {
 // bit for bit.  dm around c - e_A needs the quads of planes z-1 and z (A = z,
 // one more plane carried) or the quads shifted by one cell in x or y (two
 // more loads per plane).
-constexpr int kVertZ = 32;
+constexpr int kVertZ = 16;
 
 template <class R>
 struct VertArgs {
@@ -1154,11 +1154,10 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   const double* sc = run.sc;
   const bool write_cv2 = !predictor;
 
-  // ---- K1: cv1, cv2, db1, dc1 over the whole cell box -1..n+2 (z-marching for the
-  // z sweep and, in the exact FP64 build, the x sweep; per cell for the y
-  // sweep, the FP32 x sweep and the product FP64 x sweep, where the marching
-  // form measured slower)
-  if (A == 2 || (A == 0 && sizeof(R) == 8 && !LARE_FAST)) {
+  // ---- K1: cv1, cv2, db1, dc1 over the whole cell box -1..n+2 (z-marching for
+  // every FP32 sweep, the FP64 z sweep and the exact FP64 x sweep; per cell for
+  // the other FP64 sweeps, where the marching form measured no faster)
+  if (A == 2 || sizeof(R) == 4 || (A == 0 && !LARE_FAST)) {
     GeomArgs<R> ga;
     ga.vx1 = vx1;
     ga.vy1 = Ar.vy1.p;
@@ -1251,11 +1250,12 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     ba.na = na;
     ba.n0 = nx + 3;
     ba.n1 = (A == 1 ? nz : ny) + 3;
-    const int k = run.prof_begin(A == 0 ? "remap_sweep_bflux_x" : "remap_sweep_bflux_march", 0, 7, (double)(nx + 3) * (ny + 3) * (nz + 3));
+    const int k = run.prof_begin(A == 0 ? "remap_sweep_bflux_x" : "remap_sweep_bflux_march", 0, 7,
+                                 (double)(nx + 3) * (ny + 3) * (nz + 3));
     if (A != 0) {
       dim3 blk(32, 4, 1);
       dim3 grd((ba.n0 + 31) / 32, (ba.n1 + 3) / 4, (na + 3 + kMarch - 1) / kMarch);
-      if (sizeof(R) == 8) {  // one flux per thread: measured faster in FP64, slower in FP32
+      if (sizeof(R) == 8) {  // one flux per thread in FP64 (half the registers); FP32 measured the same either way
         dim3 grd1((ba.n0 + 31) / 32, (ba.n1 + 3) / 4, 2 * ((na + 3 + kMarch - 1) / kMarch));
         k_bflux_march1<R><<<grd1, blk, 0, run.s>>>(ba);
       } else {
