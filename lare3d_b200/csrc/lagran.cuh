@@ -423,7 +423,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
   R* const fxv = A.fx_visc.p;
   R* const fyv = A.fy_visc.p;
   R* const fzv = A.fz_visc.p;
-  LARE_BOXWH(run, 4, 2, 13, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
+  LARE_BOXWB(run, 4, 13, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
     auto d2 = [&](int p0, int p1) {
       R ux = vx[p0] - vx[p1];

@@ -1119,6 +1119,12 @@ __global__ void __launch_bounds__(128) k_mass_energy_x(MEArgs<R> a, int sx, int 
   a.energy_new[c] = e;
 }
 
+LARE_END  // namespace lare
+
+#include "remap_vm.cuh"
+
+LARE_BEGIN
+
 template <int A, class R>
 void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   constexpr int T1 = A == 0 ? 1 : 0, T2 = A == 2 ? 1 : 2;  // transverse axes, T1 < T2
@@ -1356,7 +1362,10 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   R* const cv1v = Ar.cv1v.p;
   R* const cv2v = Ar.cv2v.p;
   R* const dmv = Ar.dmv.p;
-  {
+  // product and FP32 builds, y and z sweeps, rke off: the vertex averages are
+  // formed inside the momentum march (remap_vm.cuh)
+  const bool fused_vm = LARE_FAST && A != 0 && !run.p.rke;
+  if (!fused_vm) {
     int lo[3] = {0, 0, 0}, hi[3] = {nx, ny, nz};
     lo[A] = -1;
     hi[A] = na + 1;
@@ -1419,9 +1428,19 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     gm.S3 = A == 1 ? sxy : sx;
     const bool rke = run.p.rke != 0;
     for (int q = 0; q < 3; ++q) gm.fp[q] = rke ? Ar.rke_f[q].p : nullptr;
-    const int k = run.prof_begin(A == 0 ? "remap_sweep_mom_x" : "remap_sweep_mom_march", 0, rke ? 17 : 14,
-                                 (double)(nx + 1) * (ny + 1) * (nz + 1));
-    if (A == 0) {
+    // words: fused, v (3), v1, db1, dc1, rho, cv1, cv2, dm read and the new v (3) written
+    const int k = run.prof_begin(A == 0 ? "remap_sweep_mom_x" : (fused_vm ? "remap_sweep_vert_mom_march" : "remap_sweep_mom_march"), 0,
+                                 fused_vm ? 13 : (rke ? 17 : 14), (double)(nx + 1) * (ny + 1) * (nz + 1));
+    if (fused_vm) {
+      VMArgs<R> vm;
+      vm.m = gm;
+      vm.rho = rho;
+      vm.cv1 = cv1;
+      vm.cv2 = cv2;
+      vm.dm = dm;
+      dim3 grd((nx + 1 + 31) / 32, (gm.n3 + 1 + 3) / 4, (na + 1 + kMomA - 1) / kMomA);
+      k_vm_march<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(vm);
+    } else if (A == 0) {
       dim3 grd((nx + 1 + 30) / 31, (ny + 1 + 3) / 4, nz + 1);
       if (rke)
         k_mom_x<R, true><<<grd, dim3(32, 4, 1), 0, run.s>>>(gm);
