@@ -1362,9 +1362,11 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   R* const cv1v = Ar.cv1v.p;
   R* const cv2v = Ar.cv2v.p;
   R* const dmv = Ar.dmv.p;
-  // product and FP32 builds, y and z sweeps, rke off: the vertex averages are
-  // formed inside the momentum march (remap_vm.cuh)
-  const bool fused_vm = LARE_FAST && A != 0 && !run.p.rke;
+  // FP64 product build, rke off: the vertex averages are formed inside the
+  // momentum kernel (remap_vm.cuh).  The FP32 form keeps the reference's
+  // summation order, whose rounding its 1e-5 error bar needs on the
+  // strongest shocks.
+  const bool fused_vm = LARE_FAST && sizeof(R) == 8 && !run.p.rke;
   if (!fused_vm) {
     int lo[3] = {0, 0, 0}, hi[3] = {nx, ny, nz};
     lo[A] = -1;
@@ -1429,8 +1431,9 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     const bool rke = run.p.rke != 0;
     for (int q = 0; q < 3; ++q) gm.fp[q] = rke ? Ar.rke_f[q].p : nullptr;
     // words: fused, v (3), v1, db1, dc1, rho, cv1, cv2, dm read and the new v (3) written
-    const int k = run.prof_begin(A == 0 ? "remap_sweep_mom_x" : (fused_vm ? "remap_sweep_vert_mom_march" : "remap_sweep_mom_march"), 0,
-                                 fused_vm ? 13 : (rke ? 17 : 14), (double)(nx + 1) * (ny + 1) * (nz + 1));
+    const char* site = fused_vm ? (A == 0 ? "remap_sweep_vert_mom_x" : "remap_sweep_vert_mom_march")
+                                : (A == 0 ? "remap_sweep_mom_x" : "remap_sweep_mom_march");
+    const int k = run.prof_begin(site, 0, fused_vm ? 13 : (rke ? 17 : 14), (double)(nx + 1) * (ny + 1) * (nz + 1));
     if (fused_vm) {
       VMArgs<R> vm;
       vm.m = gm;
@@ -1438,8 +1441,13 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
       vm.cv1 = cv1;
       vm.cv2 = cv2;
       vm.dm = dm;
-      dim3 grd((nx + 1 + 31) / 32, (gm.n3 + 1 + 3) / 4, (na + 1 + kMomA - 1) / kMomA);
-      k_vm_march<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(vm);
+      if (A == 0) {
+        dim3 grd((nx + 1 + kVMXOut - 1) / kVMXOut, (ny + 1 + 3) / 4, nz + 1);
+        k_vm_x<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(vm);
+      } else {
+        dim3 grd((nx + 1 + 31) / 32, (gm.n3 + 1 + 3) / 4, (na + 1 + kMomA - 1) / kMomA);
+        k_vm_march<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(vm);
+      }
     } else if (A == 0) {
       dim3 grd((nx + 1 + 30) / 31, (ny + 1 + 3) / 4, nz + 1);
       if (rke)

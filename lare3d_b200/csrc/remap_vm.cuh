@@ -1,5 +1,5 @@
-// remap_vm.cuh - vertex averages fused into the momentum march (y and z
-// sweeps of the product and FP32 builds, rke off).
+// remap_vm.cuh - vertex averages fused into the momentum kernels (FP64
+// product build, rke off).
 //
 // K7 of a sweep (xremap.f90:201-290 and the y/z mirrors) forms at each
 // vertex the eight-cell averages rho_v = sum(rho cv1) / sum(cv1),
@@ -13,9 +13,11 @@
 // per point instead of 9 + 14).  The eight-cell sums become two four-cell
 // sums added, a different association than the reference's left-to-right
 // sum, so this form serves the builds that are not bound to the
-// reference's rounding (LARE_FAST); the exact build keeps k_vert_march and
-// k_mom_march.  With rke on, the vertex arrays are needed by the kinetic
-// energy defect and the split form is used as well.
+// reference's rounding: the FP64 product build.  The exact build keeps
+// k_vert_march and k_mom_march, and so does the FP32 form, whose error bar
+// on the strongest shocks needs the reference's order.  With rke on, the
+// vertex arrays are needed by the kinetic energy defect and the split form
+// is used as well.
 #pragma once
 
 LARE_BEGIN
@@ -135,6 +137,71 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 4 : 8) k_vm_march(VMArgs
     s0 = sp;
     sp = s2;
   }
+}
+
+// The same for the x sweep: the lanes of a warp hold consecutive x
+// positions.  Each lane reduces the slice of cells at its x (the 2 x 2 cells
+// in y and z) and takes the slices of the lanes beside it by shuffles: its
+// vertex averages from its own slice and the next, the dm average below
+// from the previous, the density of the next vertex from the next lane.  A
+// lane's face flux needs the two lanes above it, and its update the flux of
+// the lane below, so a warp updates the kVMXOut = 29 vertices of lanes 1..29.
+constexpr int kVMXOut = 29;
+
+template <class R>
+__global__ void __launch_bounds__(128) k_vm_x(VMArgs<R> a) {
+  const MomArgs<R>& g = a.m;
+  const int lane = (int)threadIdx.x;                          // blockDim.x == 32: one warp per row
+  const int ix = -1 + (int)blockIdx.x * kVMXOut + lane;       // vertex / face x position
+  const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int iz = (int)blockIdx.z;
+  if (iy > g.ny) return;                                      // uniform over the warp
+  const int sx = g.sx, sxy = g.sxy;
+  const int c = min(ix, g.nx + 2) + sx * iy + sxy * iz;       // lanes past n + 2 load n + 2 (unused)
+  const R dt = (R)g.sc[g.dt_slot];
+  const R eighth = R(0.125);
+  const unsigned all = 0xffffffffu;
+  // this lane's slice: cells (x, y..y+1, z..z+1)
+  const int o[4] = {0, sx, sxy, sx + sxy};
+  R p = R(0), wv = R(0), w2 = R(0), d = R(0);
+  {
+    R c1[4], r[4], c2[4], m[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      c1[q] = a.cv1[c + o[q]];
+      r[q] = a.rho[c + o[q]];
+      c2[q] = a.cv2[c + o[q]];
+      m[q] = a.dm[c + o[q]];
+    }
+    p = r[0] * c1[0] + r[1] * c1[1] + r[2] * c1[2] + r[3] * c1[3];
+    wv = c1[0] + c1[1] + c1[2] + c1[3];
+    w2 = c2[0] + c2[1] + c2[2] + c2[3];
+    d = m[0] + m[1] + m[2] + m[3];
+  }
+  const R p1 = __shfl_down_sync(all, p, 1), wv1 = __shfl_down_sync(all, wv, 1);
+  const R w21 = __shfl_down_sync(all, w2, 1), d1 = __shfl_down_sync(all, d, 1);
+  const R dlo = __shfl_up_sync(all, d, 1);
+  const R rvc = qdiv(p + p1, wv + wv1);                       // vertex x
+  const R rvn = __shfl_down_sync(all, rvc, 1);                // vertex x + 1
+  const R dmv = (d + d1) * eighth;
+  // the face flux between vertices x and x + 1 (faces -1..n)
+  R w[3][4];
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[comp][q] = g.v[comp][c + (q - 1)];
+  R F[3], fpre[3];
+  mom_flux_vals<R, false>(g.dct1(iy) * g.dct2(iz), g.va[c], g.va[c + 1], rvc, rvn, dmv, g.db1[c], g.db1[c + 1],
+                          g.db1[c + 2], g.dc1[c], g.dc1[c + 1], w, dt, F, fpre);
+  R Fm[3];
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) Fm[comp] = __shfl_up_sync(all, F[comp], 1);
+  if (lane < 1 || lane > kVMXOut || ix < 0 || ix > g.nx) return;
+  const R cc1 = (wv + wv1) * eighth, cc2 = (w2 + w21) * eighth, dmm = (dlo + d) * eighth;
+  const R rv1 = qdiv(rvc * cc1 + dmm - dmv, cc2);
+  const R den = dv_of(cc2 * rv1);
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) g.vn[comp][c] = dv_div(rvc * w[comp][1] * cc1 + Fm[comp] - F[comp], den);
 }
 
 LARE_END  // namespace lare
