@@ -1362,11 +1362,9 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
   R* const cv1v = Ar.cv1v.p;
   R* const cv2v = Ar.cv2v.p;
   R* const dmv = Ar.dmv.p;
-  // FP64 product build, rke off: the vertex averages are formed inside the
-  // momentum kernel (remap_vm.cuh).  The FP32 form keeps the reference's
-  // summation order, whose rounding its 1e-5 error bar needs on the
-  // strongest shocks.
-  const bool fused_vm = LARE_FAST && sizeof(R) == 8 && !run.p.rke;
+  // rke off: the vertex averages are formed inside the momentum kernel, in
+  // the reference's summation order (remap_vm.cuh)
+  const bool fused_vm = !run.p.rke;
   if (!fused_vm) {
     int lo[3] = {0, 0, 0}, hi[3] = {nx, ny, nz};
     lo[A] = -1;
@@ -1441,12 +1439,12 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
       vm.cv1 = cv1;
       vm.cv2 = cv2;
       vm.dm = dm;
-      if (A == 0) {
+      if constexpr (A == 0) {
         dim3 grd((nx + 1 + kVMXOut - 1) / kVMXOut, (ny + 1 + 3) / 4, nz + 1);
         k_vm_x<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(vm);
       } else {
         dim3 grd((nx + 1 + 31) / 32, (gm.n3 + 1 + 3) / 4, (na + 1 + kMomA - 1) / kMomA);
-        k_vm_march<R><<<grd, dim3(32, 4, 1), 0, run.s>>>(vm);
+        k_vm_march<A, R><<<grd, dim3(32, 4, 1), 0, run.s>>>(vm);
       }
     } else if (A == 0) {
       dim3 grd((nx + 1 + 30) / 31, (ny + 1 + 3) / 4, nz + 1);
