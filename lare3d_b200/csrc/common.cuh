@@ -120,6 +120,21 @@ __device__ __forceinline__ R dv_div(R a, R dv) {
 #endif
 }
 
+// Asynchronous copy of one element from global to shared memory (PTX
+// cp.async, 4 or 8 bytes, cached in L1), in commit groups that complete in
+// order: a plane of a tile is copied without passing through registers.
+template <class R>
+__device__ __forceinline__ void cp_async_elem(R* smem, const R* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(gmem), "n"((int)sizeof(R)) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Wait until at most N of this thread's most recent groups are in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait_prior() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Scalar slots kept in device memory so that a whole step can run (and be
 // captured in a CUDA graph) without the host knowing dt.
 enum Slot {

@@ -304,15 +304,16 @@ inline void ghost(Run<R>& run, const GSpec& g, A3<R> a, A3<R>* b = nullptr, A3<R
 }
 
 // Deterministic sum of NV values over a box, into sc[slot..] (+=).
-// words: the algorithmic words per point the kernel moves (for the profile).
+// site names the launch in the profile; words: the algorithmic words per
+// point the kernel moves.
 template <int NV, class R, class Fn>
-inline void box_sum(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn, int slot, bool acc,
-                    int words = 0, int planes = kSumPlanes) {
+inline void box_sum(Run<R>& run, const char* site, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn, int slot,
+                    bool acc, int words = 0, int planes = kSumPlanes) {
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   dim3 blk(64, 4, 1);
   dim3 grd((ni + 63) / 64, (nj + 3) / 4, (nk + planes - 1) / planes);
   int nb = grd.x * grd.y * grd.z;
-  int k = run.prof_begin("box_sum", 0, words, (double)ni * nj * nk);
+  int k = run.prof_begin(site, 0, words, (double)ni * nj * nk);
   k_box_sum<NV><<<grd, blk, 0, run.s>>>(i0, j0, k0, ni, nj, nk, planes, fn, run.partial);
   k_sum_partials<NV><<<1, 1024, 0, run.s>>>(run.partial, nb, run.sc + slot, acc ? 1 : 0);
   run.prof_end(k);
@@ -320,11 +321,12 @@ inline void box_sum(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1,
 }
 
 template <int NV, class R, class Fn>
-inline void box_min(Run<R>& run, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn, int uslot, int words = 0) {
+inline void box_min(Run<R>& run, const char* site, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn, int uslot,
+                    int words = 0) {
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
   dim3 blk(64, 4, 1);
   dim3 grd((ni + 63) / 64, (nj + 3) / 4, nk);
-  int k = run.prof_begin("box_min", 0, words, (double)ni * nj * nk);
+  int k = run.prof_begin(site, 0, words, (double)ni * nj * nk);
   k_box_min<NV><<<grd, blk, 0, run.s>>>(i0, j0, k0, ni, nj, fn, run.us + uslot);
   run.prof_end(k);
   ++run.launches;
@@ -493,7 +495,7 @@ void calc_s_stages(Run<R>& run, int dt_slot) {
   });
   unsigned long long* us = run.us;
   launch_scalar(run.s, run.launches, [=] __device__() { us[U_DTPARAB] = (unsigned long long)__double_as_longlong(1.e10); });
-  box_min<1>(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
+  box_min<1>(run, "parabolic_dt_min", 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
     R kappa1 = k0 * larsen(ix, iy, iz);
     const R x = pip ? xia(ix, iy, iz) : xi;
     R temp = (g - R(1)) / (R(2) - x) * (energy(ix, iy, iz) - (R(1) - x) * ip);
@@ -757,9 +759,12 @@ void eulerian_remap(Run<R>& run, int step) {
   // B -> flux (remap.f90:43-69), including the -2 layers.
   LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
-    if (iy >= -1 && iz >= -1) bx[c] = bx[c] * dyb(iy) * dzb(iz);
-    if (ix >= -1 && iz >= -1) by[c] = by[c] * dxb(ix) * dzb(iz);
-    if (ix >= -1 && iy >= -1) bz[c] = bz[c] * dxb(ix) * dyb(iy);
+    // all loads before any store (the three arrays are distinct)
+    const bool ox = iy >= -1 && iz >= -1, oy = ix >= -1 && iz >= -1, oz = ix >= -1 && iy >= -1;
+    const R x = ox ? bx[c] : R(0), y = oy ? by[c] : R(0), z = oz ? bz[c] : R(0);
+    if (ox) bx[c] = x * dyb(iy) * dzb(iz);
+    if (oy) by[c] = y * dxb(ix) * dzb(iz);
+    if (oz) bz[c] = z * dxb(ix) * dyb(iy);
   });
   static const int order[6][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}, {0, 2, 1}, {2, 1, 0}, {1, 0, 2}};
   int cse = ((step % 6) + 6) % 6;
@@ -777,9 +782,12 @@ void eulerian_remap(Run<R>& run, int step) {
   const auto rbx = run.a.rdb[0], rby = run.a.rdb[1], rbz = run.a.rdb[2];
   LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
-    if (iy >= -1 && iz >= -1) qx[c] = div_rcp(div_rcp(qx[c], dyb(iy), rby(iy)), dzb(iz), rbz(iz));
-    if (ix >= -1 && iz >= -1) qy[c] = div_rcp(div_rcp(qy[c], dxb(ix), rbx(ix)), dzb(iz), rbz(iz));
-    if (ix >= -1 && iy >= -1) qz[c] = div_rcp(div_rcp(qz[c], dxb(ix), rbx(ix)), dyb(iy), rby(iy));
+    // all loads before any store (the three arrays are distinct)
+    const bool ox = iy >= -1 && iz >= -1, oy = ix >= -1 && iz >= -1, oz = ix >= -1 && iy >= -1;
+    const R x = ox ? qx[c] : R(0), y = oy ? qy[c] : R(0), z = oz ? qz[c] : R(0);
+    if (ox) qx[c] = div_rcp(div_rcp(x, dyb(iy), rby(iy)), dzb(iz), rbz(iz));
+    if (oy) qy[c] = div_rcp(div_rcp(y, dxb(ix), rbx(ix)), dzb(iz), rbz(iz));
+    if (oz) qz[c] = div_rcp(div_rcp(z, dxb(ix), rbx(ix)), dyb(iy), rby(iy));
   });
   bfield_bcs(run);
 }
@@ -799,7 +807,7 @@ void energy_account(Run<R>& run) {
   Arrays<R>& A = run.a;
   auto bx = A.bx, by = A.by, bz = A.bz, cv = A.cv, energy = A.energy, rho = A.rho;
   auto vx = A.vx, vy = A.vy, vz = A.vz;
-  box_sum<2>(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
+  box_sum<2>(run, "energy_account_cells", 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
     int ixm = ix - 1, iym = iy - 1, izm = iz - 1;
     double b0 = bx(ix, iy, iz), b1 = bx(ixm, iy, iz), c0 = by(ix, iy, iz), c1 = by(ix, iym, iz);
     double d0 = bz(ix, iy, iz), d1 = bz(ix, iy, izm);
@@ -813,7 +821,7 @@ void energy_account(Run<R>& run) {
   // SC_EN_B and SC_EN_B+1 hold en_b and en_int; move en_int to its slot.
   double* sc = run.sc;
   launch_scalar(run.s, run.launches, [=] __device__() { sc[SC_EN_INT] = sc[SC_EN_B + 1]; });
-  box_sum<1>(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz, double* v) {
+  box_sum<1>(run, "energy_account_vertices", 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz, double* v) {
     int ixp = ix + 1, iyp = iy + 1, izp = iz + 1;
     auto r = [&](int a, int b, int c) { return (double)rho(a, b, c) * (double)cv(a, b, c); };
     auto w = [&](int a, int b, int c) { return (double)cv(a, b, c); };

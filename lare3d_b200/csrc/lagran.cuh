@@ -31,6 +31,8 @@
 
 #include <utility>
 
+#include "lp4_tile.cuh"
+
 LARE_BEGIN
 
 // Vertex current of eta_calc (lagran.F90:1190-1216), rkstep (:1479-1494)
@@ -288,7 +290,7 @@ void resistive_update(Run<R>& run) {
   const R* rho = A.rho.p;
   R* const ctb = run.p.cooling_term ? A.cool_term_b.p : nullptr;  // :1290-1302
   const R alpha = (R)run.p.alpha_av;
-  box_sum<1>(run, -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz, double* v) {
+  box_sum<1>(run, "ohmic_heating_sum", -1, nx + 2, -1, ny + 2, -1, nz + 2, [=] __device__(int ix, int iy, int iz, double* v) {
     const R dt = (R)sc[SC_DTSUB];
     const int c = ix + sx * iy + sxy * iz;
     R e = energy[c];
@@ -423,59 +425,39 @@ void prologue_and_shock_viscosity(Run<R>& run) {
   R* const fxv = A.fx_visc.p;
   R* const fyv = A.fy_visc.p;
   R* const fzv = A.fz_visc.p;
-  LARE_BOXWB(run, 4, 13, 0, nx + 1, 0, ny + 1, 0, nz + 1, [=] __device__(int ix, int iy, int iz) {
-    const int c = ix + sx * iy + sxy * iz;
-    auto d2 = [&](int p0, int p1) {
-      R ux = vx[p0] - vx[p1];
-      R uy = vy[p0] - vy[p1];
-      R uz = vz[p0] - vz[p1];
-      return ux * ux + uy * uy + uz * uz;
-    };
-    const int X = 1, Y = sx, Z = sxy;
-    R a1 = d2(c - X - Y - Z, c - Y - Z);
-    R a2 = d2(c - Y - Z, c - Z);
-    R a3 = d2(c - Z, c - X - Z);
-    R a4 = d2(c - X - Z, c - X - Y - Z);
-    R a5 = d2(c - X - Y, c - Y);
-    R a6 = d2(c - Y, c);
-    R a7 = d2(c, c - X);
-    R a8 = d2(c - X, c - X - Y);
-    R a9 = d2(c - Z, c);
-    R a10 = d2(c - X - Z, c - X);
-    R a11 = d2(c - X - Y - Z, c - X - Y);
-    R a12 = d2(c - Y - Z, c - Y);
-    R pv = R(0);
-    pv = fmax(pv, -alpha1[c] * sqrt(a1));
-    pv = fmax(pv, -alpha2[c] * sqrt(a2));
-    pv = fmax(pv, -alpha3[c] * sqrt(a9));
-    p_visc[c] = pv;
-    R ddx = dxb(ix), ddy = dyb(iy), ddz = dzb(iz);
-    R vh = -R(0.25) * ddy * ddz * alpha1[c] * a1 - R(0.25) * ddx * ddz * alpha2[c] * a2 -
-           R(0.25) * ddy * ddz * alpha1[c + Y] * a3 - R(0.25) * ddx * ddz * alpha2[c - X] * a4 -
-           R(0.25) * ddy * ddz * alpha1[c + Z] * a5 - R(0.25) * ddx * ddz * alpha2[c + Z] * a6 -
-           R(0.25) * ddy * ddz * alpha1[c + Y + Z] * a7 - R(0.25) * ddx * ddz * alpha2[c - X + Z] * a8 -
-           R(0.25) * ddx * ddy * alpha3[c] * a9 - R(0.25) * ddx * ddy * alpha3[c - X] * a10 -
-           R(0.25) * ddx * ddy * alpha3[c - X - Y] * a11 - R(0.25) * ddx * ddy * alpha3[c - Y] * a12;
-    visc_heat[c] = qdiv(vh, cv[c]);
-    if (ix <= nx && iy <= ny && iz <= nz) {
-      R b1 = alpha1[c + Y + Z] * dyc(iy) * dzc(iz);
-      R b2 = alpha1[c + X + Y + Z] * dyc(iy) * dzc(iz);
-      R b3 = alpha2[c + Z] * dxc(ix) * dzc(iz);
-      R b4 = alpha2[c + Y + Z] * dxc(ix) * dzc(iz);
-      R b5 = alpha3[c] * dxc(ix) * dyc(iy);
-      R b6 = alpha3[c + Z] * dxc(ix) * dyc(iy);
-      const R cvv = dv_of(cv_v[c]);
-      auto f = [&](const R* v) {
-        R v0 = v[c];
-        return dv_div(b1 * (v0 - v[c - X]) + b2 * (v0 - v[c + X]) + b3 * (v0 - v[c - Y]) + b4 * (v0 - v[c + Y]) +
-                          b5 * (v0 - v[c - Z]) + b6 * (v0 - v[c + Z]),
-                      cvv);
-      };
-      fxv[c] = f(vx);
-      fyv[c] = f(vy);
-      fzv[c] = f(vz);
-    }
-  });
+  {
+    LP4Args<R> l4;
+    l4.vx = vx;
+    l4.vy = vy;
+    l4.vz = vz;
+    l4.alpha1 = alpha1;
+    l4.alpha2 = alpha2;
+    l4.alpha3 = alpha3;
+    l4.cv = cv;
+    l4.cv_v = cv_v;
+    l4.p_visc = p_visc;
+    l4.visc_heat = visc_heat;
+    l4.fx = fxv;
+    l4.fy = fyv;
+    l4.fz = fzv;
+    l4.dxb = dxb;
+    l4.dyb = dyb;
+    l4.dzb = dzb;
+    l4.dxc = dxc;
+    l4.dyc = dyc;
+    l4.dzc = dzc;
+    l4.nx = nx;
+    l4.ny = ny;
+    l4.nz = nz;
+    l4.sx = sx;
+    l4.sxy = sxy;
+    const dim3 blk(kL4X, kL4Y, 1);
+    const dim3 grd((nx + 2 + kL4X - 1) / kL4X, (ny + 2 + kL4Y - 1) / kL4Y, (nz + 2 + kL4Z - 1) / kL4Z);
+    const int k = run.prof_begin("shock_viscosity_lp4_tile", 0, 13, (double)(nx + 2) * (ny + 2) * (nz + 2));
+    k_lp4_tile<R><<<grd, blk, 0, run.s>>>(l4);
+    run.prof_end(k);
+    ++run.launches;
+  }
 }
 
 // ---------------------------------------------------------------------
@@ -524,7 +506,7 @@ void set_dt(Run<R>& run) {
     us[U_DTMIN] = (unsigned long long)__double_as_longlong(DBL_MAX);
     us[U_DTRMIN] = (unsigned long long)__double_as_longlong(DBL_MAX);
   });
-  box_min<2>(run, 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz, double* v) {
+  box_min<2>(run, "set_dt_min", 0, nx, 0, ny, 0, nz, [=] __device__(int ix, int iy, int iz, double* v) {
     const int c = ix + sx * iy + sxy * iz;
     R w1 = bx[c] * bx[c] + by[c] * by[c] + bz[c] * bz[c];
     R rho0 = fmax(rho[c], Num<R>::tiny());
@@ -532,7 +514,7 @@ void set_dt(Run<R>& run) {
     R w2 = dv_div(w1, dr);
     R gb = gamma_boris[c];
     if (boris && (w2 >= va_max2)) {
-      gb = R(1) / (R(1) + w2 / va_max2);
+      gb = qdiv(R(1), R(1) + qdiv(w2, va_max2));
       gamma_boris[c] = gb;
     }
     R cs2 = dv_div(g * pressure[c] + gb * w1, dr);
@@ -544,12 +526,11 @@ void set_dt(Run<R>& run) {
                  qdiv(dzb(iz), fmax(fabs(vz[c]), Num<R>::tiny())));
     dt_local = fmin(dt_local, dt2);
     R dt3 = Num<R>::huge();
-    if (cowling) {  // lagran.F90:1132-1134
-      R dxlocal = R(1) / (R(1) / (dxb(ix) * dxb(ix)) + R(1) / (dyb(iy) * dyb(iy)) + R(1) / (dzb(iz) * dzb(iz)));
-      dt3 = R(0.2) * dxlocal / fmax(fmax(eta[c], eta_perp[c]), Num<R>::tiny());
-    } else if (resistive) {
-      R dxlocal = R(1) / (R(1) / (dxb(ix) * dxb(ix)) + R(1) / (dyb(iy) * dyb(iy)) + R(1) / (dzb(iz) * dzb(iz)));
-      dt3 = R(0.2) * dxlocal / fmax(eta[c], Num<R>::tiny());
+    if (cowling || resistive) {  // lagran.F90:1132-1134 (Cowling), :1136-1138
+      const R dxlocal =
+          qdiv(R(1), qdiv(R(1), dxb(ix) * dxb(ix)) + qdiv(R(1), dyb(iy) * dyb(iy)) + qdiv(R(1), dzb(iz) * dzb(iz)));
+      const R e = cowling ? fmax(eta[c], eta_perp[c]) : eta[c];
+      dt3 = qdiv(R(0.2) * dxlocal, fmax(e, Num<R>::tiny()));
     }
     v[0] = (double)dt_local;
     v[1] = (double)dt3;
@@ -604,9 +585,12 @@ void predictor_remap(Run<R>& run, int step) {
   auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb;
   LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
-    if (iy >= -1 && iz >= -1) px[c] = bx[c] * dyb(iy) * dzb(iz);
-    if (ix >= -1 && iz >= -1) py[c] = by[c] * dxb(ix) * dzb(iz);
-    if (ix >= -1 && iy >= -1) pz[c] = bz[c] * dxb(ix) * dyb(iy);
+    // all loads before any store
+    const bool ox = iy >= -1 && iz >= -1, oy = ix >= -1 && iz >= -1, oz = ix >= -1 && iy >= -1;
+    const R x = ox ? bx[c] : R(0), y = oy ? by[c] : R(0), z = oz ? bz[c] : R(0);
+    if (ox) px[c] = x * dyb(iy) * dzb(iz);
+    if (oy) py[c] = y * dxb(ix) * dzb(iz);
+    if (oz) pz[c] = z * dxb(ix) * dyb(iy);
   });
   std::swap(A.bx.p, A.bx0.p);
   std::swap(A.by.p, A.by0.p);
@@ -642,22 +626,29 @@ void predictor_remap(Run<R>& run, int step) {
   const auto rbx = run.a.rdb[0], rby = run.a.rdb[1], rbz = run.a.rdb[2];
   LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
     const int c = ix + sx * iy + sxy * iz;
-    if (iy >= -1 && iz >= -1) qx[c] = div_rcp(div_rcp(qx[c], dyb(iy), rby(iy)), dzb(iz), rbz(iz));
-    if (ix >= -1 && iz >= -1) qy[c] = div_rcp(div_rcp(qy[c], dxb(ix), rbx(ix)), dzb(iz), rbz(iz));
-    if (ix >= -1 && iy >= -1) qz[c] = div_rcp(div_rcp(qz[c], dxb(ix), rbx(ix)), dyb(iy), rby(iy));
+    // all loads before any store (the three arrays are distinct)
+    const bool ox = iy >= -1 && iz >= -1, oy = ix >= -1 && iz >= -1, oz = ix >= -1 && iy >= -1;
+    const R x = ox ? qx[c] : R(0), y = oy ? qy[c] : R(0), z = oz ? qz[c] : R(0);
+    if (ox) qx[c] = div_rcp(div_rcp(x, dyb(iy), rby(iy)), dzb(iz), rbz(iz));
+    if (oy) qy[c] = div_rcp(div_rcp(y, dxb(ix), rbx(ix)), dzb(iz), rbz(iz));
+    if (oz) qz[c] = div_rcp(div_rcp(z, dxb(ix), rbx(ix)), dyb(iy), rby(iy));
   });
   bfield_bcs(run);
 }
 
-// PC3 (shock_heating, lagran.F90:396-458, and v = 2 v1 - v) as a
-// z-marching kernel: a thread owns an (x, y) column of cells and walks a
-// chunk of z.  The twelve edge terms of cell (x, y, z) join the four
-// corners of plane z-1 (c-Z, c-X-Z, c-Y-Z, c-X-Y-Z) and of plane z (c,
-// c-X, c-Y, c-X-Y); the plane z-1 edges are the previous cell's plane z
-// edges, and the plane z-1 corner values are the previous step's, so a step
-// loads the four new corners and forms eight edge terms instead of twelve.
-// alpha1 and alpha2 at c+Z, c+Y+Z, c-X+Z are the next cell's c, c+Y, c-X.
-// Same expressions, same operands, same results bit for bit.
+// PC3 (shock_heating, lagran.F90:396-458, and v = 2 v1 - v) as a tiled
+// z-march: a CTA of 32 x 8 threads owns 32 x 8 cells and walks a chunk of z
+// with the corner planes z-1 and z of the six velocity arrays (v and v1,
+// with a one-vertex halo below in x and y) in shared memory; plane z+1 is
+// loaded into registers while plane z is computed.  The twelve edge terms of
+// cell (x, y, z) join the four corners of plane z-1 (c-Z, c-X-Z, c-Y-Z,
+// c-X-Y-Z) and of plane z (c, c-X, c-Y, c-X-Y); the four plane z-1 edges are
+// the previous cell's plane z edges and are carried, and alpha1 and alpha2
+// at c+Z, c+Y+Z, c-X+Z are the next cell's c, c+Y, c-X.  Each velocity is
+// read from memory about once per CTA, and no thread holds a window of
+// corner values (a register-window march needed 130 registers and ran
+// 0.59-0.64 ms against 0.55 ms at 256^3 in FP64, 0.33 against 0.30 ms in
+// FP32).  Same expressions, same operands, same results bit for bit.
 constexpr int kShockZ = 32;
 
 template <class R>
@@ -673,66 +664,93 @@ struct ShockArgs {
   int nx, ny, nz, sx, sxy;
 };
 
+constexpr int kShX = 32, kShY = 8;
+constexpr int kShW = kShX + 1, kShP = kShW * (kShY + 1);  // plane row and size
+
 template <class R>
-__global__ void __launch_bounds__(128) k_shock_march(ShockArgs<R> g) {
-  // distinct arrays (no output is an input): restrict lets the compiler
-  // hoist the next plane's loads above this plane's stores
-  const R* __restrict__ alpha1_r = g.alpha1;
-  const R* __restrict__ alpha2_r = g.alpha2;
-  const R* __restrict__ alpha3_r = g.alpha3;
-  const R* __restrict__ cv_r = g.cv;
-  R* __restrict__ vhp_r = g.vhp;
-  const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y);
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
+__global__ void __launch_bounds__(kShX * kShY, sizeof(R) == 8 ? 2 : 4) k_shock_tile(ShockArgs<R> g) {
+  __shared__ R Vs[2][6][kShP];  // [plane slot][array][element]
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kShX + tx;
+  const int ix0 = blockIdx.x * kShX, iy0 = blockIdx.y * kShY;
+  const int ix = ix0 + tx, iy = iy0 + ty;
   const int z0 = (int)blockIdx.z * kShockZ;
   const int z1 = min(z0 + kShockZ - 1, g.nz + 1);
   const int sx = g.sx, sxy = g.sxy;
-  const int X = 1, Y = sx;
-  const int off[4] = {0, -X, -Y, -X - Y};  // corners c, c-X, c-Y, c-X-Y of a plane
-  R lo[6][4];
-  int c = ix + sx * iy + sxy * z0;
+  const bool cell = ix <= g.nx + 1 && iy <= g.ny + 1;
+  // the plane elements this thread loads (vertex x in ix0-1..ix0+31, y in
+  // iy0-1..iy0+7, clamped to the array: clamped values are never used)
+  int off[2];
+  bool has[2];
 #pragma unroll
-  for (int k = 0; k < 6; ++k)
+  for (int q = 0; q < 2; ++q) {
+    const int e = tid + q * kShX * kShY;
+    has[q] = e < kShP;
+    const int jj = has[q] ? e / kShW : 0, ii = has[q] ? e - jj * kShW : 0;
+    off[q] = min(ix0 - 1 + ii, g.nx + 2) + sx * min(iy0 - 1 + jj, g.ny + 2);
+  }
+  R nxt[6][2];  // plane k's elements, in flight
+  auto fetch = [&](int k) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) lo[k][q] = g.v[k][c - sxy + off[q]];
-  // dd of two corners: sum over the components of dv * dv1
-  auto dd = [](const R (&p)[6][4], int i, const R (&r)[6][4], int j) {
-    return (p[0][i] - r[0][j]) * (p[3][i] - r[3][j]) + (p[1][i] - r[1][j]) * (p[4][i] - r[4][j]) +
-           (p[2][i] - r[2][j]) * (p[5][i] - r[5][j]);
+    for (int m = 0; m < 6; ++m)
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        if (has[q]) nxt[m][q] = __ldg(g.v[m] + off[q] + sxy * k);
   };
+  auto stash = [&](int k) {
+#pragma unroll
+    for (int m = 0; m < 6; ++m)
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        if (has[q]) Vs[k & 1][m][tid + q * kShX * kShY] = nxt[m][q];
+  };
+  const int e = (ty + 1) * kShW + tx + 1;  // corner c of this thread's cell in a plane slot
+  const int oc[4] = {0, -1, -kShW, -1 - kShW};  // corners c, c-X, c-Y, c-X-Y
+  // dd of two corners (slot, corner): the components' dv * dv1 summed in order
+  auto dd = [&](int s1, int i, int s2, int j) {
+    const int p = e + oc[i], r = e + oc[j];
+    return (Vs[s1][0][p] - Vs[s2][0][r]) * (Vs[s1][3][p] - Vs[s2][3][r]) +
+           (Vs[s1][1][p] - Vs[s2][1][r]) * (Vs[s1][4][p] - Vs[s2][4][r]) +
+           (Vs[s1][2][p] - Vs[s2][2][r]) * (Vs[s1][5][p] - Vs[s2][5][r]);
+  };
+  fetch(z0 - 1);
+  stash(z0 - 1);
+  fetch(z0);
+  __syncthreads();
+  const int sl0 = (z0 - 1) & 1;
   // plane z0-1 edges: a1 = (c-X-Y-Z, c-Y-Z), a2 = (c-Y-Z, c-Z), a3 = (c-Z, c-X-Z), a4 = (c-X-Z, c-X-Y-Z)
-  R a1 = dd(lo, 3, lo, 2), a2 = dd(lo, 2, lo, 0), a3 = dd(lo, 0, lo, 1), a4 = dd(lo, 1, lo, 3);
-  R al1 = alpha1_r[c], al1y = alpha1_r[c + Y], al2 = alpha2_r[c], al2x = alpha2_r[c - X];
-  const R ddx = g.dxb(ix), ddy = g.dyb(iy);
+  R a1 = dd(sl0, 3, sl0, 2), a2 = dd(sl0, 2, sl0, 0), a3 = dd(sl0, 0, sl0, 1), a4 = dd(sl0, 1, sl0, 3);
+  int c = min(ix, g.nx + 1) + sx * min(iy, g.ny + 1) + sxy * z0;
+  R al1 = g.alpha1[c], al1y = g.alpha1[c + sx], al2 = g.alpha2[c], al2x = g.alpha2[c - 1];
+  const R ddx = g.dxb(min(ix, g.nx + 1)), ddy = g.dyb(min(iy, g.ny + 1));
   for (int iz = z0; iz <= z1; ++iz, c += sxy) {
-    R up[6][4];
+    stash(iz);  // its slot held plane iz - 2, last read before the previous barrier
+    if (iz < z1) fetch(iz + 1);
+    __syncthreads();
+    const int su = iz & 1, sl = su ^ 1;
+    const R a5 = dd(su, 3, su, 2);   // (c-X-Y, c-Y)
+    const R a6 = dd(su, 2, su, 0);   // (c-Y, c)
+    const R a7 = dd(su, 0, su, 1);   // (c, c-X)
+    const R a8 = dd(su, 1, su, 3);   // (c-X, c-X-Y)
+    const R a9 = dd(sl, 0, su, 0);   // (c-Z, c)
+    const R a10 = dd(sl, 1, su, 1);  // (c-X-Z, c-X)
+    const R a11 = dd(sl, 3, su, 3);  // (c-X-Y-Z, c-X-Y)
+    const R a12 = dd(sl, 2, su, 2);  // (c-Y-Z, c-Y)
+    const R al1z = g.alpha1[c + sxy], al1yz = g.alpha1[c + sx + sxy];
+    const R al2z = g.alpha2[c + sxy], al2xz = g.alpha2[c - 1 + sxy];
+    if (cell) {
+      const R ddz = g.dzb(iz);
+      const R vh = -R(0.25) * ddy * ddz * al1 * a1 - R(0.25) * ddx * ddz * al2 * a2 -
+                   R(0.25) * ddy * ddz * al1y * a3 - R(0.25) * ddx * ddz * al2x * a4 -
+                   R(0.25) * ddy * ddz * al1z * a5 - R(0.25) * ddx * ddz * al2z * a6 -
+                   R(0.25) * ddy * ddz * al1yz * a7 - R(0.25) * ddx * ddz * al2xz * a8 -
+                   R(0.25) * ddx * ddy * g.alpha3[c] * a9 - R(0.25) * ddx * ddy * g.alpha3[c - 1] * a10 -
+                   R(0.25) * ddx * ddy * g.alpha3[c - 1 - sx] * a11 - R(0.25) * ddx * ddy * g.alpha3[c - sx] * a12;
+      const R v = qdiv(vh, g.cv[c]);
+      g.vhp[c] = v > R(0) ? v : R(0);
+      if (ix <= g.nx && iy <= g.ny && iz <= g.nz) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) up[k][q] = g.v[k][c + off[q]];
-    const R a5 = dd(up, 3, up, 2);   // (c-X-Y, c-Y)
-    const R a6 = dd(up, 2, up, 0);   // (c-Y, c)
-    const R a7 = dd(up, 0, up, 1);   // (c, c-X)
-    const R a8 = dd(up, 1, up, 3);   // (c-X, c-X-Y)
-    const R a9 = dd(lo, 0, up, 0);   // (c-Z, c)
-    const R a10 = dd(lo, 1, up, 1);  // (c-X-Z, c-X)
-    const R a11 = dd(lo, 3, up, 3);  // (c-X-Y-Z, c-X-Y)
-    const R a12 = dd(lo, 2, up, 2);  // (c-Y-Z, c-Y)
-    const R al1z = alpha1_r[c + sxy], al1yz = alpha1_r[c + Y + sxy];
-    const R al2z = alpha2_r[c + sxy], al2xz = alpha2_r[c - X + sxy];
-    const R ddz = g.dzb(iz);
-    R vh = -R(0.25) * ddy * ddz * al1 * a1 - R(0.25) * ddx * ddz * al2 * a2 -
-           R(0.25) * ddy * ddz * al1y * a3 - R(0.25) * ddx * ddz * al2x * a4 -
-           R(0.25) * ddy * ddz * al1z * a5 - R(0.25) * ddx * ddz * al2z * a6 -
-           R(0.25) * ddy * ddz * al1yz * a7 - R(0.25) * ddx * ddz * al2xz * a8 -
-           R(0.25) * ddx * ddy * alpha3_r[c] * a9 - R(0.25) * ddx * ddy * alpha3_r[c - X] * a10 -
-           R(0.25) * ddx * ddy * alpha3_r[c - X - Y] * a11 - R(0.25) * ddx * ddy * alpha3_r[c - Y] * a12;
-    R v = qdiv(vh, cv_r[c]);
-    vhp_r[c] = v > R(0) ? v : R(0);
-    if (ix <= g.nx && iy <= g.ny && iz <= g.nz) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) g.nv[k][c] = R(2) * up[k + 3][0] - up[k][0];
+        for (int k = 0; k < 3; ++k) g.nv[k][c] = R(2) * Vs[su][k + 3][e] - Vs[su][k][e];
+      }
     }
     a1 = a5;
     a2 = a6;
@@ -742,10 +760,7 @@ __global__ void __launch_bounds__(128) k_shock_march(ShockArgs<R> g) {
     al1y = al1yz;
     al2 = al2z;
     al2x = al2xz;
-#pragma unroll
-    for (int k = 0; k < 6; ++k)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) lo[k][q] = up[k][q];
+    __syncthreads();
   }
 }
 
@@ -882,10 +897,10 @@ void predictor_corrector_step(Run<R>& run) {
     ga.nz = nz;
     ga.sx = sx;
     ga.sxy = sxy;
-    dim3 blk(32, 4, 1);
-    dim3 grd((nx + 2 + 31) / 32, (ny + 2 + 3) / 4, (nz + 2 + kShockZ - 1) / kShockZ);
+    dim3 blk(kShX, kShY, 1);
+    dim3 grd((nx + 2 + kShX - 1) / kShX, (ny + 2 + kShY - 1) / kShY, (nz + 2 + kShockZ - 1) / kShockZ);
     const int k = run.prof_begin("shock_heating", 0, 14, (double)(nx + 2) * (ny + 2) * (nz + 2));
-    k_shock_march<R><<<grd, blk, 0, run.s>>>(ga);
+    k_shock_tile<R><<<grd, blk, 0, run.s>>>(ga);
     run.prof_end(k);
     ++run.launches;
   }
@@ -904,7 +919,7 @@ void predictor_corrector_step(Run<R>& run) {
   R* const rhow = A.rho.p;
   R* const visc_dep = A.visc_dep.p;
   const A1<R> rbx = A.rdb[0], rby = A.rdb[1], rbz = A.rdb[2];
-  box_sum<1>(run, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
+  box_sum<1>(run, "corrector_visc_heating_sum", 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz, double* v) {
     const R dt = (R)sc[SC_DT];
     const int c = ix + sx * iy + sxy * iz;
     const int X = 1, Y = sx, Z = sxy;
