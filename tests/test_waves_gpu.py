@@ -1,0 +1,47 @@
+"""The linear sound, Alfven and fast waves of tests/test_waves_cpu.py through
+the three GPU engines, along each axis: the exact engine bit for bit with
+the oracle, the FP64 product engine within 1e-10 of it (relative L2 of
+every state field, the perturbation-only ones included), and each engine's
+wave at its analytic speed within 0.1 % (0.2 % in FP32, whose rounding is
+6e-8 of the background against a perturbation of 1e-4).  Shapes of
+64 x 4 x 4 and its rotations exercise the kernels' partial tiles and chunks
+on every axis."""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import STATE, rel_l2
+from test_waves_cpu import EPS, measured_mode, run_to_end, wave_deck
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("kind", ["sound", "alfven", "fast"])
+@pytest.mark.parametrize("axis", [0, 1, 2], ids=["x", "y", "z"])
+def test_wave_through_engines(built, kind, axis):
+    from lare3d_b200 import gpu
+    from oracle import oracle
+    d, speed, probe, base = wave_deck(kind, axis)
+    r = oracle.simulation(d)
+    r.start(d.state)
+    t_ref = run_to_end(r)
+    for precision, tol in ((gpu.EXACT64, 0.0), (gpu.FP64, 1e-10), (gpu.FP32, None)):
+        d, _, _, _ = wave_deck(kind, axis)
+        g = gpu.simulation(d, precision=precision)
+        g.start(d.state)
+        t = run_to_end(g)
+        assert abs(t - t_ref) <= (1e-12 if precision != gpu.FP32 else 1e-5) * t_ref
+        for f in STATE if tol is not None else ():
+            a, b = g.get_field(f), r.get_field(f)
+            if tol == 0.0:
+                assert np.array_equal(a, b), f"{kind} {axis} {f}: exact engine differs from the oracle"
+            else:
+                err = rel_l2(a, b)
+                assert err <= tol, (kind, axis, precision, f, err)
+        phi, amp = measured_mode(g, d, axis, probe, base)
+        bar = 1e-3 if precision != gpu.FP32 else 2e-3
+        assert abs(phi / (2.0 * math.pi * t) / speed - 1.0) < bar, (precision, phi, t, speed)
+        lo = 0.99 if precision != gpu.FP32 else 0.98
+        assert lo * EPS < amp <= 1.001 * EPS, (precision, amp)
+        g.close()
