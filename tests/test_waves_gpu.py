@@ -45,3 +45,41 @@ def test_wave_through_engines(built, kind, axis):
         lo = 0.99 if precision != gpu.FP32 else 0.98
         assert lo * EPS < amp <= 1.001 * EPS, (precision, amp)
         g.close()
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2], ids=["x", "y", "z"])
+def test_diffusion_through_engines(built, axis):
+    """The resistive and conductive modes of tests/test_diffusion_cpu.py: the
+    exact engine bit for bit with the oracle, the product engine within
+    1e-10 and at the analytic decay rate within 0.2 %."""
+    from lare3d_b200 import gpu
+    from oracle import oracle
+    from test_diffusion_cpu import DT_COND, EPS as E, GAMMA, T0, conduction_deck, mode, resistive_deck, run_resistive
+    for case in ("resistive", "conduction"):
+        d, lam = (resistive_deck(axis)[:2] if case == "resistive" else conduction_deck(axis))
+        r = oracle.simulation(d)
+        r.start(d.state)
+        if case == "resistive":
+            run_resistive(r)
+        else:
+            r.conduct_heat(DT_COND)
+        for precision, tol in ((gpu.EXACT64, 0.0), (gpu.FP64, 1e-10)):
+            d = (resistive_deck(axis)[0] if case == "resistive" else conduction_deck(axis)[0])
+            g = gpu.simulation(d, precision=precision)
+            g.start(d.state)
+            if case == "resistive":
+                t = run_resistive(g)
+                name, base, a0 = "bx by bz".split()[(axis + 1) % 3], 0.0, E
+            else:
+                g.conduct_heat(DT_COND)
+                t = DT_COND
+                name, base, a0 = "energy", 2.0 * T0 / (GAMMA - 1.0), 2.0 * T0 * E / (GAMMA - 1.0)
+            for f in STATE:
+                a, b = g.get_field(f), r.get_field(f)
+                if tol == 0.0:
+                    assert np.array_equal(a, b), f"{case} {axis} {f}: exact engine differs from the oracle"
+                else:
+                    assert rel_l2(a, b) <= tol, (case, axis, f, rel_l2(a, b))
+            _, amp = mode(g, d, axis, name, base)
+            assert abs(-math.log(amp / a0) / t / lam - 1.0) < 2e-3, (case, precision)
+            g.close()
