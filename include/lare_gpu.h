@@ -53,7 +53,7 @@ extern "C" {
 #define LARE_ESTAGES (-5)    /* RKL2 stage count not representable */
 #define LARE_ENOTFOUND (-6)  /* unknown field name */
 #define LARE_ENONFINITE (-7) /* non-finite value in uploaded state */
-#define LARE_ETOOLARGE (-8)  /* grid beyond a fixed-capacity entry point's limit */
+#define LARE_ETOOLARGE (-8)  /* grid beyond 32-bit indexing or a fixed-capacity entry point's limit */
 #define LARE_EEOS (-9)       /* neutral_fraction's temperature bracket is empty (neutral.f90:171-174) */
 
 /* Precision codes of lare_gpu_init. */
@@ -164,6 +164,11 @@ typedef struct lare_ctx lare_ctx;
  *                         (conduction's pow excepted); slower;
  *   LARE_FP32 (32)        the FP32 form: field arithmetic in FP32, dt
  *                         reduction, budgets and RKL2 coefficients in FP64.
+ * Device indices are 32-bit: the padded box of an array, (nx + 5 rounded up
+ * to a multiple of 4) * (ny + 5) * (nz + 5) points, must stay below 2^31,
+ * else LARE_ETOOLARGE before the device is touched (a cube up to 1284^3;
+ * such a grid needs about 50 arrays of 8 or 4 bytes a point, far beyond
+ * one GPU's memory, which returns LARE_ENOMEM first).
  * Replaces mpi_initialise's allocation (mpi_routines.F90:295-334) for the
  * device copy.
  */

@@ -57,6 +57,8 @@ int lare_gpu_init(const lare_params* p, int nx, int ny, int nz, const double* dx
     return LARE_EINVAL;  // the ionisation model's constants must be set
   if (p->radiation && !(p->temp_norm > 0.0 && p->time_norm > 0.0 && p->rho_norm > 0.0 && p->mf > 0.0))
     return LARE_EINVAL;  // radiative losses need the normalisation
+  // every device index is 32-bit: the padded box must stay below 2^31 points
+  if (((long long)nx + 5 + 3) / 4 * 4 * (ny + 5LL) * (nz + 5LL) >= (1LL << 31)) return LARE_ETOOLARGE;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return LARE_ECUDA;
   const double* m6[6] = {dxb, dxc, dyb, dyc, dzb, dzc};

@@ -96,6 +96,11 @@ def test_host_side_argument_checks(built):
     assert lib.lare_gpu_init(C.byref(p), 8, 8, 8, *ptr, 64, C.byref(out)) == -1
     p = default_params(xbc_min=3)
     assert lib.lare_gpu_init(C.byref(p), 8, 8, 8, *ptr, 64, C.byref(out)) == -1
+    # grids whose padded box reaches 2^31 points (32-bit device indices) are
+    # refused before the device or the metrics are touched: the smallest
+    # such cube, and a thin grid
+    assert lib.lare_gpu_init(C.byref(d.params), 1285, 1285, 1285, *ptr, 64, C.byref(out)) == -8
+    assert lib.lare_gpu_init(C.byref(d.params), 4, 4, 20000000, *ptr, 32, C.byref(out)) == -8
     assert not out.value
     # calls on a null context fail cleanly
     lib.lare_gpu_eta_calc.restype = C.c_int

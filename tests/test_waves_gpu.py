@@ -1,8 +1,10 @@
 """The linear sound, Alfven and fast waves of tests/test_waves_cpu.py through
 the three GPU engines, along each axis: the exact engine bit for bit with
-the oracle, the FP64 product engine within 1e-10 of it (relative L2 of
-every state field, the perturbation-only ones included), and each engine's
-wave at its analytic speed within 0.1 % (0.2 % in FP32, whose rounding is
+the oracle, the FP64 product engine within 1e-10 of it (L2 norm of the
+difference of every state field over that of the field or, for fields that
+carry only the perturbation or its second-order flows, of a field of the
+perturbation's amplitude), and each engine's wave at its analytic speed
+within 0.1 % (0.2 % and an amplitude within 0.5 % in FP32, whose rounding is
 6e-8 of the background against a perturbation of 1e-4).  Shapes of
 64 x 4 x 4 and its rotations exercise the kernels' partial tiles and chunks
 on every axis."""
@@ -11,10 +13,17 @@ import math
 import numpy as np
 import pytest
 
-from conftest import STATE, rel_l2
+from conftest import STATE
 from test_waves_cpu import EPS, measured_mode, run_to_end, wave_deck
 
 pytestmark = pytest.mark.gpu
+
+
+def scaled_l2(a, b):
+    """||a - b|| over max(||b||, ||EPS||): relative for the background
+    fields, relative to the perturbation's scale for the perturbation-only
+    ones (whose second-order parts are round-off-sized in relative terms)."""
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), EPS * math.sqrt(b.size)))
 
 
 @pytest.mark.parametrize("kind", ["sound", "alfven", "fast"])
@@ -37,13 +46,13 @@ def test_wave_through_engines(built, kind, axis):
             if tol == 0.0:
                 assert np.array_equal(a, b), f"{kind} {axis} {f}: exact engine differs from the oracle"
             else:
-                err = rel_l2(a, b)
+                err = scaled_l2(a, b)
                 assert err <= tol, (kind, axis, precision, f, err)
         phi, amp = measured_mode(g, d, axis, probe, base)
         bar = 1e-3 if precision != gpu.FP32 else 2e-3
         assert abs(phi / (2.0 * math.pi * t) / speed - 1.0) < bar, (precision, phi, t, speed)
-        lo = 0.99 if precision != gpu.FP32 else 0.98
-        assert lo * EPS < amp <= 1.001 * EPS, (precision, amp)
+        lo, hi = (0.99, 1.001) if precision != gpu.FP32 else (0.98, 1.005)
+        assert lo * EPS < amp <= hi * EPS, (precision, amp)
         g.close()
 
 
@@ -79,7 +88,7 @@ def test_diffusion_through_engines(built, axis):
                 if tol == 0.0:
                     assert np.array_equal(a, b), f"{case} {axis} {f}: exact engine differs from the oracle"
                 else:
-                    assert rel_l2(a, b) <= tol, (case, axis, f, rel_l2(a, b))
+                    assert scaled_l2(a, b) <= tol, (case, axis, f, scaled_l2(a, b))
             _, amp = mode(g, d, axis, name, base)
             assert abs(-math.log(amp / a0) / t / lam - 1.0) < 2e-3, (case, precision)
             g.close()
