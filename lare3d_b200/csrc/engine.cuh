@@ -747,48 +747,23 @@ template <class R>
 void eulerian_remap(Run<R>& run, int step) {
   const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
   const int sx = run.sx, sxy = run.sxy;
-  R* const bx = run.a.bx.p;
-  R* const by = run.a.by.p;
-  R* const bz = run.a.bz.p;
-  auto dxb = run.a.dxb, dyb = run.a.dyb, dzb = run.a.dzb;
   int pass[3] = {1, 1, 1};
   if (run.p.rke) {  // remap.f90:38
     R* const dke = run.a.delta_ke.p;
     LARE_BOXW(run, 1, 1, nx, 1, ny, 1, nz, [=] __device__(int ix, int iy, int iz) { dke[ix + sx * iy + sxy * iz] = R(0); });
   }
-  // B -> flux (remap.f90:43-69), including the -2 layers.
-  LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
-    const int c = ix + sx * iy + sxy * iz;
-    // all loads before any store (the three arrays are distinct)
-    const bool ox = iy >= -1 && iz >= -1, oy = ix >= -1 && iz >= -1, oz = ix >= -1 && iy >= -1;
-    const R x = ox ? bx[c] : R(0), y = oy ? by[c] : R(0), z = oz ? bz[c] : R(0);
-    if (ox) bx[c] = x * dyb(iy) * dzb(iz);
-    if (oy) by[c] = y * dxb(ix) * dzb(iz);
-    if (oz) bz[c] = z * dxb(ix) * dyb(iy);
-  });
+  // B -> flux form (remap.f90:43-69) and back (:101-127) are done by the
+  // first and last sweeps' B kernels on the way (remap_sweep's bmode).
   static const int order[6][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}, {0, 2, 1}, {2, 1, 0}, {1, 0, 2}};
   int cse = ((step % 6) + 6) % 6;
   for (int s = 0; s < 3; ++s) {
+    const int bmode = s == 0 ? 1 : (s == 2 ? 2 : 0);
     switch (order[cse][s]) {
-      case 0: remap_sweep<0>(run, false, SC_DT, pass); break;
-      case 1: remap_sweep<1>(run, false, SC_DT, pass); break;
-      default: remap_sweep<2>(run, false, SC_DT, pass); break;
+      case 0: remap_sweep<0>(run, false, SC_DT, pass, bmode); break;
+      case 1: remap_sweep<1>(run, false, SC_DT, pass, bmode); break;
+      default: remap_sweep<2>(run, false, SC_DT, pass, bmode); break;
     }
   }
-  // flux -> B (remap.f90:101-127); the sweeps swap buffers, so re-read.
-  R* const qx = run.a.bx.p;
-  R* const qy = run.a.by.p;
-  R* const qz = run.a.bz.p;
-  const auto rbx = run.a.rdb[0], rby = run.a.rdb[1], rbz = run.a.rdb[2];
-  LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
-    const int c = ix + sx * iy + sxy * iz;
-    // all loads before any store (the three arrays are distinct)
-    const bool ox = iy >= -1 && iz >= -1, oy = ix >= -1 && iz >= -1, oz = ix >= -1 && iy >= -1;
-    const R x = ox ? qx[c] : R(0), y = oy ? qy[c] : R(0), z = oz ? qz[c] : R(0);
-    if (ox) qx[c] = div_rcp(div_rcp(x, dyb(iy), rby(iy)), dzb(iz), rbz(iz));
-    if (oy) qy[c] = div_rcp(div_rcp(y, dxb(ix), rbx(ix)), dzb(iz), rbz(iz));
-    if (oz) qz[c] = div_rcp(div_rcp(z, dxb(ix), rbx(ix)), dyb(iy), rby(iy));
-  });
   bfield_bcs(run);
 }
 

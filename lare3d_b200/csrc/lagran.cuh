@@ -573,28 +573,10 @@ void set_dt(Run<R>& run) {
 // run.a.bx holds the predicted B and run.a.bx0 the untouched B of the step.
 template <class R>
 void predictor_remap(Run<R>& run, int step) {
-  const int nx = run.n[0], ny = run.n[1], nz = run.n[2];
-  const int sx = run.sx, sxy = run.sxy;
   Arrays<R>& A = run.a;
-  const R* bx = A.bx.p;
-  const R* by = A.by.p;
-  const R* bz = A.bz.p;
-  R* const px = A.bx0.p;
-  R* const py = A.by0.p;
-  R* const pz = A.bz0.p;
-  auto dxb = A.dxb, dyb = A.dyb, dzb = A.dzb;
-  LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
-    const int c = ix + sx * iy + sxy * iz;
-    // all loads before any store
-    const bool ox = iy >= -1 && iz >= -1, oy = ix >= -1 && iz >= -1, oz = ix >= -1 && iy >= -1;
-    const R x = ox ? bx[c] : R(0), y = oy ? by[c] : R(0), z = oz ? bz[c] : R(0);
-    if (ox) px[c] = x * dyb(iy) * dzb(iz);
-    if (oy) py[c] = y * dxb(ix) * dzb(iz);
-    if (oz) pz[c] = z * dxb(ix) * dyb(iy);
-  });
-  std::swap(A.bx.p, A.bx0.p);
-  std::swap(A.by.p, A.by0.p);
-  std::swap(A.bz.p, A.bz0.p);
+  // B -> flux form (remap.f90:43-69, into the B0 buffers, which are then
+  // swapped in so that B itself is kept as B0) and back (:101-127) are done
+  // by the first and last sweeps' B kernels on the way (remap_sweep's bmode).
   // vx1 = vx (lagran.F90:1051-1053): the sweeps read v itself.  vx1's own
   // nodes 0:n are rewritten by the predictor force and its ghosts by
   // remap_v_bcs, except on an open side: there the copy's ghost values are
@@ -611,28 +593,16 @@ void predictor_remap(Run<R>& run, int step) {
   int cse = ((step % 6) + 6) % 6;
   int pass[3] = {1, 1, 1};
   for (int s = 0; s < 3; ++s) {
+    const int bmode = s == 0 ? 1 : (s == 2 ? 2 : 0);
     switch (order[cse][s]) {
-      case 0: remap_sweep<0>(run, true, SC_DT2, pass); break;
-      case 1: remap_sweep<1>(run, true, SC_DT2, pass); break;
-      default: remap_sweep<2>(run, true, SC_DT2, pass); break;
+      case 0: remap_sweep<0>(run, true, SC_DT2, pass, bmode); break;
+      case 1: remap_sweep<1>(run, true, SC_DT2, pass, bmode); break;
+      default: remap_sweep<2>(run, true, SC_DT2, pass, bmode); break;
     }
   }
   A.vx1.p = keep[0];
   A.vy1.p = keep[1];
   A.vz1.p = keep[2];
-  R* const qx = A.bx.p;
-  R* const qy = A.by.p;
-  R* const qz = A.bz.p;
-  const auto rbx = run.a.rdb[0], rby = run.a.rdb[1], rbz = run.a.rdb[2];
-  LARE_BOXWH(run, 0, 4, 6, -2, nx + 2, -2, ny + 2, -2, nz + 2, [=] __device__(int ix, int iy, int iz) {
-    const int c = ix + sx * iy + sxy * iz;
-    // all loads before any store (the three arrays are distinct)
-    const bool ox = iy >= -1 && iz >= -1, oy = ix >= -1 && iz >= -1, oz = ix >= -1 && iy >= -1;
-    const R x = ox ? qx[c] : R(0), y = oy ? qy[c] : R(0), z = oz ? qz[c] : R(0);
-    if (ox) qx[c] = div_rcp(div_rcp(x, dyb(iy), rby(iy)), dzb(iz), rbz(iz));
-    if (oy) qy[c] = div_rcp(div_rcp(y, dxb(ix), rbx(ix)), dzb(iz), rbz(iz));
-    if (oz) qz[c] = div_rcp(div_rcp(z, dxb(ix), rbx(ix)), dyb(iy), rby(iy));
-  });
   bfield_bcs(run);
 }
 

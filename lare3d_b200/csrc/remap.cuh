@@ -67,16 +67,70 @@ struct BfArgs {
   int SX, SY;                  // strides of the thread grid's two axes (x and the other transverse axis)
   int na;                      // cells along A
   int n0, n1;                  // extents of the thread grid (-1..n+1 each)
+  // for the first sweep of a remap, which reads B itself and forms its
+  // flux form on the fly: the metrics, the components' axes, the sweep axis
+  A1<R> dbm[3];
+  int j1, j2, ax;
 };
+
+// remap.f90:43-69 on one value: B component j at (ix, iy, iz) times the
+// widths of its face along the other two axes, in axis order, where the
+// reference converts (its B arrays start at -1 on the other axes).
+template <class R>
+__device__ __forceinline__ R to_flux(R b, int j, int ix, int iy, int iz, const A1<R> (&m)[3]) {
+  if (j == 0) return (iy >= -1 && iz >= -1) ? b * m[1](iy) * m[2](iz) : b;
+  if (j == 1) return (ix >= -1 && iz >= -1) ? b * m[0](ix) * m[2](iz) : b;
+  return (ix >= -1 && iy >= -1) ? b * m[0](ix) * m[1](iy) : b;
+}
+// remap.f90:101-127 on one value: the flux form back to B.
+template <class R>
+__device__ __forceinline__ R from_flux(R b, int j, int ix, int iy, int iz, const A1<R> (&m)[3],
+                                       const A1<R> (&r)[3]) {
+  if (j == 0) return (iy >= -1 && iz >= -1) ? div_rcp(div_rcp(b, m[1](iy), r[1](iy)), m[2](iz), r[2](iz)) : b;
+  if (j == 1) return (ix >= -1 && iz >= -1) ? div_rcp(div_rcp(b, m[0](ix), r[0](ix)), m[2](iz), r[2](iz)) : b;
+  return (ix >= -1 && iy >= -1) ? div_rcp(div_rcp(b, m[0](ix), r[0](ix)), m[1](iy), r[1](iy)) : b;
+}
+
+// to_flux along a y/z-sweep march line (the first sweep of a remap): the
+// line's points have every coordinate >= -1, so the reference converts them
+// all; of component j's two face widths, the one across the line (axis c =
+// 3 - j - A, at the thread's x or second grid coordinate) is fixed and is
+// formed once, the one along the sweep axis is loaded per point and shared
+// by both components; they multiply in axis order as in remap.f90:43-69.
+template <class R>
+struct LineConv {
+  const R* mA;  // widths along the sweep axis
+  R cf1, cf2;   // the fixed widths of the two components
+  bool af1, af2;  // the sweep axis comes first
+};
+template <class R>
+__device__ __forceinline__ LineConv<R> line_conv(const BfArgs<R>& a, int x, int g2) {
+  LineConv<R> L;
+  L.mA = a.ax == 1 ? a.dbm[1].p : a.dbm[2].p;
+  const int ay = 3 - a.ax;  // the grid's second axis: z for the y sweep, y for the z sweep
+  auto fixed = [&](int j) {
+    const int c = 3 - j - a.ax;
+    return c == 0 ? a.dbm[0](x) : (ay == 1 ? a.dbm[1](g2) : a.dbm[2](g2));
+  };
+  L.cf1 = fixed(a.j1);
+  L.cf2 = fixed(a.j2);
+  L.af1 = a.ax < 3 - a.j1 - a.ax;
+  L.af2 = a.ax < 3 - a.j2 - a.ax;
+  return L;
+}
+template <class R>
+__device__ __forceinline__ R line_form(R b, R ma, R cf, bool afirst) {
+  return afirst ? b * ma * cf : b * cf * ma;
+}
 
 // B / dbv at q, with dbv (in the carried divisor form dv_of) returned in dvb
 template <class R>
-__device__ __forceinline__ R bf_quot(const R* Bb, const R* db1, int q, int SB, R& dvb) {
+__device__ __forceinline__ R bf_quot(R b, const R* db1, int q, int SB, R& dvb) {
   dvb = dv_of((db1[q] + db1[q + SB]) * R(0.5));
-  return dv_div(Bb[q], dvb);
+  return dv_div(b, dvb);
 }
 
-template <class R>
+template <class R, bool PRE>
 __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
   const int t1 = blockIdx.y * blockDim.y + threadIdx.y;
@@ -91,18 +145,30 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
   R q1m, q10, q1p, q1p2, d1m, d10, d1p, d1p2;  // flux 1: quotients, dbv
   R q2m, q20, q2p, q2p2, d2m, d20, d2p, d2p2;  // flux 2
   R dcm, dc0, dcp, dbc0, dbcp;                 // dc1 at cm, c, cp; db1 at c, cp
+  const int gx = t0 - 1, g2 = t1 - 1;  // the thread grid's coordinates
+  LineConv<R> lc{};
+  if constexpr (PRE) lc = line_conv(a, gx, g2);
   {
-    const int cm = ia0 > -1 ? c - SA : c;
+    const int am = ia0 > -1 ? ia0 - 1 : ia0, ap2 = ia0 + 2 <= a.na + 2 ? ia0 + 2 : ia0 + 1;
+    const int cm = c + (am - ia0) * SA;
     const int cp = c + SA;
-    const int cp2 = ia0 + 2 <= a.na + 2 ? c + 2 * SA : cp;
-    q1m = bf_quot(a.b1, a.db1, cm, a.SB1, d1m);
-    q10 = bf_quot(a.b1, a.db1, c, a.SB1, d10);
-    q1p = bf_quot(a.b1, a.db1, cp, a.SB1, d1p);
-    q1p2 = bf_quot(a.b1, a.db1, cp2, a.SB1, d1p2);
-    q2m = bf_quot(a.b2, a.db1, cm, a.SB2, d2m);
-    q20 = bf_quot(a.b2, a.db1, c, a.SB2, d20);
-    q2p = bf_quot(a.b2, a.db1, cp, a.SB2, d2p);
-    q2p2 = bf_quot(a.b2, a.db1, cp2, a.SB2, d2p2);
+    const int cp2 = c + (ap2 - ia0) * SA;
+    auto b1 = [&](int q, int ia) {
+      if constexpr (PRE) return line_form(a.b1[q], lc.mA[ia], lc.cf1, lc.af1);
+      return a.b1[q];
+    };
+    auto b2 = [&](int q, int ia) {
+      if constexpr (PRE) return line_form(a.b2[q], lc.mA[ia], lc.cf2, lc.af2);
+      return a.b2[q];
+    };
+    q1m = bf_quot(b1(cm, am), a.db1, cm, a.SB1, d1m);
+    q10 = bf_quot(b1(c, ia0), a.db1, c, a.SB1, d10);
+    q1p = bf_quot(b1(cp, ia0 + 1), a.db1, cp, a.SB1, d1p);
+    q1p2 = bf_quot(b1(cp2, ap2), a.db1, cp2, a.SB1, d1p2);
+    q2m = bf_quot(b2(cm, am), a.db1, cm, a.SB2, d2m);
+    q20 = bf_quot(b2(c, ia0), a.db1, c, a.SB2, d20);
+    q2p = bf_quot(b2(cp, ia0 + 1), a.db1, cp, a.SB2, d2p);
+    q2p2 = bf_quot(b2(cp2, ap2), a.db1, cp2, a.SB2, d2p2);
     dcm = dv_of(a.dc1[cm]);
     dc0 = dv_of(a.dc1[c]);
     dcp = dv_of(a.dc1[cp]);
@@ -124,6 +190,11 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
     if (fetch) {
       nb1 = a.b1[qn];
       nb2 = a.b2[qn];
+      if constexpr (PRE) {
+        const R ma = lc.mA[ia + 3];
+        nb1 = line_form(nb1, ma, lc.cf1, lc.af1);
+        nb2 = line_form(nb2, ma, lc.cf2, lc.af2);
+      }
       nd = a.db1[qn];
       nd1 = a.db1[qn + a.SB1];
       nd2 = a.db1[qn + a.SB2];
@@ -179,17 +250,23 @@ __global__ void __launch_bounds__(256, 2) k_bflux_march(BfArgs<R> a) {
 // few spills (measured at 256^3).
 constexpr int kXOut = 29;
 
-template <class R>
+template <class R, bool PRE>
 __global__ void __launch_bounds__(128, 10) k_bflux_x(BfArgs<R> a, int sx, int sxy, int nx, int ny) {
   const int lane = (int)threadIdx.x;                           // blockDim.x == 32: one warp per row
   const int ix = -2 + (int)blockIdx.x * kXOut + lane;          // this lane's x position
   const int iy = -1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
   const int iz = -1 + (int)blockIdx.z;
   if (iy > ny + 1) return;                                      // uniform over the warp
-  const int c = min(ix, nx + 2) + sx * iy + sxy * iz;           // positions past n+2 load n+2 (unused)
+  const int cx = min(ix, nx + 2);
+  const int c = cx + sx * iy + sxy * iz;                        // positions past n+2 load n+2 (unused)
   R d1, d2;
-  const R q1 = bf_quot(a.b1, a.db1, c, a.SB1, d1);
-  const R q2 = bf_quot(a.b2, a.db1, c, a.SB2, d2);
+  R bv1 = a.b1[c], bv2 = a.b2[c];
+  if constexpr (PRE) {  // the first sweep of a remap reads B itself (by and bz)
+    bv1 = to_flux(bv1, 1, cx, iy, iz, a.dbm);
+    bv2 = to_flux(bv2, 2, cx, iy, iz, a.dbm);
+  }
+  const R q1 = bf_quot(bv1, a.db1, c, a.SB1, d1);
+  const R q2 = bf_quot(bv2, a.db1, c, a.SB2, d2);
   const R dc = dv_of(a.dc1[c]), db = a.db1[c];
   const unsigned all = 0xffffffffu;
   const R q1m = __shfl_up_sync(all, q1, 1), q1p = __shfl_down_sync(all, q1, 1), q1p2 = __shfl_down_sync(all, q1, 2);
@@ -220,7 +297,7 @@ __global__ void __launch_bounds__(128, 10) k_bflux_x(BfArgs<R> a, int sx, int sx
 // (even: first, odd: second) and the chunk, so a thread carries one
 // four-point window instead of two; twice the threads, about half the
 // registers each.
-template <class R>
+template <class R, bool PRE>
 __global__ void __launch_bounds__(128) k_bflux_march1(BfArgs<R> a) {
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
   const int t1 = blockIdx.y * blockDim.y + threadIdx.y;
@@ -233,18 +310,33 @@ __global__ void __launch_bounds__(128) k_bflux_march1(BfArgs<R> a) {
   const int SB = second ? a.SB2 : a.SB1;
   const int SO = second ? a.SO2 : a.SO1;
   R* const fo = second ? a.f2 : a.f1;
-  int c = (t0 - 1) * a.SX + (t1 - 1) * a.SY + ia0 * SA;
+  const int gx = t0 - 1, g2 = t1 - 1;  // the thread grid's coordinates
+  R cf = R(0);
+  bool af = false;
+  const R* mA = nullptr;
+  if constexpr (PRE) {
+    const LineConv<R> lc = line_conv(a, gx, g2);
+    cf = second ? lc.cf2 : lc.cf1;
+    af = second ? lc.af2 : lc.af1;
+    mA = lc.mA;
+  }
+  int c = gx * a.SX + g2 * a.SY + ia0 * SA;
   const R dt = (R)a.sc[a.dt_slot];
   R qm, q0, qp, qp2, dm, d0, dp, dp2;  // quotients and dbv at cm, c, cp, cp2
   R dcm, dc0, dcp, dbc0, dbcp;
   {
-    const int cm = ia0 > -1 ? c - SA : c;
+    const int am = ia0 > -1 ? ia0 - 1 : ia0, ap2 = ia0 + 2 <= a.na + 2 ? ia0 + 2 : ia0 + 1;
+    const int cm = c + (am - ia0) * SA;
     const int cp = c + SA;
-    const int cp2 = ia0 + 2 <= a.na + 2 ? c + 2 * SA : cp;
-    qm = bf_quot(B, a.db1, cm, SB, dm);
-    q0 = bf_quot(B, a.db1, c, SB, d0);
-    qp = bf_quot(B, a.db1, cp, SB, dp);
-    qp2 = bf_quot(B, a.db1, cp2, SB, dp2);
+    const int cp2 = c + (ap2 - ia0) * SA;
+    auto b = [&](int q, int ia) {
+      if constexpr (PRE) return line_form(B[q], mA[ia], cf, af);
+      return B[q];
+    };
+    qm = bf_quot(b(cm, am), a.db1, cm, SB, dm);
+    q0 = bf_quot(b(c, ia0), a.db1, c, SB, d0);
+    qp = bf_quot(b(cp, ia0 + 1), a.db1, cp, SB, dp);
+    qp2 = bf_quot(b(cp2, ap2), a.db1, cp2, SB, dp2);
     dcm = dv_of(a.dc1[cm]);
     dc0 = dv_of(a.dc1[c]);
     dcp = dv_of(a.dc1[cp]);
@@ -262,6 +354,7 @@ __global__ void __launch_bounds__(128) k_bflux_march1(BfArgs<R> a) {
     R nb = R(0), nd = R(0), nds = R(0), ndc = R(0), ndb = R(0), nva = R(0), nvo = R(0);
     if (fetch) {
       nb = B[qn];
+      if constexpr (PRE) nb = line_form(nb, mA[ia + 3], cf, af);
       nd = a.db1[qn];
       nds = a.db1[qn + SB];
     }
@@ -809,47 +902,70 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? 4 : 8) k_mom_march(MomAr
 // itself), so each thread keeps several independent loads in flight; the
 // FP32 form, 4 bytes a word, is otherwise latency-bound well below HBM
 // speed.  Same expressions and predicates as the per-point form.
+//
+// MODE 0, a middle sweep: the update in place over the box 0..n+1.
+// MODE 1, the first sweep of a remap: B is read as stored, put in flux form
+// (remap.f90:43-69) and updated over 0..n+1; every point of the arrays' box
+// -2..n+2 is written, to the output arrays (the predictor's B0 buffers,
+// whose B is kept, or B itself).  MODE 2, the last sweep: updated over
+// 0..n+1, then every point of -2..n+2 is put back from flux form
+// (remap.f90:101-127).  The conversions are the reference's expressions on
+// the same operands, so the result equals converting in separate passes.
 template <class R>
 struct BUpdArgs {
   const R* f1;
   const R* f2;
-  R* Ba;
-  R* Bb1;
+  R* Ba;   // B along the sweep axis
+  R* Bb1;  // the two transported components
   R* Bb2;
+  R* oa;   // where MODE 1 writes them
+  R* ob1;
+  R* ob2;
+  A1<R> dbm[3], rdbm[3];
   int nx, ny, nz, sx, sxy, SA, SB1, SB2;
 };
 
-template <int A, int PTS, class R>
+template <int A, int PTS, int MODE, class R>
 __global__ void __launch_bounds__(128) k_bupdate(BUpdArgs<R> g) {
-  const int ix = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  const int iy = (int)(blockIdx.y * blockDim.y + threadIdx.y);
-  if (ix > g.nx + 1 || iy > g.ny + 1) return;
-  const int z0 = (int)blockIdx.z * PTS;
+  constexpr int JA = A, J1 = A == 0 ? 1 : 0, J2 = A == 2 ? 1 : 2;  // the components' axes
+  constexpr int LO = MODE == 0 ? 0 : -2, EXT = MODE == 0 ? 1 : 2;   // the box LO..n+EXT
+  const int ix = LO + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int iy = LO + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  if (ix > g.nx + EXT || iy > g.ny + EXT) return;
+  const int z0 = LO + (int)blockIdx.z * PTS;
+  const bool in_xy = ix >= 0 && ix <= g.nx + 1 && iy >= 0 && iy <= g.ny + 1;
   R b1[PTS], f1c[PTS], f1a[PTS], ba[PTS], f1b[PTS], b2[PTS], f2c[PTS], f2a[PTS], f2b[PTS];
-  bool ok[PTS];
+  bool ok[PTS], in[PTS];
 #pragma unroll
   for (int p = 0; p < PTS; ++p) {
     const int iz = z0 + p;
-    ok[p] = iz <= g.nz + 1;
+    ok[p] = iz <= g.nz + EXT;
+    in[p] = in_xy && iz >= 0 && iz <= g.nz + 1;  // the update box
     const int c = ix + g.sx * iy + g.sxy * (ok[p] ? iz : z0);
     b1[p] = g.Bb1[c];
-    f1c[p] = g.f1[c];
-    f1a[p] = g.f1[c - g.SA];
     ba[p] = g.Ba[c];
-    f1b[p] = g.f1[c - g.SB1];
     b2[p] = g.Bb2[c];
-    f2c[p] = g.f2[c];
-    f2a[p] = g.f2[c - g.SA];
-    f2b[p] = g.f2[c - g.SB2];
+    f1c[p] = f1a[p] = f1b[p] = f2c[p] = f2a[p] = f2b[p] = R(0);
+    if (in[p]) {
+      f1c[p] = g.f1[c];
+      f1a[p] = g.f1[c - g.SA];
+      f1b[p] = g.f1[c - g.SB1];
+      f2c[p] = g.f2[c];
+      f2a[p] = g.f2[c - g.SA];
+      f2b[p] = g.f2[c - g.SB2];
+    }
   }
 #pragma unroll
   for (int p = 0; p < PTS; ++p) {
     if (!ok[p]) continue;
     const int iz = z0 + p;
     const int c = ix + g.sx * iy + g.sxy * iz;
-    // first flux: b1 over 0:n+1 all, a-component over 0:n+1 all
-    g.Bb1[c] = b1[p] - f1c[p] + f1a[p];
-    R b = ba[p] + f1c[p] - f1b[p];
+    R v1 = b1[p], va = ba[p], v2 = b2[p];
+    if constexpr (MODE == 1) {
+      v1 = to_flux(v1, J1, ix, iy, iz, g.dbm);
+      va = to_flux(va, JA, ix, iy, iz, g.dbm);
+      v2 = to_flux(v2, J2, ix, iy, iz, g.dbm);
+    }
     // second flux ranges (xremap.f90:141-157; yremap.f90:142-158)
     bool r2a = true, r2b = true;
     if (A == 0) {
@@ -858,9 +974,28 @@ __global__ void __launch_bounds__(128) k_bupdate(BUpdArgs<R> g) {
     } else if (A == 1) {
       r2b = ix >= 1 && ix <= g.nx && iy <= g.ny && iz >= 1 && iz <= g.nz;
     }
-    if (r2a) g.Bb2[c] = b2[p] - f2c[p] + f2a[p];
-    if (r2b) b = b + f2c[p] - f2b[p];
-    g.Ba[c] = b;
+    if (in[p]) {
+      // first flux: b1 over 0:n+1 all, a-component over 0:n+1 all
+      v1 = v1 - f1c[p] + f1a[p];
+      R b = va + f1c[p] - f1b[p];
+      if (r2a) v2 = v2 - f2c[p] + f2a[p];
+      if (r2b) b = b + f2c[p] - f2b[p];
+      va = b;
+    }
+    if constexpr (MODE == 0) {
+      g.Bb1[c] = v1;
+      if (r2a) g.Bb2[c] = v2;
+      g.Ba[c] = va;
+    } else {
+      if constexpr (MODE == 2) {
+        v1 = from_flux(v1, J1, ix, iy, iz, g.dbm, g.rdbm);
+        va = from_flux(va, JA, ix, iy, iz, g.dbm, g.rdbm);
+        v2 = from_flux(v2, J2, ix, iy, iz, g.dbm, g.rdbm);
+      }
+      g.ob1[c] = v1;
+      g.oa[c] = va;
+      g.ob2[c] = v2;
+    }
   }
 }
 
@@ -1126,7 +1261,9 @@ LARE_END  // namespace lare
 LARE_BEGIN
 
 template <int A, class R>
-void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
+// bmode: 1 for the first sweep of a remap (B read as stored, put in flux
+// form on the way), 2 for the last (B put back from flux form), 0 between.
+void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3], int bmode) {
   constexpr int T1 = A == 0 ? 1 : 0, T2 = A == 2 ? 1 : 2;  // transverse axes, T1 < T2
   constexpr int B1 = A == 0 ? 1 : 0, B2 = A == 2 ? 1 : 2;  // transported components, in file order
   constexpr int O1 = 3 - A - B1, O2 = 3 - A - B2;          // the remaining axis for each
@@ -1256,6 +1393,13 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     ba.na = na;
     ba.n0 = nx + 3;
     ba.n1 = (A == 1 ? nz : ny) + 3;
+    ba.dbm[0] = Ar.dxb;
+    ba.dbm[1] = Ar.dyb;
+    ba.dbm[2] = Ar.dzb;
+    ba.j1 = B1;
+    ba.j2 = B2;
+    ba.ax = A;
+    const bool pre = bmode == 1;
     const int k = run.prof_begin(A == 0 ? "remap_sweep_bflux_x" : "remap_sweep_bflux_march", 0, 7,
                                  (double)(nx + 3) * (ny + 3) * (nz + 3));
     if (A != 0) {
@@ -1263,30 +1407,52 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
       dim3 grd((ba.n0 + 31) / 32, (ba.n1 + 3) / 4, (na + 3 + kMarch - 1) / kMarch);
       if (sizeof(R) == 8) {  // one flux per thread in FP64 (half the registers); FP32 measured the same either way
         dim3 grd1((ba.n0 + 31) / 32, (ba.n1 + 3) / 4, 2 * ((na + 3 + kMarch - 1) / kMarch));
-        k_bflux_march1<R><<<grd1, blk, 0, run.s>>>(ba);
+        if (pre) {
+          k_bflux_march1<R, true><<<grd1, blk, 0, run.s>>>(ba);
+        } else {
+          k_bflux_march1<R, false><<<grd1, blk, 0, run.s>>>(ba);
+        }
+      } else if (pre) {
+        k_bflux_march<R, true><<<grd, blk, 0, run.s>>>(ba);
       } else {
-        k_bflux_march<R><<<grd, blk, 0, run.s>>>(ba);
+        k_bflux_march<R, false><<<grd, blk, 0, run.s>>>(ba);
       }
     } else {
       dim3 blk(32, 4, 1);
       dim3 grd((nx + 3 + kXOut - 1) / kXOut, (ny + 3 + 3) / 4, nz + 3);
-      k_bflux_x<R><<<grd, blk, 0, run.s>>>(ba, sx, sxy, nx, ny);
+      if (pre) {
+        k_bflux_x<R, true><<<grd, blk, 0, run.s>>>(ba, sx, sxy, nx, ny);
+      } else {
+        k_bflux_x<R, false><<<grd, blk, 0, run.s>>>(ba, sx, sxy, nx, ny);
+      }
     }
     run.prof_end(k);
     ++run.launches;
   }
 
-  // ---- K3: the four updates, each over its file's range
+  // ---- K3: the four updates, each over its file's range (the first sweep
+  // of a remap also puts B in flux form, the last puts it back)
   {
     R* const Ba = Bp[A];
     R* const Bb1 = Bp[B1];
     R* const Bb2 = Bp[B2];
+    // the predictor keeps B as B0: its first sweep writes the B0 buffers,
+    // which are then swapped in (lagran.F90:945-1062)
+    const bool keep = bmode == 1 && predictor;
+    R* const B0p[3] = {Ar.bx0.p, Ar.by0.p, Ar.bz0.p};
     BUpdArgs<R> gu;
     gu.f1 = f1;
     gu.f2 = f2;
     gu.Ba = Ba;
     gu.Bb1 = Bb1;
     gu.Bb2 = Bb2;
+    gu.oa = keep ? B0p[A] : Ba;
+    gu.ob1 = keep ? B0p[B1] : Bb1;
+    gu.ob2 = keep ? B0p[B2] : Bb2;
+    for (int d = 0; d < 3; ++d) {
+      gu.dbm[d] = dbm[d];
+      gu.rdbm[d] = Ar.rdb[d];
+    }
     gu.nx = nx;
     gu.ny = ny;
     gu.nz = nz;
@@ -1296,11 +1462,24 @@ void remap_sweep(Run<R>& run, bool predictor, int dt_slot, int pass[3]) {
     gu.SB1 = SB1;
     gu.SB2 = SB2;
     constexpr int kPts = sizeof(R) == 4 ? kBUpdZ32 : kBUpdZ64;
-    dim3 grd((nx + 2 + 31) / 32, (ny + 2 + 3) / 4, (nz + 2 + kPts - 1) / kPts);
-    const int k = run.prof_begin("remap_sweep_bupd", 0, 8, (double)(nx + 2) * (ny + 2) * (nz + 2));
-    k_bupdate<A, kPts, R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gu);
+    const int e = bmode == 0 ? 2 : 5;  // points per axis: the update box 0..n+1, or the arrays' -2..n+2
+    dim3 grd((nx + e + 31) / 32, (ny + e + 3) / 4, (nz + e + kPts - 1) / kPts);
+    // words: B (3) read and written, the two fluxes read
+    const int k = run.prof_begin("remap_sweep_bupd", 0, 8, (double)(nx + e) * (ny + e) * (nz + e));
+    if (bmode == 1) {
+      k_bupdate<A, kPts, 1, R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gu);
+    } else if (bmode == 2) {
+      k_bupdate<A, kPts, 2, R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gu);
+    } else {
+      k_bupdate<A, kPts, 0, R><<<grd, dim3(32, 4, 1), 0, run.s>>>(gu);
+    }
     run.prof_end(k);
     ++run.launches;
+    if (keep) {
+      std::swap(Ar.bx.p, Ar.bx0.p);
+      std::swap(Ar.by.p, Ar.by0.p);
+      std::swap(Ar.bz.p, Ar.bz0.p);
+    }
   }
   if (predictor) return;  // xremap.f90:159-162 (pass flag not reset)
 
