@@ -28,6 +28,10 @@
 // The face-averaged vx1 written back at :265 is only read again as
 // REAL(xpass)*(...) with xpass = 0, so it is formed in K8 and not stored.
 // Predictor sweeps (predictor_step = .TRUE.) stop after K3.
+// B's conversion to flux form before a remap's three sweeps
+// (remap.f90:43-69) and back after them (:101-127) happens in the first
+// sweep's K2 and K3 and the last sweep's K3 (remap_sweep's bmode), not in
+// passes of their own.
 //
 // Indexing is linear: c = ix + sx*iy + sxy*iz, neighbours by constant
 // offsets, with the axis a compile-time parameter.
