@@ -193,6 +193,12 @@ class EngineT : public EngineBase {
     run.elems = (size_t)elems;
     const long long off = 2 + 2LL * run.sx + 2LL * sxy;
     if (cudaStreamCreateWithFlags(&run.s, cudaStreamNonBlocking) != cudaSuccess) { err = "stream"; return LARE_ECUDA; }
+    // kernels with more than the default 48 KiB of dynamic shared memory
+    if (cudaFuncSetAttribute(k_lp4_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lp4_smem_bytes<R>()) !=
+        cudaSuccess) {
+      err = "shared memory attribute";
+      return LARE_ECUDA;
+    }
 
     std::vector<A3<R>*> all = {
         &run.a.rho, &run.a.energy, &run.a.temperature, &run.a.eta, &run.a.cv, &run.a.cv1, &run.a.p_visc,

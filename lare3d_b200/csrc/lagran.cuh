@@ -454,7 +454,7 @@ void prologue_and_shock_viscosity(Run<R>& run) {
     const dim3 blk(kL4X, kL4Y, 1);
     const dim3 grd((nx + 2 + kL4X - 1) / kL4X, (ny + 2 + kL4Y - 1) / kL4Y, (nz + 2 + kL4Z - 1) / kL4Z);
     const int k = run.prof_begin("shock_viscosity_lp4_tile", 0, 13, (double)(nx + 2) * (ny + 2) * (nz + 2));
-    k_lp4_tile<R><<<grd, blk, 0, run.s>>>(l4);
+    k_lp4_tile<R><<<grd, blk, lp4_smem_bytes<R>(), run.s>>>(l4);
     run.prof_end(k);
     ++run.launches;
   }
