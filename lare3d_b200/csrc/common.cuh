@@ -308,12 +308,23 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long* u, double v) 
 }
 
 template <int NV, class Fn>
-__global__ void __launch_bounds__(256) k_box_min(int i0, int j0, int k0, int ni, int nj, Fn fn, unsigned long long* out) {
+__global__ void __launch_bounds__(256) k_box_min(int i0, int j0, int k0, int ni, int nj, int nk, int planes, Fn fn,
+                                                 unsigned long long* out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   double v[NV];
   for (int q = 0; q < NV; ++q) v[q] = DBL_MAX;
-  if (i < ni && j < nj) fn(i0 + i, j0 + j, k0 + (int)blockIdx.z, v);
+  // `planes` consecutive planes per block (the min does not depend on the
+  // order), so that few blocks contend for the atomic on the result
+  if (i < ni && j < nj) {
+    const int kb = (int)blockIdx.z * planes;
+    for (int kk = kb; kk < kb + planes && kk < nk; ++kk) {
+      double w[NV];
+      for (int q = 0; q < NV; ++q) w[q] = DBL_MAX;
+      fn(i0 + i, j0 + j, k0 + kk, w);
+      for (int q = 0; q < NV; ++q) v[q] = fmin(v[q], w[q]);
+    }
+  }
   __shared__ double sh[NV][8];
   for (int q = 0; q < NV; ++q) {
     double x = v[q];

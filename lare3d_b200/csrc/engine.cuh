@@ -324,10 +324,14 @@ template <int NV, class R, class Fn>
 inline void box_min(Run<R>& run, const char* site, int i0, int i1, int j0, int j1, int k0, int k1, Fn fn, int uslot,
                     int words = 0) {
   int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+  // planes per block: fewer blocks contend for the atomic, at the cost of
+  // resident warps; measured at 256^3: 8 in FP32 (0.23 -> 0.18 ms for set_dt),
+  // 1 in FP64 (8 took 0.38 -> 0.42 ms)
+  constexpr int kMinPlanes = sizeof(R) == 4 ? 8 : 1;
   dim3 blk(64, 4, 1);
-  dim3 grd((ni + 63) / 64, (nj + 3) / 4, nk);
+  dim3 grd((ni + 63) / 64, (nj + 3) / 4, (nk + kMinPlanes - 1) / kMinPlanes);
   int k = run.prof_begin(site, 0, words, (double)ni * nj * nk);
-  k_box_min<NV><<<grd, blk, 0, run.s>>>(i0, j0, k0, ni, nj, fn, run.us + uslot);
+  k_box_min<NV><<<grd, blk, 0, run.s>>>(i0, j0, k0, ni, nj, nk, kMinPlanes, fn, run.us + uslot);
   run.prof_end(k);
   ++run.launches;
 }
