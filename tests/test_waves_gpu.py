@@ -1,4 +1,5 @@
-"""The linear sound, Alfven and fast waves of tests/test_waves_cpu.py through
+"""The linear sound, Alfven and fast waves of tests/test_waves_cpu.py (and Sod's
+shock tube of tests/test_shock_tube_cpu.py) through
 the three GPU engines, along each axis: the exact engine bit for bit with
 the oracle, the FP64 product engine within 1e-10 of it (L2 norm of the
 difference of every state field over that of the field or, for fields that
@@ -92,3 +93,33 @@ def test_diffusion_through_engines(built, axis):
             _, amp = mode(g, d, axis, name, base)
             assert abs(-math.log(amp / a0) / t / lam - 1.0) < 2e-3, (case, precision)
             g.close()
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2], ids=["x", "y", "z"])
+def test_shock_tube_through_engines(built, axis):
+    """Sod's tube of tests/test_shock_tube_cpu.py, shock viscosity on: the
+    exact engine bit for bit with the oracle, the product engine within
+    1e-10, and every engine within the exact Riemann solution's bars."""
+    from lare3d_b200 import gpu
+    from oracle import oracle
+    from test_shock_tube_cpu import L1_BAR, N, PLATEAU_BAR, SHOCK_BAR, run_tube, tube_deck, tube_errors, tube_profile
+    d = tube_deck(axis)
+    r = oracle.simulation(d)
+    r.start(d.state)
+    t_ref = run_tube(r)
+    x = d.metrics["xyz"[axis] + "c"][2:2 + N]
+    for precision, tol in ((gpu.EXACT64, 0.0), (gpu.FP64, 1e-10), (gpu.FP32, None)):
+        d = tube_deck(axis)
+        g = gpu.simulation(d, precision=precision)
+        g.start(d.state)
+        t = run_tube(g)
+        assert abs(t - t_ref) <= (1e-12 if precision != gpu.FP32 else 1e-5) * t_ref
+        for f in STATE if tol is not None else ():
+            a, b = g.get_field(f), r.get_field(f)
+            if tol == 0.0:
+                assert np.array_equal(a, b), f"sod {axis} {f}: exact engine differs from the oracle"
+            else:
+                assert scaled_l2(a, b) <= tol, (axis, f, scaled_l2(a, b))
+        l1, dxs, dplat = tube_errors(tube_profile(g.get_field("rho"), axis), x, t)
+        assert l1 < L1_BAR and abs(dxs) < SHOCK_BAR / N and dplat < PLATEAU_BAR, (precision, l1, dxs * N, dplat)
+        g.close()
