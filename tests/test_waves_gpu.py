@@ -1,5 +1,6 @@
 """The linear sound, Alfven and fast waves of tests/test_waves_cpu.py (and Sod's
-shock tube of tests/test_shock_tube_cpu.py) through
+shock tube of tests/test_shock_tube_cpu.py and the heat wave of
+tests/test_heat_wave_cpu.py) through
 the three GPU engines, along each axis: the exact engine bit for bit with
 the oracle, the FP64 product engine within 1e-10 of it (L2 norm of the
 difference of every state field over that of the field or, for fields that
@@ -122,4 +123,32 @@ def test_shock_tube_through_engines(built, axis):
                 assert scaled_l2(a, b) <= tol, (axis, f, scaled_l2(a, b))
         l1, dxs, dplat = tube_errors(tube_profile(g.get_field("rho"), axis), x, t)
         assert l1 < L1_BAR and abs(dxs) < SHOCK_BAR / N and dplat < PLATEAU_BAR, (precision, l1, dxs * N, dplat)
+        g.close()
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2], ids=["x", "y", "z"])
+def test_heat_wave_through_engines(built, axis):
+    """The Zel'dovich heat wave of tests/test_heat_wave_cpu.py: the FP64
+    engines within 1e-12 (exact; T^2.5 is formed as T*T*sqrt(T), not by pow)
+    and 1e-10 (product) of the oracle, every engine within the similarity
+    solution's bars."""
+    from lare3d_b200 import gpu
+    from oracle import oracle
+    from test_heat_wave_cpu import NW, advance, heat_wave_deck, wave_errors, wave_profile
+    d = heat_wave_deck(axis)
+    r = oracle.simulation(d)
+    r.start(d.state)
+    advance(r)
+    ref = r.get_field("energy")
+    x = d.metrics["xyz"[axis] + "c"][2:2 + NW]
+    for precision, tol in ((gpu.EXACT64, 1e-12), (gpu.FP64, 1e-10), (gpu.FP32, None)):
+        d = heat_wave_deck(axis)
+        g = gpu.simulation(d, precision=precision)
+        g.start(d.state)
+        advance(g)
+        energy = g.get_field("energy")
+        if tol is not None:
+            assert scaled_l2(energy, ref) <= tol, (precision, scaled_l2(energy, ref))
+        dtc, l1, fronts = wave_errors(x, wave_profile(energy, axis))
+        assert dtc < 5e-3 and l1 < 3e-3 and max(abs(f) for f in fronts) < 1.0, (precision, dtc, l1, fronts)
         g.close()
